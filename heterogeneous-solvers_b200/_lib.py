@@ -1,0 +1,115 @@
+"""ctypes binding of libhs_b200.so (the C ABI declared in include/hs_b200.h).
+
+The shared library is built in place (``make -C heterogeneous-solvers_b200``)
+and must be present: there is no fallback path, a missing or stale library
+raises immediately.
+"""
+import ctypes
+import os
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libhs_b200.so"
+ABI_VERSION = 1
+
+HS_OK = 0
+STATUS_NAMES = {
+    0: "HS_OK", 1: "HS_ERR_INVALID_ARG", 2: "HS_ERR_OOM", 3: "HS_ERR_NOT_SPD", 4: "HS_ERR_NO_CONVERGENCE",
+    5: "HS_ERR_REFINEMENT_STALLED", 6: "HS_ERR_CUDA", 7: "HS_ERR_TIMEOUT", 8: "HS_ERR_UNSUPPORTED",
+}
+
+
+class HSError(RuntimeError):
+    """A non-OK hs_status; ``status`` holds the code, the message is hs_last_error()."""
+
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class NotSPDError(HSError):
+    pass
+
+
+class NoConvergenceError(HSError):
+    pass
+
+
+class SolveReport(ctypes.Structure):
+    _fields_ = [("info", ctypes.c_int64), ("iterations", ctypes.c_int64), ("assemble_ms", ctypes.c_double),
+                ("factor_ms", ctypes.c_double), ("solve_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+
+# name -> argument types (all return hs_status unless listed in _RESTYPES)
+SIGNATURES = {
+    "hs_abi_version": [],
+    "hs_last_error": [],
+    "hs_status_string": [_I],
+    "hs_ctx_create": [_I, _P, ctypes.POINTER(_P)],
+    "hs_ctx_destroy": [_P],
+    "hs_ctx_set_stream": [_P, _P],
+    "hs_ctx_set_problem": [_P, _I64, _I],
+    "hs_sync": [_P],
+    "hs_packed_matrix_size": [_I64, _I],
+    "hs_padded_vector_size": [_I64, _I],
+    "hs_potrf_block": [_P, _P, _I, _I],
+    "hs_ctx_take_info": [_P, ctypes.POINTER(_I64)],
+    "hs_trsm_panel": [_P, _P, _I, _I, _I, _I],
+    "hs_syrk_diag": [_P, _P, _I, _I, _I, _I, _I],
+    "hs_gemm_trailing": [_P, _P, _I, _I, _I, _I, _I],
+    "hs_symv_block": [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I],
+    "hs_trsv_block": [_P, _P, _P, _I, _I, _I],
+    "hs_column_update": [_P, _P, _P, _I, _I, _I, _I, _I, _I],
+    "hs_scale_block": [_P, _P, _D, _P, _I, _I],
+    "hs_add_block": [_P, _P, _P, _P, _I, _I],
+    "hs_sub_block": [_P, _P, _P, _P, _I, _I],
+    "hs_axpy_block": [_P, _P, _D, _P, _P, _I, _I],
+    "hs_dot_block": [_P, _P, _P, _P, _I, _I],
+    "hs_rbf_assemble": [_P, _P, _P, _I, _P, _I, _D, _D],
+    "hs_cholesky_factor": [_P, _P, ctypes.POINTER(_I64)],
+    "hs_cholesky_solve": [_P, _P, _P],
+    "hs_cg_solve": [_P, _P, _P, _P, _D, _I64, ctypes.POINTER(_I64), ctypes.POINTER(_D), ctypes.POINTER(_D)],
+    "hs_gp_solve_host": [_P, _P, _P, _I, _P, _I, _D, _D, _I, _D, _I64, _P, ctypes.POINTER(SolveReport)],
+}
+_RESTYPES = {"hs_abi_version": _I, "hs_last_error": ctypes.c_char_p, "hs_status_string": ctypes.c_char_p,
+             "hs_packed_matrix_size": _I64, "hs_padded_vector_size": _I64}
+
+_lib = None
+
+
+def load():
+    """Load the library once; raises if it is missing or has another ABI version."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {_HERE}` (no CPU fallback exists)")
+    lib = ctypes.CDLL(os.fspath(LIB_PATH))
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = _RESTYPES.get(name, _I)
+    if lib.hs_abi_version() != ABI_VERSION:
+        raise ImportError(f"{LIB_PATH}: ABI version {lib.hs_abi_version()} != {ABI_VERSION}")
+    _lib = lib
+    return lib
+
+
+def check(status):
+    if status == HS_OK:
+        return
+    msg = load().hs_last_error().decode(errors="replace")
+    if status == 3:
+        raise NotSPDError(status, msg)
+    if status == 4:
+        raise NoConvergenceError(status, msg)
+    raise HSError(status, msg)
+
+
+def call(name, *args):
+    check(getattr(load(), name)(*args))

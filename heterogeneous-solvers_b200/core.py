@@ -1,0 +1,471 @@
+"""Host-side mirror of the reference's operator and solver interface.
+
+Names, argument order and meaning follow TimThuering/Heterogeneous-Solvers
+(paths relative to its root); a ``Context`` takes the place of the
+``sycl::queue`` argument and of the ``conf::N`` / ``conf::matrixBlockSize``
+globals (src/utility/Configuration.hpp:21-118).  Device memory is held in
+torch CUDA tensors (float64); every operator launches the CUDA kernels of
+libhs_b200.so through its C ABI.  There is no CPU implementation here.
+"""
+import ctypes
+import math
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import HSError, NoConvergenceError, NotSPDError, SolveReport, call
+
+__all__ = [
+    "Context", "SymmetricMatrix", "RightHandSide", "MatrixOperations", "MatrixMatrixOperations",
+    "MatrixVectorOperations", "VectorOperations", "Cholesky", "TriangularSystemSolver", "CG",
+    "MatrixGenerator", "MatrixParser", "HSError", "NotSPDError", "NoConvergenceError", "block_id",
+    "packed_size", "padded_size", "gp_solve_host",
+]
+
+
+def block_id(i, j, nb):
+    """Id of block (i, j), i >= j, in column-by-column order (SymmetricMatrix.hpp:9-35)."""
+    return i + nb * (nb - 1) // 2 - (nb - j - 1) * (nb - j) // 2
+
+
+def packed_size(N, bsz):
+    nb = -(-N // bsz)
+    return nb * (nb + 1) // 2 * bsz * bsz
+
+
+def padded_size(N, bsz):
+    return -(-N // bsz) * bsz
+
+
+def _dptr(t, ctx=None):
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"expected a torch CUDA float64 tensor, got {type(t).__name__}")
+    if not t.is_cuda or t.dtype != torch.float64 or not t.is_contiguous():
+        raise TypeError(f"expected a contiguous CUDA float64 tensor, got {t.dtype} on {t.device}")
+    if ctx is not None and t.device.index != ctx.device:
+        raise ValueError(f"tensor on cuda:{t.device.index}, context on cuda:{ctx.device}")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Context:
+    """Device, stream and problem size of a sequence of calls.
+
+    Replaces the sycl::queue of every reference call plus conf::N and
+    conf::matrixBlockSize.  By default the context runs on torch's current
+    stream of ``device`` so that it orders with torch's own work.
+    """
+
+    def __init__(self, device=0, stream=None, N=None, matrixBlockSize=None):
+        _lib.load()
+        self.device = int(device)
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        self.stream = stream
+        handle = ctypes.c_void_p()
+        call("hs_ctx_create", self.device, ctypes.c_void_p(stream.cuda_stream), ctypes.byref(handle))
+        self.handle = handle
+        self.N = None
+        self.matrixBlockSize = None
+        if N is not None:
+            self.set_problem(N, matrixBlockSize)
+
+    def set_problem(self, N, matrixBlockSize):
+        call("hs_ctx_set_problem", self.handle, int(N), int(matrixBlockSize))
+        self.N = int(N)
+        self.matrixBlockSize = int(matrixBlockSize)
+        return self
+
+    @property
+    def blockCountXY(self):
+        return -(-self.N // self.matrixBlockSize)
+
+    def sync(self):
+        call("hs_sync", self.handle)
+
+    def take_info(self):
+        v = ctypes.c_int64()
+        call("hs_ctx_take_info", self.handle, ctypes.byref(v))
+        return v.value
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and _lib._lib is not None:
+            _lib._lib.hs_ctx_destroy(self.handle)
+        self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SymmetricMatrix:
+    """Packed lower block triangle (src/dataStructures/SymmetricMatrix.hpp:36-54).
+
+    ``matrixData`` is a float64 tensor of T*bsz*bsz entries (host by default,
+    ``device=`` for a CUDA tensor), zero-initialised like the reference's
+    std::vector.
+    """
+
+    def __init__(self, N, blockSize, device=None):
+        self.N = int(N)
+        self.blockSize = int(blockSize)
+        self.blockCountXY = int(math.ceil(self.N / self.blockSize))
+        self.matrixData = torch.zeros(packed_size(self.N, self.blockSize), dtype=torch.float64,
+                                      device=device if device is not None else "cpu")
+
+    def block(self, i, j):
+        """View of stored block (i, j), i >= j, as bsz x bsz."""
+        b = self.blockSize
+        s = block_id(i, j, self.blockCountXY) * b * b
+        return self.matrixData[s:s + b * b].view(b, b)
+
+    def to_dense(self):
+        """Full N x N matrix (lower blocks mirrored) as a float64 numpy array."""
+        b, nb = self.blockSize, self.blockCountXY
+        data = self.matrixData.detach().cpu().numpy()
+        full = np.zeros((nb * b, nb * b))
+        for j in range(nb):
+            for i in range(j, nb):
+                s = block_id(i, j, nb) * b * b
+                blk = data[s:s + b * b].reshape(b, b)
+                full[i * b:(i + 1) * b, j * b:(j + 1) * b] = blk
+                if i != j:
+                    full[j * b:(j + 1) * b, i * b:(i + 1) * b] = blk.T
+        return full[:self.N, :self.N]
+
+
+class RightHandSide:
+    """Zero-padded vector of nb*bsz entries (src/dataStructures/RightHandSide.hpp:12-30)."""
+
+    def __init__(self, N, blockSize, device=None):
+        self.N = int(N)
+        self.blockSize = int(blockSize)
+        self.blockCountX = int(math.ceil(self.N / self.blockSize))
+        self.rightHandSideData = torch.zeros(self.blockCountX * self.blockSize, dtype=torch.float64,
+                                             device=device if device is not None else "cpu")
+
+
+# ------------------------------------------------------------------ operators
+class MatrixOperations:
+    """src/kernel/MatrixOperations.hpp:9-56 — POTRF of one diagonal block."""
+
+    @staticmethod
+    def cholesky(ctx, A, blockID, blockRow):
+        call("hs_potrf_block", ctx.handle, _dptr(A, ctx), int(blockID), int(blockRow))
+
+    cholesky_GPU = cholesky
+    cholesky_optimizedGPU = cholesky
+
+
+class MatrixMatrixOperations:
+    """src/kernel/MatrixMatrixOperations.hpp:8-295 — TRSM, SYRK and GEMM steps."""
+
+    @staticmethod
+    def triangularSolve(ctx, A, blockID, blockRow, blockStart, blockCount):
+        call("hs_trsm_panel", ctx.handle, _dptr(A, ctx), int(blockID), int(blockRow), int(blockStart),
+             int(blockCount))
+
+    triangularSolve_optimizedGPU = triangularSolve
+    triangularSolve_optimizedCPU = triangularSolve
+
+    @staticmethod
+    def symmetricMatrixMatrixDiagonal(ctx, A, blockID, blockRow, blockStart, blockCount, blockCountXY):
+        call("hs_syrk_diag", ctx.handle, _dptr(A, ctx), int(blockID), int(blockRow), int(blockStart),
+             int(blockCount), int(blockCountXY))
+
+    symmetricMatrixMatrixDiagonal_optimizedGPU = symmetricMatrixMatrixDiagonal
+    symmetricMatrixMatrixDiagonal_optimizedCPU = symmetricMatrixMatrixDiagonal
+
+    @staticmethod
+    def matrixMatrixStep(ctx, A, blockID, blockRow, blockStart, blockCount, blockCountXY):
+        call("hs_gemm_trailing", ctx.handle, _dptr(A, ctx), int(blockID), int(blockRow), int(blockStart),
+             int(blockCount), int(blockCountXY))
+
+    matrixMatrixStep_optimizedGPU = matrixMatrixStep
+    matrixMatrixStep_optimizedGPU2 = matrixMatrixStep
+    matrixMatrixStep_optimizedGPU3 = matrixMatrixStep
+    matrixMatrixStep_optimizedCPU = matrixMatrixStep
+    matrixMatrixStep_optimizedCPU2 = matrixMatrixStep
+
+
+class MatrixVectorOperations:
+    """src/kernel/MatrixVectorOperations.hpp:8-114 — SYMV, TRSV, column update."""
+
+    @staticmethod
+    def matrixVectorBlock(ctx, A, b, result, blockStart_i, blockStart_j, blockCount_i, blockCount_j,
+                          blockCountXY, reset=True):
+        call("hs_symv_block", ctx.handle, _dptr(A, ctx), _dptr(b, ctx), _dptr(result, ctx), int(blockStart_i),
+             int(blockStart_j), int(blockCount_i), int(blockCount_j), int(blockCountXY), int(bool(reset)))
+
+    matrixVectorBlock_GPU = matrixVectorBlock
+    matrixVectorBlock_CPU = matrixVectorBlock
+
+    @staticmethod
+    def triangularSolveBlockVector(ctx, A, b, blockRow, blockID, transposed):
+        call("hs_trsv_block", ctx.handle, _dptr(A, ctx), _dptr(b, ctx), int(blockRow), int(blockID),
+             int(bool(transposed)))
+
+    @staticmethod
+    def matrixVectorColumnUpdate(ctx, A, b, blockStart, blockCount, blockRow, blockID, blockCountXY, transposed):
+        call("hs_column_update", ctx.handle, _dptr(A, ctx), _dptr(b, ctx), int(blockStart), int(blockCount),
+             int(blockRow), int(blockID), int(blockCountXY), int(bool(transposed)))
+
+
+class VectorOperations:
+    """src/kernel/VectorOperations.hpp:8-126 — block-range vector kernels."""
+
+    @staticmethod
+    def scaleVectorBlock(ctx, x, alpha, result, blockStart_i, blockCount_i):
+        call("hs_scale_block", ctx.handle, _dptr(x, ctx), float(alpha), _dptr(result, ctx), int(blockStart_i),
+             int(blockCount_i))
+
+    @staticmethod
+    def addVectorBlock(ctx, x, y, result, blockStart_i, blockCount_i):
+        call("hs_add_block", ctx.handle, _dptr(x, ctx), _dptr(y, ctx), _dptr(result, ctx), int(blockStart_i),
+             int(blockCount_i))
+
+    @staticmethod
+    def subVectorBlock(ctx, x, y, result, blockStart_i, blockCount_i):
+        call("hs_sub_block", ctx.handle, _dptr(x, ctx), _dptr(y, ctx), _dptr(result, ctx), int(blockStart_i),
+             int(blockCount_i))
+
+    @staticmethod
+    def scaleAndAddVectorBlock(ctx, x, alpha, y, result, blockStart_i, blockCount_i):
+        call("hs_axpy_block", ctx.handle, _dptr(x, ctx), float(alpha), _dptr(y, ctx), _dptr(result, ctx),
+             int(blockStart_i), int(blockCount_i))
+
+    @staticmethod
+    def scalarProduct(ctx, x, y, result, blockStart_i, blockCount_i):
+        """Writes the finished dot product to result[0] and returns 1 (one
+        partial), so that a following sumFinalScalarProduct is the identity —
+        the reference's two calls (VectorOperations.cpp:84-185) in one."""
+        call("hs_dot_block", ctx.handle, _dptr(x, ctx), _dptr(y, ctx), _dptr(result, ctx), int(blockStart_i),
+             int(blockCount_i))
+        return 1
+
+    scalarProduct_CPU = scalarProduct
+
+    @staticmethod
+    def sumFinalScalarProduct(ctx, result, workGroupCount):
+        if workGroupCount != 1:
+            raise ValueError("workGroupCount must come from scalarProduct")
+
+    sumFinalScalarProduct_CPU = sumFinalScalarProduct
+
+
+# ------------------------------------------------------------------ solvers
+def _to_device(t, ctx):
+    return t if t.is_cuda else t.to(f"cuda:{ctx.device}", non_blocking=False).contiguous()
+
+
+class Cholesky:
+    """src/solver/cholesky/Cholesky.hpp:22-168: blocked right-looking Cholesky.
+
+    ``solve_heterogeneous()`` factors A in place on the GPU (every block row on
+    the GPU, no split or load balancing) and copies L back into
+    ``A.matrixData`` when that lives on the host (copyResultFromGPU,
+    Cholesky.cpp:361-397).  ``A_gpu`` keeps the device copy for the
+    TriangularSystemSolver, as main.cpp:232 lends it.
+    """
+
+    def __init__(self, A, ctx):
+        self.A = A
+        self.ctx = ctx
+        self.A_gpu = None
+        self.info = -1
+        self.factor_ms = None
+
+    def solve_heterogeneous(self):
+        ctx = self.ctx
+        ctx.set_problem(self.A.N, self.A.blockSize)
+        self.A_gpu = _to_device(self.A.matrixData, ctx)
+        info = ctypes.c_int64(-1)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(ctx.stream)
+        status = _lib.load().hs_cholesky_factor(ctx.handle, _dptr(self.A_gpu, ctx), ctypes.byref(info))
+        ev1.record(ctx.stream)
+        self.info = info.value
+        _lib.check(status)
+        ctx.stream.synchronize()
+        self.factor_ms = ev0.elapsed_time(ev1)
+        if not self.A.matrixData.is_cuda:
+            self.A.matrixData.copy_(self.A_gpu.cpu())
+        else:
+            self.A.matrixData = self.A_gpu
+        return self
+
+
+class TriangularSystemSolver:
+    """src/solver/cholesky/TriangularSystemSolver.hpp:10-39: forward then
+    backward block substitution with the factor, in place on b."""
+
+    def __init__(self, A, A_gpu, b, ctx):
+        self.A = A
+        self.A_gpu = A_gpu if A_gpu is not None else _to_device(A.matrixData, ctx)
+        self.b = b
+        self.ctx = ctx
+
+    def solve(self):
+        """Overwrites b.rightHandSideData with the solution; returns the time in ms."""
+        ctx = self.ctx
+        ctx.set_problem(self.A.N, self.A.blockSize)
+        t0 = time.perf_counter()
+        b_gpu = _to_device(self.b.rightHandSideData, ctx)
+        if b_gpu is self.b.rightHandSideData:
+            b_gpu = b_gpu.clone()
+        call("hs_cholesky_solve", ctx.handle, _dptr(self.A_gpu, ctx), _dptr(b_gpu, ctx))
+        ctx.stream.synchronize()
+        if self.b.rightHandSideData.is_cuda:
+            self.b.rightHandSideData.copy_(b_gpu)
+        else:
+            self.b.rightHandSideData.copy_(b_gpu.cpu())
+        return (time.perf_counter() - t0) * 1e3
+
+
+class CG:
+    """src/solver/cg/CG.hpp:14-142: conjugate gradients on the packed matrix.
+
+    ``solveHeterogeneous(epsilon, iMax)`` runs on the GPU (every block row);
+    the solution lands in ``self.x`` (host tensor), the iteration count in
+    ``self.iterations``.  Defaults follow Configuration.hpp:26-27.
+    """
+
+    def __init__(self, A, b, ctx):
+        if A.N != b.N:
+            raise ValueError(f"Dimensions of A and b do not match: {A.N} != {b.N}")
+        if A.blockCountXY != b.blockCountX:
+            raise ValueError(f"Block count of A and b do not match: {A.blockCountXY} != {b.blockCountX}")
+        self.A = A
+        self.b = b
+        self.ctx = ctx
+        self.x = torch.zeros_like(b.rightHandSideData, device="cpu")
+        self.iterations = 0
+        self.delta_new = None
+        self.delta_zero = None
+
+    def solveHeterogeneous(self, epsilon=1.0e-6, iMax=100000):
+        ctx = self.ctx
+        ctx.set_problem(self.A.N, self.A.blockSize)
+        A_gpu = _to_device(self.A.matrixData, ctx)
+        b_gpu = _to_device(self.b.rightHandSideData, ctx)
+        x_gpu = torch.empty_like(b_gpu)
+        it, dn, d0 = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+        status = _lib.load().hs_cg_solve(ctx.handle, _dptr(A_gpu, ctx), _dptr(b_gpu, ctx), _dptr(x_gpu, ctx),
+                                         float(epsilon), int(iMax), ctypes.byref(it), ctypes.byref(dn),
+                                         ctypes.byref(d0))
+        self.iterations, self.delta_new, self.delta_zero = it.value, dn.value, d0.value
+        self.x = x_gpu.cpu()
+        if status != 4:  # reaching iMax is reported but, as in the reference, not an exception
+            _lib.check(status)
+        return self
+
+
+class MatrixGenerator:
+    """src/utility/MatrixGenerator.hpp:11-65 — kernel-matrix generation on the GPU."""
+
+    @staticmethod
+    def windowInputs(series):
+        """The reference's sliding window of 8 regressors (MatrixGenerator.cpp:76-99):
+        X[i, k] = series[i + k - 7], zeros before the series start."""
+        s = np.asarray(series, dtype=np.float64)
+        padded = np.concatenate([np.zeros(7), s])
+        return np.lib.stride_tricks.sliding_window_view(padded, 8)[: len(s)].copy()
+
+    @staticmethod
+    def assemble(ctx, A, X, lengthscale=1.0, signal_variance=1.0, noise_variance=0.01):
+        """K = sf2 * exp(-|x_i - x_j|^2 / (2 l^2)) + sn2 I into the packed device
+        tensor A; ``lengthscale`` is a scalar or one value per feature (ARD)."""
+        Xd = X if isinstance(X, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(X, dtype=np.float64))
+        Xd = _to_device(Xd.to(torch.float64), ctx).contiguous()
+        if Xd.dim() != 2 or Xd.shape[0] != ctx.N:
+            raise ValueError("X must be N x d")
+        ell = np.atleast_1d(np.asarray(lengthscale, dtype=np.float64))
+        call("hs_rbf_assemble", ctx.handle, _dptr(A, ctx), _dptr(Xd, ctx), int(Xd.shape[1]),
+             ell.ctypes.data_as(ctypes.c_void_p), int(ell.size), float(signal_variance), float(noise_variance))
+
+    @staticmethod
+    def generateSPDMatrix(ctx, series, N, matrixBlockSize, lengthscale=1.0, signal_variance=1.0,
+                          noise_variance=0.01):
+        """generateSPDMatrix (MatrixGenerator.cpp:73-162): the first N values of
+        a 1-D series (array or path of one value per line), 8-sample window,
+        defaults l = 1, sf2 = 1, sn2 = 0.01; returns a device SymmetricMatrix."""
+        if isinstance(series, (str, Path)):
+            series = np.loadtxt(series, dtype=np.float64, ndmin=1)
+        series = np.asarray(series, dtype=np.float64)
+        if series.size < N:
+            raise ValueError("Not enough data available!")
+        ctx.set_problem(N, matrixBlockSize)
+        A = SymmetricMatrix(N, matrixBlockSize, device=f"cuda:{ctx.device}")
+        MatrixGenerator.assemble(ctx, A.matrixData, MatrixGenerator.windowInputs(series[:N]), lengthscale,
+                                 signal_variance, noise_variance)
+        return A
+
+
+class MatrixParser:
+    """src/utility/MatrixParser.hpp:10-73 — the reference's text formats."""
+
+    @staticmethod
+    def _rows(text):
+        lines = [ln for ln in text.strip().splitlines()]
+        if not lines or not lines[0].startswith("#"):
+            raise ValueError("Invalid matrix format. First line has to be '# <N>!'")
+        return int(lines[0][2:]), lines[1:]
+
+    @staticmethod
+    def parseSymmetricMatrix(path, matrixBlockSize):
+        """`# N` then row i holding its lower-triangle values `v; v; ...`
+        (MatrixParser.cpp:11-41, processRow :107-168); diagonal blocks mirrored."""
+        N, lines = MatrixParser._rows(Path(path).read_text())
+        A = SymmetricMatrix(N, matrixBlockSize)
+        b, nb = matrixBlockSize, A.blockCountXY
+        data = A.matrixData.numpy()
+        for i, line in enumerate(lines[:N]):
+            vals = [float(v) for v in line.split(";")]
+            if len(vals) != i + 1:
+                raise ValueError(f"row {i} has {len(vals)} values, expected {i + 1}")
+            bi, ri = divmod(i, b)
+            for j, v in enumerate(vals):
+                bj, rj = divmod(j, b)
+                base = block_id(bi, bj, nb) * b * b
+                data[base + ri * b + rj] = v
+                if bi == bj:
+                    data[base + rj * b + ri] = v
+        return A
+
+    @staticmethod
+    def parseRightHandSide(path, matrixBlockSize):
+        """`# N` then one line `v; v; ...` (MatrixParser.cpp:43-72)."""
+        N, lines = MatrixParser._rows(Path(path).read_text())
+        vals = [float(v) for v in lines[0].split(";")]
+        b = RightHandSide(N, matrixBlockSize)
+        b.rightHandSideData[:N] = torch.tensor(vals[:N], dtype=torch.float64)
+        return b
+
+
+def gp_solve_host(ctx, X, y, lengthscale=1.0, signal_variance=1.0, noise_variance=0.01, algorithm="cholesky",
+                  epsilon=1e-10, iMax=100000):
+    """End-to-end GP solve through host buffers (hs_gp_solve_host): host X
+    (N x d) and y (N) in, host x = K^-1 y out, plus the phase report."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    N, d = X.shape
+    if ctx.N != N:
+        raise ValueError("context N differs from X")
+    ell = np.atleast_1d(np.asarray(lengthscale, dtype=np.float64))
+    x = np.empty(N, dtype=np.float64)
+    rep = SolveReport()
+    call("hs_gp_solve_host", ctx.handle, X.ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p), d,
+         ell.ctypes.data_as(ctypes.c_void_p), int(ell.size), float(signal_variance), float(noise_variance),
+         0 if algorithm == "cholesky" else 1, float(epsilon), int(iMax), x.ctypes.data_as(ctypes.c_void_p),
+         ctypes.byref(rep))
+    return x, rep

@@ -1,0 +1,338 @@
+// hs_api.cu — the C ABI: context management, error reporting, argument
+// validation and the operator-level entry points of include/hs_b200.h.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "hs_internal.cuh"
+
+namespace hs {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+hs_status cuda_fail(cudaError_t e, const char* what) {
+    set_error(std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+    return e == cudaErrorMemoryAllocation ? HS_ERR_OOM : HS_ERR_CUDA;
+}
+
+hs_status require_ctx(hs_ctx ctx, const char* fn) {
+    if (!ctx) {
+        set_error(std::string(fn) + ": null context");
+        return HS_ERR_INVALID_ARG;
+    }
+    if (ctx->bsz <= 0 && std::strcmp(fn, "hs_ctx_set_problem") != 0) {
+        set_error(std::string(fn) + ": call hs_ctx_set_problem first");
+        return HS_ERR_INVALID_ARG;
+    }
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    return HS_OK;
+}
+
+hs_status ensure_scratch(hs_ctx ctx, size_t bytes) {
+    if (ctx->scratch_bytes >= bytes) return HS_OK;
+    size_t want = bytes + bytes / 8;
+    if (want < 1024 * 1024) want = 1024 * 1024;
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->side) HS_CUDA(cudaStreamSynchronize(ctx->side));
+    if (ctx->scratch) HS_CUDA(cudaFree(ctx->scratch));
+    ctx->scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    HS_CUDA(cudaMalloc(&ctx->scratch, want));
+    ctx->scratch_bytes = want;
+    return HS_OK;
+}
+
+hs_status ensure_work(hs_ctx ctx, size_t bytes) {
+    if (ctx->work_bytes >= bytes) return HS_OK;
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->work) HS_CUDA(cudaFree(ctx->work));
+    ctx->work = nullptr;
+    ctx->work_bytes = 0;
+    HS_CUDA(cudaMalloc(&ctx->work, bytes));
+    ctx->work_bytes = bytes;
+    return HS_OK;
+}
+
+__global__ void set_i64_kernel(long long* p, long long v) { *p = v; }
+
+}  // namespace hs
+
+using namespace hs;
+
+#define HS_API_BEGIN(fn)                         \
+    {                                            \
+        hs_status st_ = require_ctx(ctx, fn);    \
+        if (st_ != HS_OK) return st_;            \
+    }
+
+#define HS_ARG(cond, msg)                                   \
+    do {                                                    \
+        if (!(cond)) {                                      \
+            set_error(std::string(__func__) + ": " + (msg)); \
+            return HS_ERR_INVALID_ARG;                      \
+        }                                                   \
+    } while (0)
+
+extern "C" {
+
+int hs_abi_version(void) { return HS_B200_ABI_VERSION; }
+
+const char* hs_last_error(void) { return g_last_error.c_str(); }
+
+const char* hs_status_string(hs_status s) {
+    switch (s) {
+        case HS_OK: return "HS_OK";
+        case HS_ERR_INVALID_ARG: return "HS_ERR_INVALID_ARG";
+        case HS_ERR_OOM: return "HS_ERR_OOM";
+        case HS_ERR_NOT_SPD: return "HS_ERR_NOT_SPD";
+        case HS_ERR_NO_CONVERGENCE: return "HS_ERR_NO_CONVERGENCE";
+        case HS_ERR_REFINEMENT_STALLED: return "HS_ERR_REFINEMENT_STALLED";
+        case HS_ERR_CUDA: return "HS_ERR_CUDA";
+        case HS_ERR_TIMEOUT: return "HS_ERR_TIMEOUT";
+        case HS_ERR_UNSUPPORTED: return "HS_ERR_UNSUPPORTED";
+    }
+    return "HS_ERR_UNKNOWN";
+}
+
+int64_t hs_packed_matrix_size(int64_t N, int bsz) {
+    if (N <= 0 || bsz <= 0) return 0;
+    const int64_t nb = (N + bsz - 1) / bsz;
+    return nb * (nb + 1) / 2 * (int64_t)bsz * bsz;
+}
+
+int64_t hs_padded_vector_size(int64_t N, int bsz) {
+    if (N <= 0 || bsz <= 0) return 0;
+    return (N + bsz - 1) / bsz * (int64_t)bsz;
+}
+
+hs_status hs_ctx_create(int device, void* stream, hs_ctx* out) {
+    if (!out) {
+        set_error("hs_ctx_create: null output");
+        return HS_ERR_INVALID_ARG;
+    }
+    *out = nullptr;
+    int count = 0;
+    HS_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) {
+        set_error("hs_ctx_create: no CUDA device " + std::to_string(device));
+        return HS_ERR_INVALID_ARG;
+    }
+    HS_CUDA(cudaSetDevice(device));
+    hs_ctx ctx = new hs_ctx_s();
+    ctx->device = device;
+    cudaDeviceProp prop;
+    HS_CUDA(cudaGetDeviceProperties(&prop, device));
+    ctx->num_sms = prop.multiProcessorCount;
+    if (stream) {
+        ctx->stream = static_cast<cudaStream_t>(stream);
+    } else {
+        HS_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        ctx->own_stream = true;
+    }
+    HS_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    HS_CUDA(cudaEventCreateWithFlags(&ctx->ev_a, cudaEventDisableTiming));
+    HS_CUDA(cudaEventCreateWithFlags(&ctx->ev_b, cudaEventDisableTiming));
+    HS_CUDA(cudaMalloc(&ctx->d_info, sizeof(long long)));
+    HS_CUDA(cudaMallocHost(&ctx->h_pinned, 64 * sizeof(double)));
+    set_i64_kernel<<<1, 1, 0, ctx->stream>>>(ctx->d_info, INT64_MAX);
+    HS_CUDA(cudaGetLastError());
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    *out = ctx;
+    return HS_OK;
+}
+
+hs_status hs_ctx_destroy(hs_ctx ctx) {
+    if (!ctx) return HS_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->side) {
+        cudaStreamSynchronize(ctx->side);
+        cudaStreamDestroy(ctx->side);
+    }
+    if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
+    if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->work) cudaFree(ctx->work);
+    if (ctx->d_info) cudaFree(ctx->d_info);
+    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return HS_OK;
+}
+
+hs_status hs_ctx_set_stream(hs_ctx ctx, void* stream) {
+    if (!ctx) {
+        set_error("hs_ctx_set_stream: null context");
+        return HS_ERR_INVALID_ARG;
+    }
+    HS_CUDA(cudaSetDevice(ctx->device));
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->own_stream) {
+        HS_CUDA(cudaStreamDestroy(ctx->stream));
+        ctx->own_stream = false;
+    }
+    if (stream) {
+        ctx->stream = static_cast<cudaStream_t>(stream);
+    } else {
+        HS_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        ctx->own_stream = true;
+    }
+    return HS_OK;
+}
+
+hs_status hs_ctx_set_problem(hs_ctx ctx, int64_t N, int bsz) {
+    HS_API_BEGIN("hs_ctx_set_problem");
+    HS_ARG(N > 0, "N must be positive");
+    HS_ARG(bsz > 0 && bsz <= 1024, "matrixBlockSize must be in [1, 1024]");
+    const int64_t nb = (N + bsz - 1) / bsz;
+    HS_ARG(nb < (1 << 20), "too many block rows");
+    ctx->N = N;
+    ctx->bsz = bsz;
+    ctx->nb = (int)nb;
+    return HS_OK;
+}
+
+hs_status hs_sync(hs_ctx ctx) {
+    if (!ctx) {
+        set_error("hs_sync: null context");
+        return HS_ERR_INVALID_ARG;
+    }
+    HS_CUDA(cudaSetDevice(ctx->device));
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HS_OK;
+}
+
+hs_status hs_ctx_take_info(hs_ctx ctx, int64_t* info) {
+    HS_API_BEGIN("hs_ctx_take_info");
+    long long v = 0;
+    HS_CUDA(cudaMemcpyAsync(&v, ctx->d_info, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    set_i64_kernel<<<1, 1, 0, ctx->stream>>>(ctx->d_info, INT64_MAX);
+    HS_CHECK_LAUNCH("reset info");
+    if (info) *info = (v == INT64_MAX) ? -1 : (int64_t)v;
+    return HS_OK;
+}
+
+// ---------------------------------------------------------------- operators
+hs_status hs_potrf_block(hs_ctx ctx, double* A, int blockID, int blockRow) {
+    HS_API_BEGIN("hs_potrf_block");
+    const int64_t T = total_blocks(ctx->nb);
+    HS_ARG(A != nullptr, "null matrix");
+    HS_ARG(blockID >= 0 && blockID < T, "blockID out of range");
+    HS_ARG(blockRow >= 0 && blockRow < ctx->nb, "blockRow out of range");
+    return launch_potrf(ctx, A, blockID, blockRow, ctx->stream);
+}
+
+hs_status hs_trsm_panel(hs_ctx ctx, double* A, int blockID, int blockRow, int blockStart, int blockCount) {
+    HS_API_BEGIN("hs_trsm_panel");
+    const int64_t T = total_blocks(ctx->nb);
+    HS_ARG(A != nullptr, "null matrix");
+    HS_ARG(blockID >= 0 && blockID < T, "blockID out of range");
+    HS_ARG(blockRow >= 0 && blockRow < ctx->nb, "blockRow out of range");
+    HS_ARG(blockCount >= 0, "negative blockCount");
+    HS_ARG(blockCount == 0 || (blockStart > blockRow && blockStart + blockCount <= ctx->nb),
+           "blocks must lie below the diagonal block and inside the matrix");
+    HS_ARG(blockCount == 0 || (int64_t)blockID + (blockStart - blockRow) + blockCount <= T, "blocks outside storage");
+    return launch_trsm(ctx, A, blockID, blockRow, blockStart, blockCount, ctx->stream);
+}
+
+hs_status hs_syrk_diag(hs_ctx ctx, double* A, int blockID, int blockRow, int blockStart, int blockCount,
+                       int blockCountXY) {
+    HS_API_BEGIN("hs_syrk_diag");
+    HS_ARG(A != nullptr, "null matrix");
+    HS_ARG(blockCountXY == ctx->nb, "blockCountXY does not match the context's N / matrixBlockSize");
+    HS_ARG(blockID >= 0 && blockID < total_blocks(ctx->nb), "blockID out of range");
+    HS_ARG(blockRow >= 0 && blockRow < ctx->nb, "blockRow out of range");
+    HS_ARG(blockCount >= 0, "negative blockCount");
+    HS_ARG(blockCount == 0 || (blockStart > blockRow && blockStart + blockCount <= ctx->nb),
+           "diagonal blocks must lie below blockRow and inside the matrix");
+    return launch_update(ctx, A, blockID, blockRow, blockStart, blockCount, 0, 0, ctx->stream);
+}
+
+hs_status hs_gemm_trailing(hs_ctx ctx, double* A, int blockID, int blockRow, int blockStart, int blockCount,
+                           int blockCountXY) {
+    HS_API_BEGIN("hs_gemm_trailing");
+    HS_ARG(A != nullptr, "null matrix");
+    HS_ARG(blockCountXY == ctx->nb, "blockCountXY does not match the context's N / matrixBlockSize");
+    HS_ARG(blockID >= 0 && blockID < total_blocks(ctx->nb), "blockID out of range");
+    HS_ARG(blockRow >= 0 && blockRow < ctx->nb, "blockRow out of range");
+    HS_ARG(blockCount >= 0, "negative blockCount");
+    HS_ARG(blockCount == 0 || (blockStart >= blockRow + 2 && blockStart + blockCount <= ctx->nb),
+           "rows must lie in [blockRow+2, blockCountXY)");
+    return launch_update(ctx, A, blockID, blockRow, 0, 0, blockStart, blockCount, ctx->stream);
+}
+
+hs_status hs_symv_block(hs_ctx ctx, const double* A, const double* b, double* result, int bi0, int bj0, int nbi,
+                        int nbj, int blockCountXY, int reset) {
+    HS_API_BEGIN("hs_symv_block");
+    HS_ARG(A && b && result, "null pointer");
+    HS_ARG(blockCountXY == ctx->nb, "blockCountXY does not match the context's N / matrixBlockSize");
+    HS_ARG(bi0 >= 0 && nbi >= 0 && bi0 + nbi <= ctx->nb, "row blocks out of range");
+    HS_ARG(bj0 >= 0 && nbj >= 0 && bj0 + nbj <= ctx->nb, "column blocks out of range");
+    return launch_symv(ctx, A, b, result, bi0, bj0, nbi, nbj, reset, nullptr, nullptr, ctx->stream);
+}
+
+hs_status hs_trsv_block(hs_ctx ctx, const double* A, double* b, int blockRow, int blockID, int transposed) {
+    HS_API_BEGIN("hs_trsv_block");
+    HS_ARG(A && b, "null pointer");
+    HS_ARG(blockRow >= 0 && blockRow < ctx->nb, "blockRow out of range");
+    HS_ARG(blockID >= 0 && blockID < total_blocks(ctx->nb), "blockID out of range");
+    return launch_trsv(ctx, A, b, blockRow, blockID, transposed, ctx->stream);
+}
+
+hs_status hs_column_update(hs_ctx ctx, const double* A, double* b, int blockStart, int blockCount, int blockRow,
+                           int blockID, int blockCountXY, int transposed) {
+    HS_API_BEGIN("hs_column_update");
+    HS_ARG(A && b, "null pointer");
+    HS_ARG(blockCountXY == ctx->nb, "blockCountXY does not match the context's N / matrixBlockSize");
+    HS_ARG(blockRow >= 0 && blockRow < ctx->nb, "blockRow out of range");
+    HS_ARG(blockCount >= 0 && blockStart >= 0 && blockStart + blockCount <= ctx->nb, "blocks out of range");
+    if (!transposed) {
+        HS_ARG(blockCount == 0 || blockStart > blockRow, "forward update needs blocks below blockRow");
+        HS_ARG(blockCount == 0 || (int64_t)blockID + (blockStart - blockRow) + blockCount <= total_blocks(ctx->nb),
+               "blocks outside storage");
+    } else {
+        HS_ARG(blockCount == 0 || blockStart + blockCount <= blockRow, "transposed update needs blocks left of blockRow");
+    }
+    return launch_column_update(ctx, A, b, blockStart, blockCount, blockRow, blockID, transposed, ctx->stream);
+}
+
+static hs_status vec_common(hs_ctx ctx, int op, const double* x, const double* y, double alpha, double* out,
+                            int bi0, int nbi, const char* fn) {
+    HS_API_BEGIN(fn);
+    if (!x || !out || (op != 0 && !y)) {
+        set_error(std::string(fn) + ": null pointer");
+        return HS_ERR_INVALID_ARG;
+    }
+    if (bi0 < 0 || nbi < 0 || bi0 + nbi > ctx->nb) {
+        set_error(std::string(fn) + ": blocks out of range");
+        return HS_ERR_INVALID_ARG;
+    }
+    return launch_vec(ctx, op, x, y, alpha, out, (int64_t)bi0 * ctx->bsz, (int64_t)nbi * ctx->bsz, ctx->stream);
+}
+
+hs_status hs_scale_block(hs_ctx ctx, const double* x, double alpha, double* result, int bi0, int nbi) {
+    return vec_common(ctx, 0, x, nullptr, alpha, result, bi0, nbi, "hs_scale_block");
+}
+hs_status hs_add_block(hs_ctx ctx, const double* x, const double* y, double* result, int bi0, int nbi) {
+    return vec_common(ctx, 1, x, y, 0.0, result, bi0, nbi, "hs_add_block");
+}
+hs_status hs_sub_block(hs_ctx ctx, const double* x, const double* y, double* result, int bi0, int nbi) {
+    return vec_common(ctx, 2, x, y, 0.0, result, bi0, nbi, "hs_sub_block");
+}
+hs_status hs_axpy_block(hs_ctx ctx, const double* x, double alpha, const double* y, double* result, int bi0,
+                        int nbi) {
+    return vec_common(ctx, 3, x, y, alpha, result, bi0, nbi, "hs_axpy_block");
+}
+
+hs_status hs_dot_block(hs_ctx ctx, const double* x, const double* y, double* result, int bi0, int nbi) {
+    HS_API_BEGIN("hs_dot_block");
+    HS_ARG(x && y && result, "null pointer");
+    HS_ARG(bi0 >= 0 && nbi >= 0 && bi0 + nbi <= ctx->nb, "blocks out of range");
+    return launch_dot(ctx, x, y, result, (int64_t)bi0 * ctx->bsz, (int64_t)nbi * ctx->bsz, ctx->stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,134 @@
+// hs_internal.cuh — shared internals of the B200 blocked SPD library: the
+// context object, error plumbing and packed-storage index arithmetic.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/hs_b200.h"
+
+struct hs_ctx_s {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int num_sms = 148;
+
+    int64_t N = 0;   // conf::N
+    int bsz = 0;     // conf::matrixBlockSize
+    int nb = 0;      // blockCountXY
+
+    // grow-only device scratch shared by the kernels that need temporaries
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    // grow-only device work vectors of the solver drivers (CG r/d/q, ...)
+    void* work = nullptr;
+    size_t work_bytes = 0;
+
+    // device word holding the smallest failing pivot row (INT64_MAX = none)
+    long long* d_info = nullptr;
+    // pinned host staging for scalars read back by the solver drivers
+    double* h_pinned = nullptr;
+    // second stream + events used by the drivers for lookahead
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+};
+
+namespace hs {
+
+void set_error(const std::string& msg);
+
+hs_status cuda_fail(cudaError_t e, const char* what);
+
+#define HS_CUDA(call)                                                   \
+    do {                                                                \
+        cudaError_t hs_e_ = (call);                                     \
+        if (hs_e_ != cudaSuccess) return ::hs::cuda_fail(hs_e_, #call); \
+    } while (0)
+
+#define HS_CHECK_LAUNCH(name)                                                 \
+    do {                                                                      \
+        cudaError_t hs_e_ = cudaGetLastError();                               \
+        if (hs_e_ != cudaSuccess) return ::hs::cuda_fail(hs_e_, name);        \
+    } while (0)
+
+#define HS_REQUIRE(cond, msg)                                  \
+    do {                                                       \
+        if (!(cond)) {                                         \
+            ::hs::set_error(std::string(__func__) + ": " + (msg)); \
+            return HS_ERR_INVALID_ARG;                         \
+        }                                                      \
+    } while (0)
+
+hs_status require_ctx(hs_ctx ctx, const char* fn);
+// makes sure at least `bytes` of scratch are available (stream-ordered safe:
+// the old buffer is released after a stream sync)
+hs_status ensure_scratch(hs_ctx ctx, size_t bytes);
+hs_status ensure_work(hs_ctx ctx, size_t bytes);
+
+// scratch layout: [0, 32 KB) reduction partials, [32 KB, 48 KB) solver scalars,
+// [56 KB, 64 KB) small constants; matvec partial blocks start at 64 KB
+constexpr size_t kSmallScratch = 64 * 1024;
+constexpr size_t kScalarOffset = 32 * 1024;
+constexpr size_t kConstOffset = 56 * 1024;
+constexpr int kMaxPartials = 4096;
+
+// --------------------------------------------------------- packed storage
+// block (i,j), i >= j: id = i + nb(nb-1)/2 - (nb-j-1)(nb-j)/2
+__host__ __device__ __forceinline__ int64_t block_id(int64_t i, int64_t j, int64_t nb) {
+    return i + nb * (nb - 1) / 2 - (nb - j - 1) * (nb - j) / 2;
+}
+// first block id of block column j
+__host__ __device__ __forceinline__ int64_t column_start(int64_t j, int64_t nb) {
+    return j * nb - j * (j - 1) / 2;
+}
+__host__ __device__ __forceinline__ int64_t total_blocks(int64_t nb) { return nb * (nb + 1) / 2; }
+
+// inverse of block_id: column j such that column_start(j) <= id < column_start(j+1)
+__host__ __device__ __forceinline__ void block_coords(int64_t id, int64_t nb, int* i_out, int* j_out) {
+    int lo = 0, hi = (int)nb - 1;
+    while (lo < hi) {  // largest j with column_start(j) <= id
+        const int mid = (lo + hi + 1) >> 1;
+        if (column_start(mid, nb) <= id) lo = mid; else hi = mid - 1;
+    }
+    *j_out = lo;
+    *i_out = (int)(lo + (id - column_start(lo, nb)));
+}
+
+// inverse triangular number: largest r with r(r+1)/2 <= t
+__host__ __device__ __forceinline__ int tri_root(int64_t t) {
+    int r = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((int64_t)(r + 1) * (r + 2) / 2 <= t) ++r;
+    while ((int64_t)r * (r + 1) / 2 > t) --r;
+    return r;
+}
+
+inline size_t block_elems(const hs_ctx ctx) { return (size_t)ctx->bsz * (size_t)ctx->bsz; }
+
+// ---------------------------------------------------------- kernel entry points
+// (implemented in the k_*.cu files; all stream-ordered on ctx->stream unless a
+// stream is passed)
+hs_status launch_potrf(hs_ctx ctx, double* A, int blockID, int blockRow, cudaStream_t s);
+hs_status launch_trsm(hs_ctx ctx, double* A, int blockID, int blockRow, int blockStart, int blockCount,
+                      cudaStream_t s);
+// SYRK over diag blocks [syrkStart, syrkStart+syrkCount) and GEMM over rows
+// [gemmStart, gemmStart+gemmCount) of the trailing triangle of column blockRow,
+// in one launch (either count may be zero)
+hs_status launch_update(hs_ctx ctx, double* A, int blockID, int blockRow, int syrkStart, int syrkCount,
+                        int gemmStart, int gemmCount, cudaStream_t s);
+hs_status launch_symv(hs_ctx ctx, const double* A, const double* b, double* result, int bi0, int bj0, int nbi,
+                      int nbj, int reset, double* dot_with /*nullable: also dot(result, dot_with) */,
+                      double* dot_out, cudaStream_t s);
+hs_status launch_trsv(hs_ctx ctx, const double* A, double* b, int blockRow, int blockID, int transposed,
+                      cudaStream_t s);
+hs_status launch_column_update(hs_ctx ctx, const double* A, double* b, int blockStart, int blockCount,
+                               int blockRow, int blockID, int transposed, cudaStream_t s);
+hs_status launch_dot(hs_ctx ctx, const double* x, const double* y, double* result, int64_t first, int64_t len,
+                     cudaStream_t s);
+hs_status launch_vec(hs_ctx ctx, int op, const double* x, const double* y, double alpha, double* out,
+                     int64_t first, int64_t len, cudaStream_t s);
+hs_status launch_rbf_assemble(hs_ctx ctx, double* A, const double* X, int d, const double* ell_host, int n_ell,
+                              double sf2, double sn2, cudaStream_t s);
+
+}  // namespace hs

@@ -1,0 +1,469 @@
+// k_factor.cu — kernels of the blocked right-looking Cholesky in FP64:
+// diagonal-block POTRF, panel TRSM and the SYRK/GEMM trailing update.
+//
+// Reference kernels replaced (paths relative to the reference root):
+//   MatrixOperations.cpp:7-191          cholesky / cholesky_GPU / cholesky_optimizedGPU
+//   MatrixMatrixOperations.cpp:5-144    triangularSolve{,_optimizedGPU,_optimizedCPU}
+//   MatrixMatrixOperations.cpp:146-361  symmetricMatrixMatrixDiagonal{,...}
+//   MatrixMatrixOperations.cpp:364-906  matrixMatrixStep{,...}
+//
+// The trailing update is the only O(N^3) part.  For bsz a multiple of 128 it
+// runs on the FP64 tensor pipe (DMMA, mma.sync m8n8k4 f64): 128x128 output
+// tiles per CTA, K streamed in 16-wide slabs through a 4-stage cp.async ring in
+// shared memory, accumulators held in registers and initialised with -C so the
+// result is C - sum_k a_ik b_jk accumulated in k order.  Other block sizes use
+// a scalar fallback with the reference's accumulation order.
+#include "hs_internal.cuh"
+
+namespace hs {
+namespace {
+
+// ------------------------------------------------------------------ POTRF
+// In-shared-memory POTRF of an n x n (n <= 128) sub-block with leading
+// dimension ld: the reference's column-by-column right-looking order
+// (MatrixOperations.cpp:23-57), rows >= valid untouched, strict upper triangle
+// of valid rows zeroed.  A pivot that is not > 0 on a valid row records its
+// global row in *info.
+__global__ void __launch_bounds__(512) potrf_smem_kernel(double* __restrict__ Ablk, int ld, int n, int valid,
+                                                         long long* __restrict__ info, long long row_base) {
+    extern __shared__ double S[];
+    const int sld = n + 1;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int i = e / n, j = e % n;
+        S[i * sld + j] = Ablk[(size_t)i * ld + j];
+    }
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        const double piv = S[k * sld + k];
+        const double s = sqrt(piv);
+        if (threadIdx.x == 0 && k < valid && !(piv > 0.0)) atomicMin(info, row_base + k);
+        for (int i = k + 1 + (int)threadIdx.x; i < valid; i += blockDim.x) S[i * sld + k] = S[i * sld + k] / s;
+        __syncthreads();
+        if (threadIdx.x == 0) S[k * sld + k] = s;
+        // lower trailing part: j in (k, n), i in [j, valid)
+        const int m = n - k - 1;
+        for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+            const int j = k + 1 + e / m;
+            const int i = k + 1 + e % m;
+            if (i >= j && i < valid) S[i * sld + j] = S[i * sld + j] - S[i * sld + k] * S[j * sld + k];
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int i = e / n, j = e % n;
+        if (i >= valid) continue;
+        Ablk[(size_t)i * ld + j] = (j > i) ? 0.0 : S[i * sld + j];
+    }
+    // the reference also writes a_kk = sqrt(a_kk) on padding rows (MatrixOperations.cpp:38-40)
+    for (int k = valid + (int)threadIdx.x; k < n; k += blockDim.x) Ablk[(size_t)k * ld + k] = S[k * sld + k];
+}
+
+// global-memory fallback (bsz > 256): one CTA, same order as the reference
+__global__ void __launch_bounds__(1024) potrf_global_kernel(double* __restrict__ B, int n, int valid,
+                                                            long long* __restrict__ info, long long row_base) {
+    for (int k = 0; k < n; ++k) {
+        const double piv = B[(size_t)k * n + k];
+        const double s = sqrt(piv);
+        if (threadIdx.x == 0 && k < valid && !(piv > 0.0)) atomicMin(info, row_base + k);
+        __syncthreads();
+        for (int i = k + 1 + (int)threadIdx.x; i < valid; i += blockDim.x) B[(size_t)i * n + k] /= s;
+        __syncthreads();
+        if (threadIdx.x == 0) B[(size_t)k * n + k] = s;
+        const int m = n - k - 1;
+        for (int64_t e = threadIdx.x; e < (int64_t)m * m; e += blockDim.x) {
+            const int j = k + 1 + (int)(e / m);
+            const int i = k + 1 + (int)(e % m);
+            if (i >= j && i < valid) B[(size_t)i * n + j] -= B[(size_t)i * n + k] * B[(size_t)j * n + k];
+        }
+        __syncthreads();
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x) {
+        const int i = (int)(e / n), j = (int)(e % n);
+        if (i < valid && j > i) B[e] = 0.0;
+    }
+}
+
+__global__ void zero_tile_kernel(double* __restrict__ P, int ld, int rows, int cols) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < rows * cols; e += gridDim.x * blockDim.x)
+        P[(size_t)(e / cols) * ld + (e % cols)] = 0.0;
+}
+
+// ------------------------------------------------------------------ TRSM
+// B <- B L^-T for slabs of up to 64 rows: each CTA keeps its slab in shared
+// memory and walks the columns in 32-wide chunks: solve the chunk against the
+// chunk's diagonal triangle (column order, divisions as the reference's CPU
+// kernel, MatrixMatrixOperations.cpp:125-139), then subtract the chunk's
+// contribution from the columns to its right, accumulating in k order.
+constexpr int kTrsmRows = 64;
+constexpr int kTrsmCh = 32;
+
+struct TrsmArgs {
+    const double* L;   // triangle (lower), leading dimension ldL
+    int ldL;
+    int n;             // triangle size = columns of B
+    double* A;         // base for B items
+    int ldB;
+    int64_t item0;     // panel mode: first B block id; sub mode: ignored
+    int slabs;         // slabs per B item
+    int rows_last;     // rows in each item (bsz or sub-block rows)
+    int64_t block_elems;  // panel mode: stride between B blocks (elements); 0: single item at A
+};
+
+__global__ void __launch_bounds__(256) trsm_kernel(TrsmArgs a) {
+    extern __shared__ double sm[];
+    const int n = a.n;
+    const int bld = n + 1;
+    double* Bs = sm;                                  // kTrsmRows x (n+1)
+    double* Tc = Bs + kTrsmRows * bld;                // kTrsmCh x (kTrsmCh+1)
+    double* Lp = Tc + kTrsmCh * (kTrsmCh + 1);        // n x (kTrsmCh+1)
+    const int item = blockIdx.x / a.slabs;
+    const int slab = blockIdx.x % a.slabs;
+    double* B = a.A + (a.block_elems ? (size_t)(a.item0 + item) * a.block_elems : 0) + (size_t)slab * kTrsmRows * a.ldB;
+    const int rows = min(kTrsmRows, a.rows_last - slab * kTrsmRows);
+    for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
+        const int r = e / n, c = e % n;
+        Bs[r * bld + c] = B[(size_t)r * a.ldB + c];
+    }
+    const int nch = (n + kTrsmCh - 1) / kTrsmCh;
+    for (int ch = 0; ch < nch; ++ch) {
+        const int k0 = ch * kTrsmCh;
+        const int kn = min(kTrsmCh, n - k0);
+        const int rest = n - (k0 + kn);
+        __syncthreads();
+        for (int e = threadIdx.x; e < kn * kn; e += blockDim.x) {
+            const int i = e / kn, k = e % kn;
+            Tc[i * (kTrsmCh + 1) + k] = a.L[(size_t)(k0 + i) * a.ldL + (k0 + k)];
+        }
+        for (int e = threadIdx.x; e < rest * kn; e += blockDim.x) {
+            const int i = e / kn, k = e % kn;
+            Lp[i * (kTrsmCh + 1) + k] = a.L[(size_t)(k0 + kn + i) * a.ldL + (k0 + k)];
+        }
+        __syncthreads();
+        // chunk solve: one thread per row (rows are independent)
+        for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+            double* row = Bs + r * bld + k0;
+            for (int k = 0; k < kn; ++k) {
+                const double bk = row[k] / Tc[k * (kTrsmCh + 1) + k];
+                row[k] = bk;
+                for (int i = k + 1; i < kn; ++i) row[i] = row[i] - Tc[i * (kTrsmCh + 1) + k] * bk;
+            }
+        }
+        __syncthreads();
+        // trailing columns: b_rc -= sum_k b_rk * L[c][k], k ascending
+        for (int e = threadIdx.x; e < rows * rest; e += blockDim.x) {
+            const int r = e / rest, c = e % rest;
+            double v = Bs[r * bld + k0 + kn + c];
+            const double* bk = Bs + r * bld + k0;
+            const double* lc = Lp + c * (kTrsmCh + 1);
+            for (int k = 0; k < kn; ++k) v = v - lc[k] * bk[k];
+            Bs[r * bld + k0 + kn + c] = v;
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
+        const int r = e / n, c = e % n;
+        B[(size_t)r * a.ldB + c] = Bs[r * bld + c];
+    }
+}
+
+size_t trsm_smem(int n) {
+    return (size_t)(kTrsmRows * (n + 1) + kTrsmCh * (kTrsmCh + 1) + n * (kTrsmCh + 1)) * sizeof(double);
+}
+
+// ------------------------------------------------------------------ DMMA tile
+constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4, SPAD = 20;
+constexpr int kTileSmem = 2 * STAGES * BM * SPAD * (int)sizeof(double);  // 160 KB
+
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// C (128 x 128, ldc) -= A (128 x K, lda) * B (128 x K, ldb)^T; `lower`: only
+// entries with row >= col are written (diagonal tile of a diagonal block).
+__device__ __forceinline__ void dmma_tile(double* __restrict__ C, int64_t ldc, const double* __restrict__ Ag,
+                                          int64_t lda, const double* __restrict__ Bg, int64_t ldb, int K,
+                                          bool lower, double* smem) {
+    double* As = smem;                         // [STAGES][BM][SPAD]
+    double* Bs = smem + STAGES * BM * SPAD;    // [STAGES][BN][SPAD]
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int wm = warp >> 2, wn = warp & 3;
+    const int g = lane >> 2, t = lane & 3;
+
+    double acc[8][4][2];
+#pragma unroll
+    for (int mi = 0; mi < 8; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+            const int r = wm * 64 + mi * 8 + g;
+            const int c = wn * 32 + ni * 8 + 2 * t;
+            const double2 v = *reinterpret_cast<const double2*>(C + (size_t)r * ldc + c);
+            acc[mi][ni][0] = -v.x;
+            acc[mi][ni][1] = -v.y;
+        }
+
+    const int ktiles = K / BK;
+    auto load_stage = [&](int stage, int kt) {
+        const int kc = kt * BK;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = tid + 256 * q;
+            const int row = e >> 3, ch = e & 7;
+            cp_async16(As + (stage * BM + row) * SPAD + ch * 2, Ag + (size_t)row * lda + kc + ch * 2);
+            cp_async16(Bs + (stage * BN + row) * SPAD + ch * 2, Bg + (size_t)row * ldb + kc + ch * 2);
+        }
+    };
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+        if (s < ktiles) load_stage(s, s);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < ktiles; ++kt) {
+        cp_async_wait<STAGES - 2>();
+        __syncthreads();
+        {
+            const int nk = kt + STAGES - 1;
+            if (nk < ktiles) load_stage(nk % STAGES, nk);
+            cp_async_commit();
+        }
+        const double* as = As + (kt % STAGES) * BM * SPAD + (wm * 64 + g) * SPAD + t;
+        const double* bs = Bs + (kt % STAGES) * BN * SPAD + (wn * 32 + g) * SPAD + t;
+#pragma unroll
+        for (int kk = 0; kk < BK / 4; ++kk) {
+            double a[8], b[4];
+#pragma unroll
+            for (int mi = 0; mi < 8; ++mi) a[mi] = as[mi * 8 * SPAD + kk * 4];
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) b[ni] = bs[ni * 8 * SPAD + kk * 4];
+#pragma unroll
+            for (int mi = 0; mi < 8; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma884(acc[mi][ni], a[mi], b[ni]);
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();  // the ring is reused by the CTA's next tile
+#pragma unroll
+    for (int mi = 0; mi < 8; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+            const int r = wm * 64 + mi * 8 + g;
+            const int c = wn * 32 + ni * 8 + 2 * t;
+            double* p = C + (size_t)r * ldc + c;
+            if (!lower || c + 1 <= r) {
+                *reinterpret_cast<double2*>(p) = make_double2(-acc[mi][ni][0], -acc[mi][ni][1]);
+            } else if (c <= r) {
+                p[0] = -acc[mi][ni][0];
+            }
+        }
+}
+
+// One launch for the whole trailing update of block column blockRow: GEMM
+// pairs (r, c), r in [gemmStart, gemmStart+gemmCount), blockRow < c < r,
+// followed by SYRK diagonal blocks j in [syrkStart, syrkStart+syrkCount).
+// CTA = one 128x128 tile of one output block.
+struct UpdateArgs {
+    double* A;
+    int64_t blockID;
+    int blockRow, nb, bsz;
+    int64_t gemmPairs;   // number of GEMM pairs
+    int64_t pairBase;    // triangular offset of gemmStart
+    int syrkStart;
+    int tilesPerSide;
+    int64_t totalPairs;  // gemmPairs + SYRK blocks
+};
+
+__device__ __forceinline__ void decode_pair(const UpdateArgs& a, int64_t pair, int* r, int* c) {
+    if (pair < a.gemmPairs) {
+        const int64_t tt = pair + a.pairBase;
+        const int u = tri_root(tt);
+        *r = a.blockRow + 1 + (u + 1);
+        *c = a.blockRow + 1 + (int)(tt - (int64_t)u * (u + 1) / 2);
+    } else {
+        *r = *c = a.syrkStart + (int)(pair - a.gemmPairs);
+    }
+}
+
+__global__ void __launch_bounds__(256, 1) update_dmma_kernel(UpdateArgs a) {
+    extern __shared__ __align__(16) double smem[];
+    const int tps = a.tilesPerSide;
+    const int64_t idx = blockIdx.x;
+    const int tile = (int)(idx % (tps * tps));
+    const int64_t pair = idx / (tps * tps);
+    int r, c;
+    decode_pair(a, pair, &r, &c);
+    const int ti = tile / tps, tj = tile % tps;
+    if (r == c && tj > ti) return;
+    const size_t bb = (size_t)a.bsz * a.bsz;
+    double* C = a.A + (size_t)block_id(r, c, a.nb) * bb + (size_t)ti * BM * a.bsz + (size_t)tj * BN;
+    const double* Ag = a.A + (size_t)(a.blockID + (r - a.blockRow)) * bb + (size_t)ti * BM * a.bsz;
+    const double* Bg = a.A + (size_t)(a.blockID + (c - a.blockRow)) * bb + (size_t)tj * BN * a.bsz;
+    dmma_tile(C, a.bsz, Ag, a.bsz, Bg, a.bsz, a.bsz, r == c && ti == tj, smem);
+}
+
+// single-tile form used inside the blocked POTRF of a 256 block
+__global__ void __launch_bounds__(256, 1) tile_update_kernel(double* C, int ldc, const double* Ag, const double* Bg,
+                                                             int ld, int K, int lower) {
+    extern __shared__ __align__(16) double smem[];
+    dmma_tile(C, ldc, Ag, ld, Bg, ld, K, lower != 0, smem);
+}
+
+// scalar fallback (any bsz): one thread per output element; SYRK follows
+// MatrixMatrixOperations.cpp:346-355 (value -= c_ik c_jk in k order), GEMM
+// follows :893-900 (sum from zero, subtracted once)
+__global__ void update_scalar_kernel(UpdateArgs a) {
+    const int64_t bb = (int64_t)a.bsz * a.bsz;
+    const int64_t pair = blockIdx.y + (int64_t)blockIdx.z * 65535;
+    if (pair >= a.totalPairs) return;
+    int r, c;
+    decode_pair(a, pair, &r, &c);
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= bb) return;
+    const int i = (int)(e / a.bsz), j = (int)(e % a.bsz);
+    double* C = a.A + block_id(r, c, a.nb) * bb;
+    const double* Rk = a.A + (a.blockID + (r - a.blockRow)) * bb;
+    const double* Ck = a.A + (a.blockID + (c - a.blockRow)) * bb;
+    if (r == c) {
+        if (i < j) return;
+        double v = C[(size_t)i * a.bsz + j];
+        for (int k = 0; k < a.bsz; ++k) v = v - Rk[(size_t)i * a.bsz + k] * Rk[(size_t)j * a.bsz + k];
+        C[(size_t)i * a.bsz + j] = v;
+    } else {
+        double v = 0.0;
+        for (int k = 0; k < a.bsz; ++k) v += Rk[(size_t)i * a.bsz + k] * Ck[(size_t)j * a.bsz + k];
+        C[(size_t)i * a.bsz + j] -= v;
+    }
+}
+
+bool attrs_done[64] = {};
+hs_status set_attrs() {
+    int dev = 0;
+    HS_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && attrs_done[dev]) return HS_OK;
+    HS_CUDA(cudaFuncSetAttribute(update_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
+    HS_CUDA(cudaFuncSetAttribute(tile_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
+    HS_CUDA(cudaFuncSetAttribute(trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem(256)));
+    HS_CUDA(cudaFuncSetAttribute(potrf_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(128 * 129 * sizeof(double))));
+    if (dev >= 0 && dev < 64) attrs_done[dev] = true;
+    return HS_OK;
+}
+
+hs_status launch_trsm_args(const TrsmArgs& ta, int items, cudaStream_t s) {
+    HS_REQUIRE(ta.n <= 256, "TRSM supports triangles up to 256");
+    const size_t smem = trsm_smem(ta.n);
+    trsm_kernel<<<items * ta.slabs, 256, smem, s>>>(ta);
+    HS_CHECK_LAUNCH("trsm");
+    return HS_OK;
+}
+
+hs_status potrf_small(hs_ctx ctx, double* blk, int ld, int n, int valid, long long row_base, cudaStream_t s) {
+    const size_t smem = (size_t)n * (n + 1) * sizeof(double);
+    potrf_smem_kernel<<<1, 512, smem, s>>>(blk, ld, n, valid, ctx->d_info, row_base);
+    HS_CHECK_LAUNCH("potrf");
+    return HS_OK;
+}
+
+}  // namespace
+
+hs_status launch_potrf(hs_ctx ctx, double* A, int blockID, int blockRow, cudaStream_t s) {
+    hs_status st = set_attrs();
+    if (st != HS_OK) return st;
+    const int bsz = ctx->bsz;
+    double* blk = A + (size_t)blockID * bsz * bsz;
+    const long long row_base = (long long)blockRow * bsz;
+    const int64_t rem = ctx->N - row_base;
+    const int valid = rem <= 0 ? 0 : (rem < bsz ? (int)rem : bsz);
+    if (bsz <= 128) return potrf_small(ctx, blk, bsz, bsz, valid, row_base, s);
+    if (bsz == 256) {
+        // [A11 . ; A21 A22] with 128 x 128 quadrants: POTRF(A11), A21 <- A21 L11^-T,
+        // A22 -= A21 A21^T (lower, DMMA tile), POTRF(A22), zero the upper-right quadrant
+        const int n1 = 128, n2 = 128;
+        st = potrf_small(ctx, blk, bsz, n1, min(valid, n1), row_base, s);
+        if (st != HS_OK) return st;
+        double* A21 = blk + (size_t)n1 * bsz;
+        double* A22 = A21 + n1;
+        if (valid > n1) {
+            TrsmArgs ta{blk, bsz, n1, A21, bsz, 0, n2 / kTrsmRows, n2, 0};
+            st = launch_trsm_args(ta, 1, s);
+            if (st != HS_OK) return st;
+            tile_update_kernel<<<1, 256, kTileSmem, s>>>(A22, bsz, A21, A21, bsz, n1, 1);
+            HS_CHECK_LAUNCH("potrf syrk");
+            st = potrf_small(ctx, A22, bsz, n2, valid - n1, row_base + n1, s);
+        } else {
+            // rows >= 128 are padding; the reference still writes sqrt(0) on their diagonal
+            st = potrf_small(ctx, A22, bsz, n2, 0, row_base + n1, s);
+        }
+        if (st != HS_OK) return st;
+        zero_tile_kernel<<<16, 256, 0, s>>>(blk + n1, bsz, min(valid, n1), n2);
+        HS_CHECK_LAUNCH("potrf zero");
+        return HS_OK;
+    }
+    potrf_global_kernel<<<1, 1024, 0, s>>>(blk, bsz, valid, ctx->d_info, row_base);
+    HS_CHECK_LAUNCH("potrf");
+    return HS_OK;
+}
+
+hs_status launch_trsm(hs_ctx ctx, double* A, int blockID, int blockRow, int blockStart, int blockCount,
+                      cudaStream_t s) {
+    if (blockCount <= 0) return HS_OK;
+    hs_status st = set_attrs();
+    if (st != HS_OK) return st;
+    const int bsz = ctx->bsz;
+    HS_REQUIRE(bsz <= 256, "TRSM supports matrixBlockSize up to 256");
+    const size_t bb = (size_t)bsz * bsz;
+    TrsmArgs ta{A + (size_t)blockID * bb, bsz, bsz, A, bsz, (int64_t)blockID + (blockStart - blockRow),
+                (bsz + kTrsmRows - 1) / kTrsmRows, bsz, (int64_t)bb};
+    return launch_trsm_args(ta, blockCount, s);
+}
+
+hs_status launch_update(hs_ctx ctx, double* A, int blockID, int blockRow, int syrkStart, int syrkCount,
+                        int gemmStart, int gemmCount, cudaStream_t s) {
+    hs_status st = set_attrs();
+    if (st != HS_OK) return st;
+    UpdateArgs a{};
+    a.A = A;
+    a.blockID = blockID;
+    a.blockRow = blockRow;
+    a.nb = ctx->nb;
+    a.bsz = ctx->bsz;
+    int64_t pairs = 0;
+    if (gemmCount > 0) {
+        // rows r' = r - blockRow - 1 in [g0, g0 + gemmCount) own r' pairs each
+        const int64_t g0 = gemmStart - blockRow - 1;
+        const int64_t g1 = g0 + gemmCount;
+        a.pairBase = g0 * (g0 - 1) / 2;
+        pairs = g1 * (g1 - 1) / 2 - a.pairBase;
+    }
+    a.gemmPairs = pairs;
+    a.syrkStart = syrkStart;
+    const int64_t total = pairs + (syrkCount > 0 ? syrkCount : 0);
+    if (total <= 0) return HS_OK;
+    a.totalPairs = total;
+    if (ctx->bsz % BM == 0) {
+        a.tilesPerSide = ctx->bsz / BM;
+        const int64_t grid = total * a.tilesPerSide * a.tilesPerSide;
+        HS_REQUIRE(grid < (1LL << 31), "trailing update too large for one launch");
+        update_dmma_kernel<<<(unsigned)grid, 256, kTileSmem, s>>>(a);
+        HS_CHECK_LAUNCH("update_dmma");
+    } else {
+        const int64_t bb = (int64_t)ctx->bsz * ctx->bsz;
+        dim3 grid((unsigned)((bb + 255) / 256), (unsigned)(total < 65535 ? total : 65535),
+                  (unsigned)((total + 65534) / 65535));
+        update_scalar_kernel<<<grid, 256, 0, s>>>(a);
+        HS_CHECK_LAUNCH("update_scalar");
+    }
+    return HS_OK;
+}
+
+}  // namespace hs

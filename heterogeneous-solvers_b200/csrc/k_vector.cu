@@ -1,0 +1,416 @@
+// k_vector.cu — vector operations, deterministic dot product, symmetric block
+// matvec, single-block triangular solve and block-column update.
+//
+// Reference kernels replaced (paths relative to the reference root):
+//   VectorOperations.cpp:6-82     scale/add/sub/scaleAndAdd
+//   VectorOperations.cpp:84-185   scalarProduct + sumFinalScalarProduct
+//   MatrixVectorOperations.cpp:8-280    matrixVectorBlock{,_GPU,_CPU}
+//   MatrixVectorOperations.cpp:282-335  triangularSolveBlockVector
+//   MatrixVectorOperations.cpp:337-377  matrixVectorColumnUpdate
+//
+// The symmetric matvec streams every stored block of the touched sub-rectangle
+// exactly once and applies it both as A_ij (row part, for output block row i)
+// and as A_ij^T (column part, for output block row j).  Each part lands in its
+// own slot of a partial buffer indexed by the sub-rectangle position, and a
+// second kernel sums the slots of an output block row in a fixed order, so the
+// result is bitwise reproducible without atomics.
+#include "hs_internal.cuh"
+
+namespace hs {
+namespace {
+
+constexpr int kThreads = 256;
+
+// ------------------------------------------------------------------ elementwise
+template <int OP>
+__global__ void vec_kernel(const double* __restrict__ x, const double* __restrict__ y, double alpha,
+                           double* __restrict__ out, int64_t first, int64_t len) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < len; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = first + t;
+        double v;
+        if (OP == 0) v = x[i] * alpha;          // scaleVectorBlock          VectorOperations.cpp:19
+        else if (OP == 1) v = x[i] + y[i];      // addVectorBlock            :39
+        else if (OP == 2) v = x[i] - y[i];      // subVectorBlock            :58
+        else v = x[i] + y[i] * alpha;           // scaleAndAddVectorBlock    :78
+        out[i] = v;
+    }
+}
+
+// ------------------------------------------------------------------ dot
+constexpr int kDotBlocks = 512;
+
+__device__ __forceinline__ double block_reduce_sum(double v, double* sh) {
+    // fixed-order tree: warp butterfly, then the 8 warp sums in order
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += sh[i];
+    return s;  // valid in thread 0
+}
+
+__global__ void dot_stage1(const double* __restrict__ x, const double* __restrict__ y, int64_t first, int64_t len,
+                           double* __restrict__ partial) {
+    __shared__ double sh[32];
+    double v = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < len; t += (int64_t)gridDim.x * blockDim.x)
+        v += x[first + t] * y[first + t];
+    const double s = block_reduce_sum(v, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+__global__ void dot_stage2(const double* __restrict__ partial, int n, double* __restrict__ out) {
+    __shared__ double sh[32];
+    double v = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v += partial[i];
+    const double s = block_reduce_sum(v, sh);
+    if (threadIdx.x == 0) out[0] = s;
+}
+
+// ------------------------------------------------------------------ block apply
+// One CTA applies one bsz x bsz block M (row major) to a vector:
+//   rowOut[r] = sum_c M[r][c] * xc[c]      (row part)
+//   colOut[c] = sum_r M[r][c] * xr[r]      (column part)
+// Fast path for bsz in {128, 256}: 8 warps own bsz/8 consecutive rows each,
+// lane l owns bsz/32 consecutive columns loaded with 16-byte streaming loads.
+template <int BSZ>
+struct BlockApply {
+    static constexpr int CPL = BSZ / 32;  // columns per lane
+    static constexpr int RPW = BSZ / 8;   // rows per warp
+
+    // sums a per-lane vector s[RPW] across the warp so that lane l ends with
+    // the total for row (l % RPW); fixed butterfly order
+    __device__ static __forceinline__ double reduce_rows(double (&s)[RPW], int lane) {
+        if (RPW == 16) {
+#pragma unroll
+            for (int i = 0; i < RPW; ++i) s[i] += __shfl_xor_sync(0xffffffffu, s[i], 16);
+        }
+#pragma unroll
+        for (int step = RPW / 2; step >= 1; step >>= 1) {
+            const bool upper = (lane & step) != 0;
+#pragma unroll
+            for (int i = 0; i < step; ++i) {
+                const double send = upper ? s[i] : s[i + step];
+                const double keep = upper ? s[i + step] : s[i];
+                s[i] = keep + __shfl_xor_sync(0xffffffffu, send, step);
+            }
+        }
+        return s[0];
+    }
+
+    // mode bit 1: row part, bit 2: column part.  colOut / rowOut get "=" semantics.
+    __device__ static void run(const double* __restrict__ M, const double* __restrict__ xc,
+                               const double* __restrict__ xr, double* __restrict__ rowOut,
+                               double* __restrict__ colOut, int mode, double* smem /* 8*BSZ */) {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int r0 = warp * RPW;
+        const int c0 = lane * CPL;
+        double xcv[CPL], z[CPL], s[RPW];
+#pragma unroll
+        for (int j = 0; j < CPL; ++j) {
+            xcv[j] = (mode & 1) ? xc[c0 + j] : 0.0;
+            z[j] = 0.0;
+        }
+        const double xrl = ((mode & 2) && lane < RPW) ? xr[r0 + lane] : 0.0;
+#pragma unroll
+        for (int rr = 0; rr < RPW; ++rr) {
+            const double2* rowp = reinterpret_cast<const double2*>(M + (size_t)(r0 + rr) * BSZ + c0);
+            double a[CPL];
+#pragma unroll
+            for (int j = 0; j < CPL / 2; ++j) {
+                const double2 v = __ldcs(rowp + j);
+                a[2 * j] = v.x;
+                a[2 * j + 1] = v.y;
+            }
+            double acc = 0.0;
+#pragma unroll
+            for (int j = 0; j < CPL; ++j) acc = fma(a[j], xcv[j], acc);
+            s[rr] = acc;
+            const double xv = __shfl_sync(0xffffffffu, xrl, rr);
+#pragma unroll
+            for (int j = 0; j < CPL; ++j) z[j] = fma(a[j], xv, z[j]);
+        }
+        if (mode & 1) {
+            const double rs = reduce_rows(s, lane);
+            if (lane < RPW) rowOut[r0 + lane] = rs;
+        }
+        if (mode & 2) {
+#pragma unroll
+            for (int j = 0; j < CPL; ++j) smem[warp * BSZ + c0 + j] = z[j];
+            __syncthreads();
+            for (int c = threadIdx.x; c < BSZ; c += blockDim.x) {
+                double v = 0.0;
+#pragma unroll
+                for (int w = 0; w < 8; ++w) v += smem[w * BSZ + c];
+                colOut[c] = v;
+            }
+        }
+    }
+};
+
+// generic path for any bsz: thread per row (row part), thread per column (column part)
+__device__ void block_apply_generic(const double* __restrict__ M, int bsz, const double* __restrict__ xc,
+                                    const double* __restrict__ xr, double* __restrict__ rowOut,
+                                    double* __restrict__ colOut, int mode) {
+    if (mode & 1)
+        for (int r = threadIdx.x; r < bsz; r += blockDim.x) {
+            double v = 0.0;
+            for (int c = 0; c < bsz; ++c) v += M[(size_t)r * bsz + c] * xc[c];
+            rowOut[r] = v;
+        }
+    if (mode & 2)
+        for (int c = threadIdx.x; c < bsz; c += blockDim.x) {
+            double v = 0.0;
+            for (int r = 0; r < bsz; ++r) v += M[(size_t)r * bsz + c] * xr[r];
+            colOut[c] = v;
+        }
+}
+
+template <int BSZ>
+__device__ __forceinline__ void block_apply(const double* M, int bsz, const double* xc, const double* xr,
+                                            double* rowOut, double* colOut, int mode, double* smem) {
+    if constexpr (BSZ > 0) BlockApply<BSZ>::run(M, xc, xr, rowOut, colOut, mode, smem);
+    else block_apply_generic(M, bsz, xc, xr, rowOut, colOut, mode);
+}
+
+// ------------------------------------------------------------------ SYMV phase 1
+// grid: one CTA per sub-rectangle position (I, J); the CTA owning the stored
+// block computes every part of it the rectangle needs.
+template <int BSZ>
+__global__ void __launch_bounds__(kThreads) symv_partials(const double* __restrict__ A, const double* __restrict__ b,
+                                                          double* __restrict__ P, int bsz, int nb, int bi0,
+                                                          int bj0, int nbi, int nbj) {
+    __shared__ double smem[(BSZ > 0 ? 8 * BSZ : 1)];
+    const int64_t pos = blockIdx.x;
+    const int I = bi0 + (int)(pos / nbj);
+    const int J = bj0 + (int)(pos % nbj);
+    const auto inRect = [&](int i, int j) { return i >= bi0 && i < bi0 + nbi && j >= bj0 && j < bj0 + nbj; };
+    const size_t bb = (size_t)bsz * bsz;
+    if (J <= I) {
+        // stored block (I, J): row part for (I, J); column part for (J, I) if also requested
+        const double* M = A + (size_t)block_id(I, J, nb) * bb;
+        int mode = 1;
+        if (I != J && inRect(J, I)) mode |= 2;
+        double* rowOut = P + ((size_t)(I - bi0) * nbj + (J - bj0)) * bsz;
+        double* colOut = (mode & 2) ? P + ((size_t)(J - bi0) * nbj + (I - bj0)) * bsz : nullptr;
+        block_apply<BSZ>(M, bsz, b + (size_t)J * bsz, b + (size_t)I * bsz, rowOut, colOut, mode, smem);
+    } else if (!inRect(J, I)) {
+        // stored block (J, I) seen only transposed: column part for (I, J)
+        const double* M = A + (size_t)block_id(J, I, nb) * bb;
+        double* colOut = P + ((size_t)(I - bi0) * nbj + (J - bj0)) * bsz;
+        block_apply<BSZ>(M, bsz, nullptr, b + (size_t)J * bsz, nullptr, colOut, 2, smem);
+    }
+}
+
+// ------------------------------------------------------------------ SYMV phase 2
+// result[i] = (reset ? 0 : result[i]) + sum_J P[I][J][r] (J ascending); optional
+// fused per-CTA partial of result . w
+__global__ void __launch_bounds__(kThreads) symv_reduce(const double* __restrict__ P, double* __restrict__ result,
+                                                        int bsz, int bi0, int nbi, int nbj, int reset,
+                                                        const double* __restrict__ w, double* __restrict__ wpart) {
+    __shared__ double sh[32];
+    const int64_t rows = (int64_t)nbi * bsz;
+    double prod = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < rows; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t I = t / bsz;
+        const int r = (int)(t % bsz);
+        const int64_t i = (int64_t)bi0 * bsz + t;
+        double v = reset ? 0.0 : result[i];
+        const double* p = P + (size_t)I * nbj * bsz + r;
+        for (int J = 0; J < nbj; ++J) v += p[(size_t)J * bsz];
+        result[i] = v;
+        if (w) prod += v * w[i];
+    }
+    if (w) {
+        const double s = block_reduce_sum(prod, sh);
+        if (threadIdx.x == 0) wpart[blockIdx.x] = s;
+    }
+}
+
+// ------------------------------------------------------------------ column update
+template <int BSZ>
+__global__ void __launch_bounds__(kThreads) column_update_kernel(const double* __restrict__ A, double* __restrict__ b,
+                                                                 int bsz, int nb, int blockStart, int blockRow,
+                                                                 int64_t blockID, int transposed) {
+    __shared__ double smem[(BSZ > 0 ? 8 * BSZ : 1)];
+    __shared__ double out[(BSZ > 0 ? BSZ : 1024)];
+    const int g = blockIdx.x;
+    const size_t bb = (size_t)bsz * bsz;
+    const double* b0 = b + (size_t)blockRow * bsz;
+    double* bi = b + (size_t)(blockStart + g) * bsz;
+    if (!transposed) {
+        const double* M = A + (size_t)(blockID + (blockStart - blockRow + g)) * bb;
+        block_apply<BSZ>(M, bsz, b0, nullptr, out, nullptr, 1, smem);
+    } else {
+        const double* M = A + (size_t)block_id(blockRow, blockStart + g, nb) * bb;
+        block_apply<BSZ>(M, bsz, nullptr, b0, nullptr, out, 2, smem);
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < bsz; r += blockDim.x) bi[r] -= out[r];
+}
+
+// ------------------------------------------------------------------ TRSV
+// Blocked substitution on one diagonal block: 32-row chunks, warp 0 solves the
+// chunk's triangle (column oriented, as the reference), all warps then apply
+// the chunk to the remaining rows.  Entries with global index >= N are neither
+// written nor used (MatrixVectorOperations.cpp:303-330).
+constexpr int kCh = 32;
+
+__global__ void __launch_bounds__(kThreads) trsv_kernel(const double* __restrict__ A, double* __restrict__ b,
+                                                        int bsz, int64_t N, int blockRow, int64_t blockID,
+                                                        int transposed, double* __restrict__ vbuf /* unused */) {
+    extern __shared__ double sh[];
+    double* v = sh;                 // bsz entries of b
+    double* T = sh + bsz;           // kCh x (kCh+1) triangle
+    const double* L = A + (size_t)blockID * bsz * bsz;
+    double* bb = b + (size_t)blockRow * bsz;
+    const int64_t base = (int64_t)blockRow * bsz;
+    const int valid = (N - base) < (int64_t)bsz ? (int)(N - base) : bsz;  // rows < N in this block
+    for (int i = threadIdx.x; i < bsz; i += blockDim.x) v[i] = bb[i];
+    __syncthreads();
+    const int nch = (bsz + kCh - 1) / kCh;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int cc = 0; cc < nch; ++cc) {
+        const int c = transposed ? nch - 1 - cc : cc;
+        const int k0 = c * kCh;
+        const int kn = min(kCh, bsz - k0);
+        // stage the chunk triangle: T[i][k] = L[k0+i][k0+k] (lower) or L[k0+k][k0+i] (upper view)
+        for (int e = threadIdx.x; e < kn * kn; e += blockDim.x) {
+            const int i = e / kn, k = e % kn;
+            T[i * (kCh + 1) + k] = transposed ? L[(size_t)(k0 + k) * bsz + (k0 + i)] : L[(size_t)(k0 + i) * bsz + (k0 + k)];
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double x = lane < kn ? v[k0 + lane] : 0.0;
+            for (int s = 0; s < kn; ++s) {
+                const int k = transposed ? kn - 1 - s : s;
+                const double diag = T[k * (kCh + 1) + k];
+                const double bk = __shfl_sync(0xffffffffu, x, k) / diag;
+                if (k0 + k < valid) {
+                    if (lane == k) x = bk;
+                    const bool below = transposed ? (lane < k) : (lane > k && lane < kn);
+                    if (below) x = x - T[lane * (kCh + 1) + k] * bk;
+                }
+            }
+            if (lane < kn && k0 + lane < valid) v[k0 + lane] = x;
+        }
+        __syncthreads();
+        // apply the solved chunk to the rows not yet solved
+        const int lo = transposed ? 0 : k0 + kn;
+        const int hi = transposed ? k0 : bsz;
+        for (int r = lo + (int)threadIdx.x; r < hi; r += blockDim.x) {
+            if (r >= valid) continue;
+            double acc = v[r];
+            for (int k = 0; k < kn; ++k) {
+                const int kk = transposed ? kn - 1 - k : k;
+                if (k0 + kk >= valid) continue;
+                const double lv = transposed ? L[(size_t)(k0 + kk) * bsz + r] : L[(size_t)r * bsz + (k0 + kk)];
+                acc = acc - lv * v[k0 + kk];
+            }
+            v[r] = acc;
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < valid; i += blockDim.x) bb[i] = v[i];
+}
+
+int dot_blocks(int64_t len) {
+    int64_t g = (len + 2047) / 2048;
+    if (g < 1) g = 1;
+    if (g > kDotBlocks) g = kDotBlocks;
+    return (int)g;
+}
+
+}  // namespace
+
+hs_status launch_dot(hs_ctx ctx, const double* x, const double* y, double* result, int64_t first, int64_t len,
+                     cudaStream_t s) {
+    hs_status st = ensure_scratch(ctx, kSmallScratch);
+    if (st != HS_OK) return st;
+    double* partial = static_cast<double*>(ctx->scratch);
+    const int g = dot_blocks(len);
+    dot_stage1<<<g, kThreads, 0, s>>>(x, y, first, len, partial);
+    dot_stage2<<<1, kThreads, 0, s>>>(partial, g, result);
+    HS_CHECK_LAUNCH("dot");
+    return HS_OK;
+}
+
+hs_status launch_symv(hs_ctx ctx, const double* A, const double* b, double* result, int bi0, int bj0, int nbi,
+                      int nbj, int reset, double* dot_with, double* dot_out, cudaStream_t s) {
+    if (nbi <= 0) return HS_OK;
+    const int bsz = ctx->bsz;
+    const size_t pbytes = (size_t)nbi * (size_t)(nbj > 0 ? nbj : 1) * bsz * sizeof(double);
+    hs_status st = ensure_scratch(ctx, kSmallScratch + pbytes);
+    if (st != HS_OK) return st;
+    double* small = static_cast<double*>(ctx->scratch);
+    double* P = reinterpret_cast<double*>(static_cast<char*>(ctx->scratch) + kSmallScratch);
+    if (nbj > 0) {
+        const int64_t grid = (int64_t)nbi * nbj;
+        if (bsz == 256)
+            symv_partials<256><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
+        else if (bsz == 128)
+            symv_partials<128><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
+        else
+            symv_partials<0><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
+        HS_CHECK_LAUNCH("symv_partials");
+    }
+    const int64_t rows = (int64_t)nbi * bsz;
+    int64_t rg64 = (rows + kThreads - 1) / kThreads;
+    if (rg64 > kMaxPartials) rg64 = kMaxPartials;
+    const unsigned rg = (unsigned)rg64;
+    double* wpart = small;
+    symv_reduce<<<rg, kThreads, 0, s>>>(P, result, bsz, bi0, nbi, nbj, reset, dot_with, wpart);
+    if (dot_with) dot_stage2<<<1, kThreads, 0, s>>>(wpart, (int)rg, dot_out);
+    HS_CHECK_LAUNCH("symv_reduce");
+    return HS_OK;
+}
+
+hs_status launch_column_update(hs_ctx ctx, const double* A, double* b, int blockStart, int blockCount, int blockRow,
+                               int blockID, int transposed, cudaStream_t s) {
+    if (blockCount <= 0) return HS_OK;
+    const int bsz = ctx->bsz;
+    HS_REQUIRE(bsz <= 1024, "matrixBlockSize > 1024 is not supported by the column update");
+    if (bsz == 256)
+        column_update_kernel<256><<<blockCount, kThreads, 0, s>>>(A, b, bsz, ctx->nb, blockStart, blockRow, blockID,
+                                                                  transposed);
+    else if (bsz == 128)
+        column_update_kernel<128><<<blockCount, kThreads, 0, s>>>(A, b, bsz, ctx->nb, blockStart, blockRow, blockID,
+                                                                  transposed);
+    else
+        column_update_kernel<0><<<blockCount, kThreads, 0, s>>>(A, b, bsz, ctx->nb, blockStart, blockRow, blockID,
+                                                                transposed);
+    HS_CHECK_LAUNCH("column_update");
+    return HS_OK;
+}
+
+hs_status launch_trsv(hs_ctx ctx, const double* A, double* b, int blockRow, int blockID, int transposed,
+                      cudaStream_t s) {
+    const int bsz = ctx->bsz;
+    const size_t smem = (size_t)(bsz + kCh * (kCh + 1)) * sizeof(double);
+    HS_REQUIRE(smem <= 200 * 1024, "matrixBlockSize too large for the block triangular solve");
+    if (smem > 48 * 1024) HS_CUDA(cudaFuncSetAttribute(trsv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)smem));
+    trsv_kernel<<<1, kThreads, smem, s>>>(A, b, bsz, ctx->N, blockRow, blockID, transposed, nullptr);
+    HS_CHECK_LAUNCH("trsv");
+    return HS_OK;
+}
+
+hs_status launch_vec(hs_ctx ctx, int op, const double* x, const double* y, double alpha, double* out,
+                     int64_t first, int64_t len, cudaStream_t s) {
+    if (len <= 0) return HS_OK;
+    int64_t g = (len + kThreads - 1) / kThreads;
+    if (g > 8 * (int64_t)ctx->num_sms) g = 8 * (int64_t)ctx->num_sms;
+    switch (op) {
+        case 0: vec_kernel<0><<<(unsigned)g, kThreads, 0, s>>>(x, y, alpha, out, first, len); break;
+        case 1: vec_kernel<1><<<(unsigned)g, kThreads, 0, s>>>(x, y, alpha, out, first, len); break;
+        case 2: vec_kernel<2><<<(unsigned)g, kThreads, 0, s>>>(x, y, alpha, out, first, len); break;
+        default: vec_kernel<3><<<(unsigned)g, kThreads, 0, s>>>(x, y, alpha, out, first, len); break;
+    }
+    HS_CHECK_LAUNCH("vector op");
+    return HS_OK;
+}
+
+}  // namespace hs

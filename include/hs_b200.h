@@ -1,0 +1,175 @@
+/*
+ * hs_b200.h — C ABI of the B200-native blocked SPD solve path.
+ *
+ * Drop-in for TimThuering/Heterogeneous-Solvers' blocked SPD path for Gaussian-
+ * process kernel matrices.  Every entry point below names the reference
+ * interface it replaces (file:line relative to the reference's root).  The
+ * reference passes a sycl::queue plus globals conf::N / conf::matrixBlockSize
+ * (src/utility/Configuration.hpp:21-118); here a context carries the CUDA
+ * device, stream and the problem size, and every call takes the same integer
+ * block arguments, in the same order, as the reference kernel it replaces.
+ *
+ * Matrix storage (src/dataStructures/SymmetricMatrix.hpp:9-54): the lower
+ * block triangle of an N x N symmetric matrix in nb = ceil(N/bsz) blocks per
+ * side, T = nb(nb+1)/2 blocks of bsz*bsz doubles, enumerated column by column;
+ * block (i,j), i >= j, has id i + nb(nb-1)/2 - (nb-j-1)(nb-j)/2; row-major
+ * inside a block; diagonal blocks hold both triangles; padding is zero.
+ * Vectors (src/dataStructures/RightHandSide.hpp:12-30) are nb*bsz doubles,
+ * zero padded.
+ *
+ * Conventions: unless a parameter says "host", pointers are device pointers.
+ * All work is ordered on the context's stream; hs_sync() waits for it.
+ * Operator-level calls (hs_potrf_block ... hs_dot_block) launch and return.
+ * No C++ exception crosses this boundary: every call returns an hs_status and
+ * hs_last_error() gives the message of the calling thread's last failure.
+ */
+#ifndef HS_B200_H
+#define HS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HS_B200_ABI_VERSION 1
+
+typedef enum hs_status {
+    HS_OK = 0,
+    HS_ERR_INVALID_ARG = 1,       /* reference: std::invalid_argument / std::runtime_error */
+    HS_ERR_OOM = 2,               /* reference: "Error during GPU memory allocation" (CG.cpp:231-233) */
+    HS_ERR_NOT_SPD = 3,           /* reference: silent NaN (MatrixOperations.cpp:24) */
+    HS_ERR_NO_CONVERGENCE = 4,    /* CG reached iMax (CG.cpp:78) */
+    HS_ERR_REFINEMENT_STALLED = 5,/* mixed precision: refinement stopped improving */
+    HS_ERR_CUDA = 6,
+    HS_ERR_TIMEOUT = 7,           /* a bounded device-side wait gave up */
+    HS_ERR_UNSUPPORTED = 8
+} hs_status;
+
+typedef struct hs_ctx_s* hs_ctx;
+
+/* ------------------------------------------------------------------ context */
+int hs_abi_version(void);
+const char* hs_last_error(void);
+const char* hs_status_string(hs_status s);
+
+/* Create a context on `device`.  `stream` is a cudaStream_t (NULL: the context
+ * creates and owns a non-blocking stream). */
+hs_status hs_ctx_create(int device, void* stream, hs_ctx* out);
+hs_status hs_ctx_destroy(hs_ctx ctx);
+hs_status hs_ctx_set_stream(hs_ctx ctx, void* stream);
+/* conf::N and conf::matrixBlockSize (Configuration.hpp:22, :33).  Sets nb. */
+hs_status hs_ctx_set_problem(hs_ctx ctx, int64_t N, int matrixBlockSize);
+hs_status hs_sync(hs_ctx ctx);
+/* number of doubles of the packed matrix / of a padded vector for (N, bsz):
+ * SymmetricMatrix.cpp:11-19, RightHandSide.cpp:8-15 */
+int64_t hs_packed_matrix_size(int64_t N, int matrixBlockSize);
+int64_t hs_padded_vector_size(int64_t N, int matrixBlockSize);
+
+/* ------------------------------------------------------------------ operators */
+/* MatrixOperations::cholesky / cholesky_GPU / cholesky_optimizedGPU
+ * (src/kernel/MatrixOperations.hpp:23,39,55; MatrixOperations.cpp:7-191):
+ * in-place POTRF of diagonal block blockID (= block row blockRow); rows with
+ * global index >= N untouched; the upper triangle becomes zero.  A non-positive
+ * pivot is recorded in the context (see hs_ctx_take_info). */
+hs_status hs_potrf_block(hs_ctx ctx, double* A, int blockID, int blockRow);
+/* Read (and reset) the context's pivot record: *info = -1 when every POTRF since
+ * the last call saw positive pivots, else the smallest failing global row.
+ * Synchronises the stream. */
+hs_status hs_ctx_take_info(hs_ctx ctx, int64_t* info);
+
+/* MatrixMatrixOperations::triangularSolve{,_optimizedGPU,_optimizedCPU}
+ * (MatrixMatrixOperations.hpp:29,53,77; .cpp:5-144): B <- B L^-T for the blocks
+ * at rows blockStart .. blockStart+blockCount-1 of block column blockRow. */
+hs_status hs_trsm_panel(hs_ctx ctx, double* A, int blockID, int blockRow, int blockStart, int blockCount);
+
+/* MatrixMatrixOperations::symmetricMatrixMatrixDiagonal{,_optimizedGPU,_optimizedCPU}
+ * (MatrixMatrixOperations.hpp:98,121,145; .cpp:146-361): A_jj <- A_jj - L_jk L_jk^T,
+ * lower triangle only, for diagonal blocks j in [blockStart, blockStart+blockCount). */
+hs_status hs_syrk_diag(hs_ctx ctx, double* A, int blockID, int blockRow, int blockStart, int blockCount,
+                       int blockCountXY);
+
+/* MatrixMatrixOperations::matrixMatrixStep{,_optimizedGPU,2,3,_optimizedCPU,2}
+ * (MatrixMatrixOperations.hpp:168-290; .cpp:364-906): A_rc <- A_rc - L_rk L_ck^T
+ * for blockRow < c < r, r in [blockStart, blockStart+blockCount). */
+hs_status hs_gemm_trailing(hs_ctx ctx, double* A, int blockID, int blockRow, int blockStart, int blockCount,
+                           int blockCountXY);
+
+/* MatrixVectorOperations::matrixVectorBlock{,_GPU,_CPU}
+ * (MatrixVectorOperations.hpp:27,47,67; .cpp:8-280): result[rows of block rows
+ * blockStart_i ..] (reset ? = : +=) A_sub b over the block sub-rectangle
+ * [blockStart_i, +blockCount_i) x [blockStart_j, +blockCount_j) of the full
+ * symmetric matrix.  Each stored block is read once and applied as A_ij and
+ * A_ij^T (deterministic two-phase reduction; uses context scratch). */
+hs_status hs_symv_block(hs_ctx ctx, const double* A, const double* b, double* result, int blockStart_i,
+                        int blockStart_j, int blockCount_i, int blockCount_j, int blockCountXY, int reset);
+
+/* MatrixVectorOperations::triangularSolveBlockVector (MatrixVectorOperations.hpp:81;
+ * .cpp:282-335): b_blockRow <- L^-1 b_blockRow (transposed: L^-T). */
+hs_status hs_trsv_block(hs_ctx ctx, const double* A, double* b, int blockRow, int blockID, int transposed);
+
+/* MatrixVectorOperations::matrixVectorColumnUpdate (MatrixVectorOperations.hpp:99;
+ * .cpp:337-377): b_i -= A_{i,blockRow} b_blockRow for i in [blockStart, +blockCount)
+ * (transposed: b_i -= A_{blockRow,i}^T b_blockRow). */
+hs_status hs_column_update(hs_ctx ctx, const double* A, double* b, int blockStart, int blockCount, int blockRow,
+                           int blockID, int blockCountXY, int transposed);
+
+/* VectorOperations (VectorOperations.hpp:21-95; .cpp:6-185) on rows of block rows
+ * [blockStart_i, blockStart_i + blockCount_i): */
+hs_status hs_scale_block(hs_ctx ctx, const double* x, double alpha, double* result, int blockStart_i,
+                         int blockCount_i);                                  /* scaleVectorBlock        :6   */
+hs_status hs_add_block(hs_ctx ctx, const double* x, const double* y, double* result, int blockStart_i,
+                       int blockCount_i);                                    /* addVectorBlock          :25  */
+hs_status hs_sub_block(hs_ctx ctx, const double* x, const double* y, double* result, int blockStart_i,
+                       int blockCount_i);                                    /* subVectorBlock          :45  */
+hs_status hs_axpy_block(hs_ctx ctx, const double* x, double alpha, const double* y, double* result,
+                        int blockStart_i, int blockCount_i);                 /* scaleAndAddVectorBlock  :64  */
+/* scalarProduct + sumFinalScalarProduct (:84-185): result[0] (device) = x.y,
+ * deterministic two-stage tree reduction (uses context scratch). */
+hs_status hs_dot_block(hs_ctx ctx, const double* x, const double* y, double* result, int blockStart_i,
+                       int blockCount_i);
+
+/* ------------------------------------------------------------------ solvers */
+/* MatrixGenerator::generateSPDMatrix (src/utility/MatrixGenerator.cpp:73-162), its
+ * per-entry formula generalised from the 1-D sliding window to X (N x d, row
+ * major, device): K_ij = sf2 * exp(-0.5/l^2 * |x_i - x_j|^2) + sn2 [i == j].
+ * `ell` (host) holds 1 (isotropic) or d (ARD) lengthscales.  Writes all T
+ * blocks, padding as zero. */
+hs_status hs_rbf_assemble(hs_ctx ctx, double* A, const double* X, int d, const double* ell, int n_ell,
+                          double sf2, double sn2);
+
+/* Cholesky::solve_heterogeneous with the whole matrix on the GPU
+ * (src/solver/cholesky/Cholesky.cpp:413-493): A (packed, device) is overwritten
+ * by L.  *info (host, may be NULL) = -1 on success, else the global row of the
+ * first non-positive pivot (then HS_ERR_NOT_SPD). */
+hs_status hs_cholesky_factor(hs_ctx ctx, double* A, int64_t* info);
+
+/* TriangularSystemSolver::solve (TriangularSystemSolver.cpp:15-105): b <- L^-T L^-1 b
+ * in place (device). */
+hs_status hs_cholesky_solve(hs_ctx ctx, const double* L, double* b);
+
+/* CG::solveHeterogeneous with the whole matrix on the GPU (src/solver/cg/CG.cpp:38-163):
+ * x (device) starts at zero; stop when delta_new <= epsilon^2 delta_0 or after iMax
+ * iterations; true residual every 50 iterations (CG.cpp:95-101).  Outputs are host
+ * pointers and may be NULL.  Returns HS_ERR_NO_CONVERGENCE when iMax is reached. */
+hs_status hs_cg_solve(hs_ctx ctx, const double* A, const double* b, double* x, double epsilon, int64_t iMax,
+                      int64_t* iterations, double* delta_new, double* delta_zero);
+
+/* End-to-end GP solve through host buffers, the path of GaussianProcess::start's
+ * solve (src/gaussianProcess/GaussianProcess.cpp:20-40) and main.cpp:201-249:
+ * X_host (N x d), y_host (N) -> RBF assembly -> factor + solve (algorithm 0) or
+ * CG (algorithm 1) -> x_host (N).  Device buffers are allocated inside. */
+typedef struct hs_solve_report {
+    int64_t info;            /* factor: -1 or failing row */
+    int64_t iterations;      /* CG iterations (algorithm 1) */
+    double assemble_ms, factor_ms, solve_ms, total_ms;
+} hs_solve_report;
+hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_host, int d, const double* ell,
+                           int n_ell, double sf2, double sn2, int algorithm, double epsilon, int64_t iMax,
+                           double* x_host, hs_solve_report* report);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

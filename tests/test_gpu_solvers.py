@@ -1,0 +1,198 @@
+"""GPU suite: solver-level parity of the CUDA path with the CPU oracle (the
+reference's CPU-path arithmetic) and with dense LAPACK, on seeded inputs."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import oracle_lib as ol
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(N, d, seed=11):
+    rng = np.random.default_rng(seed)
+    X = rng.random((N, d))
+    y = np.sin(X.sum(axis=1)) + 0.1 * rng.standard_normal(N)
+    return X, y
+
+
+def _padded(y, N, bsz):
+    b = np.zeros(-(-N // bsz) * bsz)
+    b[:N] = y
+    return b
+
+
+def _assemble_gpu(hs, ctx, X, bsz, ell, sf2, sn2):
+    N = X.shape[0]
+    ctx.set_problem(N, bsz)
+    A = torch.zeros(hs.packed_size(N, bsz), dtype=torch.float64, device="cuda:0")
+    A.fill_(np.nan)  # every entry, padding included, must be written
+    hs.MatrixGenerator.assemble(ctx, A, X, ell, sf2, sn2)
+    ctx.sync()
+    return A
+
+
+@pytest.mark.parametrize("N,bsz,d,ell", [
+    (300, 128, 8, 0.5), (1000, 128, 8, 0.5), (700, 256, 16, 1.0), (100, 20, 8, 1.0), (45, 9, 3, 0.7),
+    (530, 256, 8, [0.2, 0.5, 1.0, 2.0, 0.3, 0.7, 1.5, 1.1]), (77, 6, 3, [0.5, 1.0, 2.0]),
+])
+def test_rbf_assembly_matches_oracle(hs, ctx, N, bsz, d, ell):
+    X, _ = _problem(N, d)
+    A = _assemble_gpu(hs, ctx, X, bsz, ell, 1.1, 1e-2).cpu().numpy()
+    ref = ol.rbf_assemble(X, bsz, ell, 1.1, 1e-2)
+    assert np.isfinite(A).all()
+    assert np.max(np.abs(A - ref)) <= 1e-14  # FMA contraction and exp may differ from the host by a few ulp
+
+
+@pytest.mark.parametrize("N,bsz", [(1000, 128), (1024, 256), (700, 256), (600, 256), (130, 20), (47, 6)])
+def test_cholesky_factor_matches_oracle(hs, ctx, N, bsz):
+    X, _ = _problem(N, 8)
+    A = _assemble_gpu(hs, ctx, X, bsz, 0.5, 1.0, 1e-2)
+    info = ctypes.c_int64(-2)
+    hs._lib.call("hs_cholesky_factor", ctx.handle, ctypes.c_void_p(A.data_ptr()), ctypes.byref(info))
+    assert info.value == -1
+    L = A.cpu().numpy()
+    ref = ol.cholesky(ol.rbf_assemble(X, bsz, 0.5, 1.0, 1e-2), N, bsz)
+    rel = np.linalg.norm(L - ref) / np.linalg.norm(ref)
+    assert rel <= 1e-12, rel
+    # upper triangles of diagonal blocks are zero, padding untouched (zero)
+    nb = -(-N // bsz)
+    for k in range(nb):
+        blk = L[ol.block_id(k, k, nb) * bsz * bsz:][: bsz * bsz].reshape(bsz, bsz)
+        assert not np.triu(blk, 1).any()
+    # against dense LAPACK
+    K = ol.packed_to_dense(ol.rbf_assemble(X, bsz, 0.5, 1.0, 1e-2), N, bsz)
+    Ld = ol.packed_to_dense(L, N, bsz, lower_only=True)
+    assert np.linalg.norm(Ld - np.linalg.cholesky(K)) / np.linalg.norm(Ld) <= 1e-12
+
+
+@pytest.mark.parametrize("N,bsz", [(1000, 128), (700, 256), (130, 20)])
+def test_triangular_solve_matches_oracle(hs, ctx, N, bsz):
+    X, y = _problem(N, 8)
+    K = ol.rbf_assemble(X, bsz, 0.5, 1.0, 1e-2)
+    L = ol.cholesky(K, N, bsz)
+    b = _padded(y, N, bsz)
+    ref = ol.triangular_solve(L, b, N, bsz)
+    ctx.set_problem(N, bsz)
+    Lg = torch.from_numpy(L).cuda()
+    bg = torch.from_numpy(b).cuda()
+    hs._lib.call("hs_cholesky_solve", ctx.handle, ctypes.c_void_p(Lg.data_ptr()), ctypes.c_void_p(bg.data_ptr()))
+    x = bg.cpu().numpy()
+    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) <= 1e-12
+    assert not x[N:].any()
+
+
+@pytest.mark.parametrize("N,bsz", [(1000, 128), (700, 256), (130, 20)])
+def test_cg_matches_oracle(hs, ctx, N, bsz):
+    X, y = _problem(N, 8)
+    K = ol.rbf_assemble(X, bsz, 0.5, 1.0, 1e-1)
+    b = _padded(y, N, bsz)
+    x_ref, it_ref, _, _ = ol.cg(K, b, N, bsz, 1e-10, 20000)
+    A = hs.SymmetricMatrix(N, bsz)
+    A.matrixData.copy_(torch.from_numpy(K))
+    rhs = hs.RightHandSide(N, bsz)
+    rhs.rightHandSideData.copy_(torch.from_numpy(b))
+    cg = hs.CG(A, rhs, ctx).solveHeterogeneous(epsilon=1e-10, iMax=20000)
+    assert abs(cg.iterations - it_ref) <= 1, (cg.iterations, it_ref)
+    x = cg.x.numpy()
+    assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) <= 1e-8
+
+
+def test_symv_full_matches_dense(hs, ctx):
+    N, bsz = 2000, 128
+    X, y = _problem(N, 8)
+    K = ol.rbf_assemble(X, bsz, 0.5, 1.0, 1e-2)
+    b = _padded(y, N, bsz)
+    ctx.set_problem(N, bsz)
+    Kg, bg = torch.from_numpy(K).cuda(), torch.from_numpy(b).cuda()
+    out = torch.full_like(bg, np.nan)
+    nb = -(-N // bsz)
+    hs.MatrixVectorOperations.matrixVectorBlock(ctx, Kg, bg, out, 0, 0, nb, nb, nb)
+    dense = ol.packed_to_dense(K, N, bsz) @ y
+    res = out.cpu().numpy()
+    assert np.allclose(res[:N], dense, rtol=1e-13, atol=1e-12)
+    # bitwise reproducible (fixed reduction order)
+    out2 = torch.empty_like(out)
+    hs.MatrixVectorOperations.matrixVectorBlock(ctx, Kg, bg, out2, 0, 0, nb, nb, nb)
+    assert torch.equal(out, out2)
+
+
+def test_config1_parity_with_oracle(hs, ctx):
+    """N=4096, d=8, l=0.5, sf2=1, sn2=1e-2, bsz=128: factor, solve and CG
+    against the oracle's CPU path (relative error <= 1e-12; CG iterations +-1)."""
+    import importlib
+    wl = importlib.import_module("hs_b200.workloads")
+    cfg = wl.CONFIGS["c1_n4096"]
+    N, bsz = cfg["N"], cfg["bsz"]
+    X, y = wl.gp_inputs(N, cfg["d"], cfg["seed"])
+    K = ol.rbf_assemble(X, bsz, cfg["lengthscale"], cfg["sf2"], cfg["sn2"])
+    L_ref = ol.cholesky(K, N, bsz)
+    b = _padded(y, N, bsz)
+    x_ref = ol.triangular_solve(L_ref, b, N, bsz)
+    A = _assemble_gpu(hs, ctx, X, bsz, cfg["lengthscale"], cfg["sf2"], cfg["sn2"])
+    assert np.max(np.abs(A.cpu().numpy() - K)) <= 1e-14
+    info = ctypes.c_int64(-2)
+    hs._lib.call("hs_cholesky_factor", ctx.handle, ctypes.c_void_p(A.data_ptr()), ctypes.byref(info))
+    L = A.cpu().numpy()
+    assert np.linalg.norm(L - L_ref) / np.linalg.norm(L_ref) <= 1e-12
+    bg = torch.from_numpy(b).cuda()
+    hs._lib.call("hs_cholesky_solve", ctx.handle, ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(bg.data_ptr()))
+    x = bg.cpu().numpy()
+    assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) <= 1e-12
+    # CG on the same system
+    x_cg_ref, it_ref, _, _ = ol.cg(K, b, N, bsz, cfg["eps"], 100000)
+    Ah = hs.SymmetricMatrix(N, bsz)
+    Ah.matrixData.copy_(torch.from_numpy(K))
+    rhs = hs.RightHandSide(N, bsz)
+    rhs.rightHandSideData.copy_(torch.from_numpy(b))
+    cg = hs.CG(Ah, rhs, ctx).solveHeterogeneous(epsilon=cfg["eps"], iMax=100000)
+    assert abs(cg.iterations - it_ref) <= 1, (cg.iterations, it_ref)
+    assert np.linalg.norm(cg.x.numpy() - x_cg_ref) / np.linalg.norm(x_cg_ref) <= 1e-8
+
+
+def test_not_spd_reports_first_failing_row(hs, ctx):
+    N, bsz = 300, 128
+    X, _ = _problem(N, 4)
+    K = ol.rbf_assemble(X, bsz, 0.5, 1.0, 1e-2)
+    nb = -(-N // bsz)
+    # make row 150 indefinite: a_{150,150} = -1
+    blk = ol.block_id(1, 1, nb) * bsz * bsz
+    K[blk + 22 * bsz + 22] = -1.0
+    ctx.set_problem(N, bsz)
+    Kg = torch.from_numpy(K).cuda()
+    with pytest.raises(hs.NotSPDError):
+        A = hs.SymmetricMatrix(N, bsz, device="cuda:0")
+        A.matrixData.copy_(Kg)
+        hs.Cholesky(A, ctx).solve_heterogeneous()
+    info = ctypes.c_int64(-2)
+    st = hs._lib.load().hs_cholesky_factor(ctx.handle, ctypes.c_void_p(Kg.data_ptr()), ctypes.byref(info))
+    assert st == 3 and info.value == 150
+
+
+def test_invalid_arguments_are_rejected(hs, ctx):
+    ctx.set_problem(20, 4)
+    A = torch.zeros(hs.packed_size(20, 4), dtype=torch.float64, device="cuda:0")
+    with pytest.raises(hs.HSError, match="blockID out of range"):
+        hs.MatrixOperations.cholesky(ctx, A, 15, 0)
+    with pytest.raises(hs.HSError, match="rows must lie"):
+        hs.MatrixMatrixOperations.matrixMatrixStep(ctx, A, 0, 0, 1, 3, 5)
+    with pytest.raises(hs.HSError, match="blockCountXY"):
+        hs.MatrixMatrixOperations.symmetricMatrixMatrixDiagonal(ctx, A, 0, 0, 1, 4, 6)
+    with pytest.raises(TypeError):
+        hs.MatrixOperations.cholesky(ctx, A.float(), 0, 0)
+
+
+def test_gp_solve_host_end_to_end(hs, ctx):
+    N, bsz, d = 900, 128, 8
+    X, y = _problem(N, d)
+    ctx.set_problem(N, bsz)
+    x, rep = hs.gp_solve_host(ctx, X, y, 0.5, 1.0, 1e-2, algorithm="cholesky")
+    K = ol.rbf_assemble(X, bsz, 0.5, 1.0, 1e-2)
+    x_ref = ol.triangular_solve(ol.cholesky(K, N, bsz), _padded(y, N, bsz), N, bsz)[:N]
+    assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) <= 1e-12
+    assert rep.info == -1 and rep.total_ms > 0
+    x2, rep2 = hs.gp_solve_host(ctx, X, y, 0.5, 1.0, 1e-2, algorithm="cg", epsilon=1e-12)
+    assert np.linalg.norm(x2 - x_ref) / np.linalg.norm(x_ref) <= 1e-7
+    assert rep2.iterations > 0
