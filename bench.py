@@ -1,0 +1,377 @@
+#!/usr/bin/env python3
+"""Benchmark of the blocked SPD solve path for GP kernel matrices.
+
+One step = RBF assembly of the packed kernel matrix from device-resident
+inputs, the FP64 blocked Cholesky factor and the forward/back substitution,
+at N = 131072, d = 16, l = 1, sf2 = 1, sn2 = 1e-2, matrix_bsz = 256 (68.85 GB
+packed FP64 matrix, larger than L2, so no flush is needed between steps).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line on rank 0.  `value` is whole-job throughput in solves/s
+(N independent replicas under torchrun: the path does not shard).  `e2e` is
+the same metric through hs_gp_solve_host with pinned host buffers.  The
+reference arm (--impl reference) times the CPU restatement of the reference's
+CPU path (or its sources compiled through oracle/ref_build.py when present) on
+a bounded sample and extrapolates by N^3.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+METRIC = "N=131072 SPD solve time: FP64 vs mixed-prec+IR at equal error; LML+grad time"
+WORKLOAD = "c2_n131072"
+
+
+def load_package():
+    import importlib.util
+    if "hs_b200" in sys.modules:
+        return sys.modules["hs_b200"]
+    pkg = ROOT / "heterogeneous-solvers_b200"
+    spec = importlib.util.spec_from_file_location("hs_b200", pkg / "__init__.py", submodule_search_locations=[str(pkg)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["hs_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=None, help="override N (smaller runs for profiling)")
+    ap.add_argument("--cg-iters", type=int, default=30, help="CG iterations timed for the matvec roofline")
+    ap.add_argument("--cpu-sample-n", type=int, default=8192)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(self.rows),
+                "power_w_max": max((float(r[3]) for r in self.rows if r[3].replace(".", "").isdigit()), default=None)}
+
+
+# ------------------------------------------------------------------ CPU baseline
+def cpu_reference_sample(n_sample, threads):
+    """Times the reference's CPU path (factor + solve) at N = n_sample with the
+    full configuration otherwise; returns (seconds, kind)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import numpy as np
+    hs = load_package()
+    wl = __import__("hs_b200.workloads", fromlist=["CONFIGS"])
+    cfg = wl.CONFIGS[WORKLOAD]
+    X, y = wl.gp_inputs(n_sample, cfg["d"], cfg["seed"])
+    ref_bin = ROOT / "oracle" / "_ref" / "ref_cholesky"
+    if ref_bin.exists():
+        # the reference's own sources (oracle/ref_build.py): prints the factor+solve seconds
+        inp = ROOT / "oracle" / "_ref" / "bench_inputs.bin"
+        np.concatenate([X.ravel(), y]).tofile(inp)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close")
+        out = subprocess.run([str(ref_bin), str(inp), str(n_sample), str(cfg["d"]), str(cfg["bsz"]),
+                              repr(cfg["lengthscale"]), repr(cfg["sn2"])], capture_output=True, text=True, env=env,
+                             check=True)
+        return float(json.loads(out.stdout.strip().splitlines()[-1])["seconds"]), "reference"
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import oracle_lib as ol
+    bsz = cfg["bsz"]
+    K = ol.rbf_assemble(X, bsz, cfg["lengthscale"], cfg["sf2"], cfg["sn2"])
+    b = np.zeros(hs.padded_size(n_sample, bsz))
+    b[:n_sample] = y
+    t0 = time.perf_counter()
+    L = ol.cholesky(K, n_sample, bsz)
+    ol.triangular_solve(L, b, n_sample, bsz)
+    return time.perf_counter() - t0, "port"
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    N = args.n or 131072
+    scale = (N / args.cpu_sample_n) ** 3
+    for _ in range(args.warmup):
+        cpu_reference_sample(args.cpu_sample_n, threads)
+    times = []
+    kind = "port"
+    for _ in range(args.steps):
+        t, kind = cpu_reference_sample(args.cpu_sample_n, threads)
+        times.append(t * scale)
+    t_full = sum(times) / len(times)
+    value = 1.0 / t_full
+    sample = (f"FP64 factor+solve at N={args.cpu_sample_n} (same d, l, sn2, bsz), "
+              f"extrapolated by (N/{args.cpu_sample_n})^3 to N={N}")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_full * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{WORKLOAD}: RBF assembly + FP64 blocked Cholesky factor + solve", "N": N,
+                       "d": 16, "bsz": 256},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def measure_fp64_peak(torch, device):
+    """cuBLAS DGEMM 8192^3 (torch.matmul float64), best of 5: the FP64 peak."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=device)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    hs = load_package()
+    wl = __import__("hs_b200.workloads", fromlist=["CONFIGS"])
+    device = local_rank
+    torch.cuda.set_device(device)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", device))
+
+    cfg = dict(wl.CONFIGS[WORKLOAD])
+    N = args.n or cfg["N"]
+    bsz, d = cfg["bsz"], cfg["d"]
+    X, y = wl.gp_inputs(N, d, cfg["seed"] + rank)
+    ctx = hs.Context(device=device)
+    ctx.set_problem(N, bsz)
+    n_pad = hs.padded_size(N, bsz)
+    Xd = torch.from_numpy(X).to(f"cuda:{device}")
+    bd = torch.zeros(n_pad, dtype=torch.float64, device=f"cuda:{device}")
+    bd[:N] = torch.from_numpy(y).to(f"cuda:{device}")
+    A = torch.empty(hs.packed_size(N, bsz), dtype=torch.float64, device=f"cuda:{device}")
+    xd = torch.empty_like(bd)
+    lib = hs._lib.load()
+    import ctypes
+
+    def P(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    info = ctypes.c_int64()
+
+    def step():
+        hs.MatrixGenerator.assemble(ctx, A, Xd, cfg["lengthscale"], cfg["sf2"], cfg["sn2"])
+        hs._lib.check(lib.hs_cholesky_factor(ctx.handle, P(A), ctypes.byref(info)))
+        xd.copy_(bd)
+        hs._lib.check(lib.hs_cholesky_solve(ctx.handle, P(A), P(xd)))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    fp64_peak = measure_fp64_peak(torch, device)
+
+    # ---------------- timed region (device-resident inputs)
+    sampler = ClockSampler(device)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ctx.reset_profile()
+    ctx.set_profiling(True)
+    launches0 = ctx.launch_count()
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = ctx.launch_count() - launches0
+    ctx.set_profiling(False)
+    t_ms = e0.elapsed_time(e1)
+    prof = {k: ctx.read_profile(k) for k in ("update", "potrf", "trsm", "assemble", "trsv", "colupd")}
+    t_max = torch.tensor([t_ms], dtype=torch.float64, device=f"cuda:{device}")
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    t_max_ms = float(t_max.item())
+    if world > 1:
+        dist.barrier()
+    ms_per_step = t_max_ms / args.steps
+    value = world * args.steps / (t_max_ms * 1e-3)
+
+    # ---------------- size-independent checks on the last step's result
+    x_host = xd[:N].cpu().numpy()
+    hs.MatrixGenerator.assemble(ctx, A, Xd, cfg["lengthscale"], cfg["sf2"], cfg["sn2"])
+    r = torch.empty_like(bd)
+    nb = ctx.blockCountXY
+    hs.MatrixVectorOperations.matrixVectorBlock(ctx, A, xd, r, 0, 0, nb, nb, nb)
+    res = torch.linalg.norm(r - bd).item()
+    blocks = A.view(-1, bsz * bsz)
+    diag_ids = torch.tensor([hs.block_id(k, k, nb) for k in range(nb)], device=A.device)
+    sq_all = (blocks * blocks).sum(dim=1)
+    k_fro = float(torch.sqrt(2.0 * sq_all.sum() - sq_all[diag_ids].sum()).item())
+    backward_error = res / (k_fro * float(np.linalg.norm(x_host)) + float(np.linalg.norm(y)))
+
+    # ---------------- CG matvec roofline: a bounded number of CG iterations on K
+    cg_info = None
+    if args.cg_iters > 0:
+        x_cg = torch.empty_like(bd)
+        it, dn, d0 = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+        ctx.reset_profile()
+        ctx.set_profiling(True)
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record()
+        st = lib.hs_cg_solve(ctx.handle, P(A), P(bd), P(x_cg), cfg["eps"], args.cg_iters, ctypes.byref(it),
+                             ctypes.byref(dn), ctypes.byref(d0))
+        c1.record()
+        torch.cuda.synchronize()
+        ctx.set_profiling(False)
+        symv = ctx.read_profile("symv")
+        cg_info = {"iterations": it.value, "ms_per_iteration": c0.elapsed_time(c1) / max(1, it.value),
+                   "rel_residual_sq": dn.value / d0.value if d0.value else None, "status": int(st),
+                   "matvec_ms": symv["ms"] / max(1, symv["launches"]),
+                   "matvec_gbs": symv["bytes"] / (symv["ms"] * 1e-3) / 1e9 if symv["ms"] else None,
+                   "matvec_frac_of_hbm": None}
+        del x_cg
+
+    # ---------------- e2e through the host-buffer API
+    e2e = None
+    if not args.no_e2e:
+        del A
+        torch.cuda.empty_cache()
+        Xh = torch.from_numpy(X).pin_memory()
+        yh = torch.from_numpy(y).pin_memory()
+        xh = torch.empty(N, dtype=torch.float64).pin_memory()
+        hs.gp_solve_host(ctx, Xh, yh, cfg["lengthscale"], cfg["sf2"], cfg["sn2"], out=xh)  # warm-up
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            _, rep = hs.gp_solve_host(ctx, Xh, yh, cfg["lengthscale"], cfg["sf2"], cfg["sn2"], out=xh)
+        torch.cuda.synchronize()
+        t_e2e = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=f"cuda:{device}")
+        if world > 1:
+            dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * args.steps / float(t_e2e.item()), "unit": "solves/s",
+               "h2d_bytes_per_step": int(X.nbytes + y.nbytes), "d2h_bytes_per_step": int(N * 8),
+               "report_ms": {"assemble+h2d": rep.assemble_ms, "factor": rep.factor_ms, "solve": rep.solve_ms,
+                             "total": rep.total_ms}}
+
+    # ---------------- roofline of the dominant kernel (FP64 trailing update)
+    upd = prof["update"]
+    achieved = upd["flops"] / (upd["ms"] * 1e-3) / 1e12 if upd["ms"] else None
+    traffic = None
+    tfile = ROOT / "profiles" / "update_dmma_traffic.json"
+    if tfile.exists() and upd["launches"]:
+        tj = json.loads(tfile.read_text())
+        traffic = tj["dram_bytes_per_flop"] * upd["flops"] / upd["launches"]
+    peaks = {}
+    pf = ROOT / "MEASURED_PEAKS.json"
+    if pf.exists():
+        peaks = json.loads(pf.read_text())
+    if cg_info and peaks.get("hbm_gbs") and cg_info["matvec_gbs"]:
+        cg_info["matvec_frac_of_hbm"] = cg_info["matvec_gbs"] / peaks["hbm_gbs"]
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        t_s, kind = cpu_reference_sample(args.cpu_sample_n, threads)
+        t_full = t_s * (N / args.cpu_sample_n) ** 3
+        cpu = {"value": 1.0 / t_full, "unit": "solves/s", "cores": threads, "kind": kind,
+               "sample": f"FP64 factor+solve at N={args.cpu_sample_n}, extrapolated by N^3 to N={N}",
+               "sample_seconds": t_s}
+
+    if rank == 0:
+        phases = {k: {"launches": v["launches"], "ms_per_step": v["ms"] / args.steps,
+                      "tflops": v["flops"] / (v["ms"] * 1e-3) / 1e12 if v["ms"] else None}
+                  for k, v in prof.items()}
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": f"synthetic: X~U[0,1]^({N}x{d}) seed {cfg['seed']}+rank, y=sin(sum_k x_k)+N(0,0.1^2)",
+            "config": {"workload": f"{WORKLOAD}: RBF assembly + FP64 blocked Cholesky factor + forward/back solve",
+                       "N": N, "d": d, "bsz": bsz, "lengthscale": cfg["lengthscale"], "sf2": cfg["sf2"],
+                       "sn2": cfg["sn2"], "l2": "inputs larger than L2 (packed K 68.85 GB at N=131072)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp64_peak if achieved else None, "traffic": traffic,
+                         "kernel": "update_dmma_kernel (FP64 SYRK+GEMM trailing update, DMMA)",
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is absent from "
+                                        "MEASURED_PEAKS.json)"},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+            "phases": phases, "factor_tflops_whole": (N ** 3 / 3) / (ms_per_step * 1e-3) / 1e12,
+            "backward_error": backward_error, "cg": cg_info,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

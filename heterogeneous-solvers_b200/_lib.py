@@ -40,6 +40,14 @@ class SolveReport(ctypes.Structure):
                 ("factor_ms", ctypes.c_double), ("solve_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
 
 
+class KernelProfile(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_int64), ("ms", ctypes.c_double), ("flops", ctypes.c_double),
+                ("bytes", ctypes.c_double)]
+
+
+# hs_kernel_id
+KERNEL_IDS = {"update": 0, "potrf": 1, "trsm": 2, "symv": 3, "trsv": 4, "colupd": 5, "assemble": 6, "vector": 7}
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _I64 = ctypes.c_int64
@@ -57,6 +65,11 @@ SIGNATURES = {
     "hs_sync": [_P],
     "hs_packed_matrix_size": [_I64, _I],
     "hs_padded_vector_size": [_I64, _I],
+    "hs_ctx_set_profiling": [_P, _I],
+    "hs_ctx_read_profile": [_P, _I, ctypes.POINTER(KernelProfile)],
+    "hs_ctx_reset_profile": [_P],
+    "hs_ctx_launch_count": [_P],
+    "hs_ctx_set_reference_order": [_P, _I],
     "hs_potrf_block": [_P, _P, _I, _I],
     "hs_ctx_take_info": [_P, ctypes.POINTER(_I64)],
     "hs_trsm_panel": [_P, _P, _I, _I, _I, _I],
@@ -77,7 +90,7 @@ SIGNATURES = {
     "hs_gp_solve_host": [_P, _P, _P, _I, _P, _I, _D, _D, _I, _D, _I64, _P, ctypes.POINTER(SolveReport)],
 }
 _RESTYPES = {"hs_abi_version": _I, "hs_last_error": ctypes.c_char_p, "hs_status_string": ctypes.c_char_p,
-             "hs_packed_matrix_size": _I64, "hs_padded_vector_size": _I64}
+             "hs_packed_matrix_size": _I64, "hs_padded_vector_size": _I64, "hs_ctx_launch_count": _I64}
 
 _lib = None
 

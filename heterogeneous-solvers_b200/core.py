@@ -85,6 +85,27 @@ class Context:
     def sync(self):
         call("hs_sync", self.handle)
 
+    def set_profiling(self, enable=True):
+        call("hs_ctx_set_profiling", self.handle, int(bool(enable)))
+
+    def read_profile(self, kernel):
+        """(launches, device ms, algorithmic flops, algorithmic bytes) of one kernel family."""
+        out = _lib.KernelProfile()
+        call("hs_ctx_read_profile", self.handle, _lib.KERNEL_IDS[kernel], ctypes.byref(out))
+        return {"launches": out.launches, "ms": out.ms, "flops": out.flops, "bytes": out.bytes}
+
+    def reset_profile(self):
+        call("hs_ctx_reset_profile", self.handle)
+
+    def set_reference_order(self, cpu_chunks):
+        """cpu_chunks > 0: matvec, dots, vector updates and CG follow the
+        reference CPU path's accumulation order exactly (its dot product sums
+        `cpu_chunks` = core-count chunks); 0 restores the fast kernels."""
+        call("hs_ctx_set_reference_order", self.handle, int(cpu_chunks))
+
+    def launch_count(self):
+        return _lib.load().hs_ctx_launch_count(self.handle)
+
     def take_info(self):
         v = ctypes.c_int64()
         call("hs_ctx_take_info", self.handle, ctypes.byref(v))
@@ -453,19 +474,29 @@ class MatrixParser:
 
 
 def gp_solve_host(ctx, X, y, lengthscale=1.0, signal_variance=1.0, noise_variance=0.01, algorithm="cholesky",
-                  epsilon=1e-10, iMax=100000):
+                  epsilon=1e-10, iMax=100000, out=None):
     """End-to-end GP solve through host buffers (hs_gp_solve_host): host X
-    (N x d) and y (N) in, host x = K^-1 y out, plus the phase report."""
-    X = np.ascontiguousarray(X, dtype=np.float64)
-    y = np.ascontiguousarray(y, dtype=np.float64)
+    (N x d) and y (N) in, host x = K^-1 y out, plus the phase report.  X, y
+    and ``out`` may be CPU torch tensors (pinned memory gives asynchronous
+    copies) or numpy arrays."""
+
+    def host(a, shape=None):
+        if isinstance(a, torch.Tensor):
+            if a.is_cuda or a.dtype != torch.float64 or not a.is_contiguous():
+                raise TypeError("host tensors must be contiguous CPU float64")
+            return a, ctypes.c_void_p(a.data_ptr())
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        return a, a.ctypes.data_as(ctypes.c_void_p)
+
+    X, Xp = host(X)
+    y, yp = host(y)
     N, d = X.shape
     if ctx.N != N:
         raise ValueError("context N differs from X")
     ell = np.atleast_1d(np.asarray(lengthscale, dtype=np.float64))
-    x = np.empty(N, dtype=np.float64)
+    x, xp = host(out if out is not None else np.empty(N, dtype=np.float64))
     rep = SolveReport()
-    call("hs_gp_solve_host", ctx.handle, X.ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p), d,
-         ell.ctypes.data_as(ctypes.c_void_p), int(ell.size), float(signal_variance), float(noise_variance),
-         0 if algorithm == "cholesky" else 1, float(epsilon), int(iMax), x.ctypes.data_as(ctypes.c_void_p),
-         ctypes.byref(rep))
+    call("hs_gp_solve_host", ctx.handle, Xp, yp, d, ell.ctypes.data_as(ctypes.c_void_p), int(ell.size),
+         float(signal_variance), float(noise_variance), 0 if algorithm == "cholesky" else 1, float(epsilon),
+         int(iMax), xp, ctypes.byref(rep))
     return x, rep

@@ -13,6 +13,7 @@ static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 
 hs_status cuda_fail(cudaError_t e, const char* what) {
+    cudaGetLastError();  // clear a non-sticky error so that later calls do not inherit it
     set_error(std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
     return e == cudaErrorMemoryAllocation ? HS_ERR_OOM : HS_ERR_CUDA;
 }
@@ -57,6 +58,55 @@ hs_status ensure_work(hs_ctx ctx, size_t bytes) {
 }
 
 __global__ void set_i64_kernel(long long* p, long long v) { *p = v; }
+
+static cudaEvent_t pool_get(hs_ctx ctx) {
+    if (!ctx->prof_pool.empty()) {
+        cudaEvent_t e = ctx->prof_pool.back();
+        ctx->prof_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void prof_begin(hs_ctx ctx, cudaStream_t s, int kernel) {
+    if (!ctx->profiling) return;
+    hs_ctx_s::ProfRec r{kernel, pool_get(ctx), pool_get(ctx), 0.0, 0.0};
+    cudaEventRecord(r.start, s);
+    ctx->prof_pending.push_back(r);
+}
+
+void prof_end(hs_ctx ctx, cudaStream_t s, int kernel, double flops, double bytes) {
+    if (!ctx->profiling) return;
+    for (auto it = ctx->prof_pending.rbegin(); it != ctx->prof_pending.rend(); ++it) {
+        if (it->kernel == kernel && it->flops == 0.0 && it->bytes == 0.0) {
+            cudaEventRecord(it->stop, s);
+            it->flops = flops > 0 ? flops : -1.0;  // marks the pair closed
+            it->bytes = bytes;
+            return;
+        }
+    }
+}
+
+static hs_status prof_collect(hs_ctx ctx) {
+    if (ctx->prof_pending.empty()) return HS_OK;
+    HS_CUDA(cudaDeviceSynchronize());
+    for (auto& r : ctx->prof_pending) {
+        float ms = 0.f;
+        if (r.flops != 0.0 && cudaEventElapsedTime(&ms, r.start, r.stop) == cudaSuccess) {
+            auto& t = ctx->prof_total[r.kernel];
+            t.launches += 1;
+            t.ms += ms;
+            t.flops += r.flops > 0 ? r.flops : 0.0;
+            t.bytes += r.bytes;
+        }
+        ctx->prof_pool.push_back(r.start);
+        ctx->prof_pool.push_back(r.stop);
+    }
+    ctx->prof_pending.clear();
+    return HS_OK;
+}
 
 }  // namespace hs
 
@@ -126,12 +176,7 @@ hs_status hs_ctx_create(int device, void* stream, hs_ctx* out) {
     cudaDeviceProp prop;
     HS_CUDA(cudaGetDeviceProperties(&prop, device));
     ctx->num_sms = prop.multiProcessorCount;
-    if (stream) {
-        ctx->stream = static_cast<cudaStream_t>(stream);
-    } else {
-        HS_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-        ctx->own_stream = true;
-    }
+    ctx->stream = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
     HS_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
     HS_CUDA(cudaEventCreateWithFlags(&ctx->ev_a, cudaEventDisableTiming));
     HS_CUDA(cudaEventCreateWithFlags(&ctx->ev_b, cudaEventDisableTiming));
@@ -154,11 +199,15 @@ hs_status hs_ctx_destroy(hs_ctx ctx) {
     }
     if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
     if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
+    for (auto& r : ctx->prof_pending) {
+        cudaEventDestroy(r.start);
+        cudaEventDestroy(r.stop);
+    }
+    for (auto e : ctx->prof_pool) cudaEventDestroy(e);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->work) cudaFree(ctx->work);
     if (ctx->d_info) cudaFree(ctx->d_info);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
-    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return HS_OK;
 }
@@ -170,16 +219,7 @@ hs_status hs_ctx_set_stream(hs_ctx ctx, void* stream) {
     }
     HS_CUDA(cudaSetDevice(ctx->device));
     HS_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (ctx->own_stream) {
-        HS_CUDA(cudaStreamDestroy(ctx->stream));
-        ctx->own_stream = false;
-    }
-    if (stream) {
-        ctx->stream = static_cast<cudaStream_t>(stream);
-    } else {
-        HS_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-        ctx->own_stream = true;
-    }
+    ctx->stream = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
     return HS_OK;
 }
 
@@ -205,11 +245,56 @@ hs_status hs_sync(hs_ctx ctx) {
     return HS_OK;
 }
 
+hs_status hs_ctx_set_profiling(hs_ctx ctx, int enable) {
+    if (!ctx) {
+        set_error("hs_ctx_set_profiling: null context");
+        return HS_ERR_INVALID_ARG;
+    }
+    ctx->profiling = enable != 0;
+    return HS_OK;
+}
+
+hs_status hs_ctx_read_profile(hs_ctx ctx, int kernel, hs_kernel_profile* out) {
+    if (!ctx || !out || kernel < 0 || kernel >= HS_KERNEL_COUNT) {
+        set_error("hs_ctx_read_profile: bad arguments");
+        return HS_ERR_INVALID_ARG;
+    }
+    HS_CUDA(cudaSetDevice(ctx->device));
+    hs_status st = prof_collect(ctx);
+    if (st != HS_OK) return st;
+    *out = ctx->prof_total[kernel];
+    return HS_OK;
+}
+
+hs_status hs_ctx_reset_profile(hs_ctx ctx) {
+    if (!ctx) {
+        set_error("hs_ctx_reset_profile: null context");
+        return HS_ERR_INVALID_ARG;
+    }
+    HS_CUDA(cudaSetDevice(ctx->device));
+    hs_status st = prof_collect(ctx);
+    if (st != HS_OK) return st;
+    for (auto& t : ctx->prof_total) t = hs_kernel_profile{};
+    return HS_OK;
+}
+
+int64_t hs_ctx_launch_count(hs_ctx ctx) { return ctx ? ctx->launches : -1; }
+
+hs_status hs_ctx_set_reference_order(hs_ctx ctx, int cpu_chunks) {
+    if (!ctx || cpu_chunks < 0 || cpu_chunks > 4096) {
+        set_error("hs_ctx_set_reference_order: chunks must be in [0, 4096]");
+        return HS_ERR_INVALID_ARG;
+    }
+    ctx->ref_chunks = cpu_chunks;
+    return HS_OK;
+}
+
 hs_status hs_ctx_take_info(hs_ctx ctx, int64_t* info) {
     HS_API_BEGIN("hs_ctx_take_info");
     long long v = 0;
     HS_CUDA(cudaMemcpyAsync(&v, ctx->d_info, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
     HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->launches += 1;
     set_i64_kernel<<<1, 1, 0, ctx->stream>>>(ctx->d_info, INT64_MAX);
     HS_CHECK_LAUNCH("reset info");
     if (info) *info = (v == INT64_MAX) ? -1 : (int64_t)v;
@@ -272,6 +357,7 @@ hs_status hs_symv_block(hs_ctx ctx, const double* A, const double* b, double* re
     HS_ARG(blockCountXY == ctx->nb, "blockCountXY does not match the context's N / matrixBlockSize");
     HS_ARG(bi0 >= 0 && nbi >= 0 && bi0 + nbi <= ctx->nb, "row blocks out of range");
     HS_ARG(bj0 >= 0 && nbj >= 0 && bj0 + nbj <= ctx->nb, "column blocks out of range");
+    if (ctx->ref_chunks > 0) return launch_symv_refseq(ctx, A, b, result, bi0, bj0, nbi, nbj, reset, ctx->stream);
     return launch_symv(ctx, A, b, result, bi0, bj0, nbi, nbj, reset, nullptr, nullptr, ctx->stream);
 }
 
@@ -332,6 +418,9 @@ hs_status hs_dot_block(hs_ctx ctx, const double* x, const double* y, double* res
     HS_API_BEGIN("hs_dot_block");
     HS_ARG(x && y && result, "null pointer");
     HS_ARG(bi0 >= 0 && nbi >= 0 && bi0 + nbi <= ctx->nb, "blocks out of range");
+    if (ctx->ref_chunks > 0)
+        return launch_dot_refseq(ctx, x, y, result, (int64_t)bi0 * ctx->bsz, (int64_t)nbi * ctx->bsz,
+                                 ctx->ref_chunks, ctx->stream);
     return launch_dot(ctx, x, y, result, (int64_t)bi0 * ctx->bsz, (int64_t)nbi * ctx->bsz, ctx->stream);
 }
 

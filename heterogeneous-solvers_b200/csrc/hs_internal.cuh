@@ -6,13 +6,13 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/hs_b200.h"
 
 struct hs_ctx_s {
     int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
+    cudaStream_t stream = nullptr;  // caller's stream; nullptr is the CUDA default stream
     int num_sms = 148;
 
     int64_t N = 0;   // conf::N
@@ -33,6 +33,24 @@ struct hs_ctx_s {
     // second stream + events used by the drivers for lookahead
     cudaStream_t side = nullptr;
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+
+    // > 0: matvec, dot and vector updates follow the reference CPU path's exact
+    // accumulation order (separate multiply and add, dot products in this many
+    // sequential chunks) so that CG reproduces it bit for bit
+    int ref_chunks = 0;
+
+    // kernels launched through this context (all launch sites count)
+    int64_t launches = 0;
+    // optional per-kernel timing: event pairs recorded on the launching stream
+    bool profiling = false;
+    struct ProfRec {
+        int kernel;
+        cudaEvent_t start, stop;
+        double flops, bytes;
+    };
+    std::vector<ProfRec> prof_pending;
+    std::vector<cudaEvent_t> prof_pool;
+    hs_kernel_profile prof_total[HS_KERNEL_COUNT] = {};
 };
 
 namespace hs {
@@ -62,6 +80,10 @@ hs_status cuda_fail(cudaError_t e, const char* what);
     } while (0)
 
 hs_status require_ctx(hs_ctx ctx, const char* fn);
+
+// per-kernel timing around one launch (no-ops unless ctx->profiling)
+void prof_begin(hs_ctx ctx, cudaStream_t s, int kernel);
+void prof_end(hs_ctx ctx, cudaStream_t s, int kernel, double flops, double bytes);
 // makes sure at least `bytes` of scratch are available (stream-ordered safe:
 // the old buffer is released after a stream sync)
 hs_status ensure_scratch(hs_ctx ctx, size_t bytes);
@@ -128,6 +150,11 @@ hs_status launch_dot(hs_ctx ctx, const double* x, const double* y, double* resul
                      cudaStream_t s);
 hs_status launch_vec(hs_ctx ctx, int op, const double* x, const double* y, double alpha, double* out,
                      int64_t first, int64_t len, cudaStream_t s);
+// reference-order forms (ctx->ref_chunks > 0)
+hs_status launch_symv_refseq(hs_ctx ctx, const double* A, const double* b, double* result, int bi0, int bj0,
+                             int nbi, int nbj, int reset, cudaStream_t s);
+hs_status launch_dot_refseq(hs_ctx ctx, const double* x, const double* y, double* result, int64_t first,
+                            int64_t len, int chunks, cudaStream_t s);
 hs_status launch_rbf_assemble(hs_ctx ctx, double* A, const double* X, int d, const double* ell_host, int n_ell,
                               double sf2, double sn2, cudaStream_t s);
 

@@ -138,9 +138,11 @@ hs_status cg_driver(hs_ctx ctx, const double* A, const double* b, double* x, dou
     const int nb = ctx->nb;
     const int64_t n = (int64_t)nb * ctx->bsz;
     cudaStream_t s = ctx->stream;
+    const bool ref = ctx->ref_chunks > 0;
     hs_status st = ensure_work(ctx, (size_t)3 * n * sizeof(double));
     if (st != HS_OK) return st;
-    st = ensure_scratch(ctx, kSmallScratch);
+    // size the scratch for the matvec partials now: pointers into it stay valid below
+    st = ensure_scratch(ctx, kSmallScratch + (size_t)nb * nb * ctx->bsz * sizeof(double));
     if (st != HS_OK) return st;
     double* r = static_cast<double*>(ctx->work);
     double* d = r + n;
@@ -153,48 +155,72 @@ hs_status cg_driver(hs_ctx ctx, const double* A, const double* b, double* x, dou
     volatile double* h = ctx->h_pinned;
     const int g = grid_for(n, ctx->num_sms);
 
+    auto matvec = [&](const double* v, double* out, double* dot_with, double* dot_out) -> hs_status {
+        if (!ref) return launch_symv(ctx, A, v, out, 0, 0, nb, nb, 1, dot_with, dot_out, s);
+        hs_status st2 = launch_symv_refseq(ctx, A, v, out, 0, 0, nb, nb, 1, s);
+        if (st2 != HS_OK || !dot_with) return st2;
+        return launch_dot_refseq(ctx, dot_with, out, dot_out, 0, n, ctx->ref_chunks, s);
+    };
+    // r = b - r, delta = r.r
+    auto residual = [&]() -> hs_status {
+        if (!ref) {
+            ctx->launches += 2;
+            cg_residual<<<g, kThreads, 0, s>>>(b, r, n, part);
+            sum_partials<<<1, kThreads, 0, s>>>(part, g, d_delta);
+            HS_CHECK_LAUNCH("cg residual");
+            return HS_OK;
+        }
+        hs_status st2 = launch_vec(ctx, 2, b, r, 0.0, r, 0, n, s);
+        if (st2 != HS_OK) return st2;
+        return launch_dot_refseq(ctx, r, r, d_delta, 0, n, ctx->ref_chunks, s);
+    };
+    auto read_scalar = [&](double* dev, int slot) -> hs_status {
+        HS_CUDA(cudaMemcpyAsync((void*)(h + slot), dev, sizeof(double), cudaMemcpyDeviceToHost, s));
+        HS_CUDA(cudaStreamSynchronize(s));
+        return HS_OK;
+    };
+
     HS_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));  // CG.cpp:217 leaves x_gpu uninitialised; x0 = 0
     // initCG (CG.cpp:277-340): r = A x; r = b - r; d = r; delta_0 = delta_new = r.r
-    st = launch_symv(ctx, A, x, r, 0, 0, nb, nb, 1, nullptr, nullptr, s);
-    if (st != HS_OK) return st;
-    cg_residual<<<g, kThreads, 0, s>>>(b, r, n, part);
-    sum_partials<<<1, kThreads, 0, s>>>(part, g, d_delta);
+    if ((st = matvec(x, r, nullptr, nullptr)) != HS_OK) return st;
+    if ((st = residual()) != HS_OK) return st;
     HS_CUDA(cudaMemcpyAsync(d, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    HS_CUDA(cudaMemcpyAsync((void*)(h + 1), d_delta, sizeof(double), cudaMemcpyDeviceToHost, s));
-    HS_CUDA(cudaStreamSynchronize(s));
+    if ((st = read_scalar(d_delta, 1)) != HS_OK) return st;
     double delta_new = h[1];
     const double delta_zero = delta_new;
     const double eps2 = eps * eps;
     int64_t it = 0;
     while (it < imax && delta_new > eps2 * delta_zero) {
         // q = A d fused with d.q (CG.cpp:342-431)
-        st = launch_symv(ctx, A, d, q, 0, 0, nb, nb, 1, d, d_dq, s);
-        if (st != HS_OK) return st;
-        HS_CUDA(cudaMemcpyAsync((void*)(h + 0), d_dq, sizeof(double), cudaMemcpyDeviceToHost, s));
-        HS_CUDA(cudaStreamSynchronize(s));
+        if ((st = matvec(d, q, d, d_dq)) != HS_OK) return st;
+        if ((st = read_scalar(d_dq, 0)) != HS_OK) return st;
         const double alpha = delta_new / h[0];
-        h[2] = alpha;
-        HS_CUDA(cudaMemcpyAsync(d_alpha, (const void*)(h + 2), sizeof(double), cudaMemcpyHostToDevice, s));
-        if (it % 50 == 0) {
-            // x = x + alpha d, then the true residual r = b - A x (CG.cpp:95-101, :444-470)
-            st = launch_vec(ctx, 3, x, d, alpha, x, 0, n, s);
-            if (st != HS_OK) return st;
-            st = launch_symv(ctx, A, x, r, 0, 0, nb, nb, 1, nullptr, nullptr, s);
-            if (st != HS_OK) return st;
-            cg_residual<<<g, kThreads, 0, s>>>(b, r, n, part);
+        if (it % 50 == 0 || ref) {
+            // x = x + alpha d (CG.cpp:433-442)
+            if ((st = launch_vec(ctx, 3, x, d, alpha, x, 0, n, s)) != HS_OK) return st;
+            if (it % 50 == 0) {
+                // true residual r = b - A x (CG.cpp:95-101, :444-470)
+                if ((st = matvec(x, r, nullptr, nullptr)) != HS_OK) return st;
+                if ((st = residual()) != HS_OK) return st;
+            } else {
+                // r = r - alpha q (CG.cpp:473-484), delta = r.r
+                if ((st = launch_vec(ctx, 3, r, q, -1.0 * alpha, r, 0, n, s)) != HS_OK) return st;
+                if ((st = launch_dot_refseq(ctx, r, r, d_delta, 0, n, ctx->ref_chunks, s)) != HS_OK) return st;
+            }
         } else {
+            h[2] = alpha;
+            HS_CUDA(cudaMemcpyAsync(d_alpha, (const void*)(h + 2), sizeof(double), cudaMemcpyHostToDevice, s));
+            ctx->launches += 2;
             cg_update_xr<<<g, kThreads, 0, s>>>(x, d, r, q, d_alpha, n, part);
+            sum_partials<<<1, kThreads, 0, s>>>(part, g, d_delta);
+            HS_CHECK_LAUNCH("cg step");
         }
-        sum_partials<<<1, kThreads, 0, s>>>(part, g, d_delta);
-        HS_CHECK_LAUNCH("cg step");
-        HS_CUDA(cudaMemcpyAsync((void*)(h + 1), d_delta, sizeof(double), cudaMemcpyDeviceToHost, s));
-        HS_CUDA(cudaStreamSynchronize(s));
+        if ((st = read_scalar(d_delta, 1)) != HS_OK) return st;
         const double delta_old = delta_new;
         delta_new = h[1];
         const double beta = delta_new / delta_old;
         // d = r + beta d (CG.cpp:519-528)
-        st = launch_vec(ctx, 3, r, d, beta, d, 0, n, s);
-        if (st != HS_OK) return st;
+        if ((st = launch_vec(ctx, 3, r, d, beta, d, 0, n, s)) != HS_OK) return st;
         ++it;
     }
     HS_CUDA(cudaStreamSynchronize(s));
@@ -233,6 +259,7 @@ hs_status hs_cholesky_factor(hs_ctx ctx, double* A, int64_t* info) {
         set_error("hs_cholesky_factor: null matrix");
         return HS_ERR_INVALID_ARG;
     }
+    ctx->launches += 1;
     set_i64<<<1, 1, 0, ctx->stream>>>(ctx->d_info, INT64_MAX);
     st = factor_driver(ctx, A);
     if (st != HS_OK) return st;
@@ -324,6 +351,7 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
     HS_E2E(cudaEventRecord(ev[1], s));
     int64_t info = -1, iters = 0;
     if (algorithm == 0) {
+        ctx->launches += 1;
         set_i64<<<1, 1, 0, s>>>(ctx->d_info, INT64_MAX);
         st = factor_driver(ctx, Ad);
         if (st != HS_OK) { cleanup(); return st; }

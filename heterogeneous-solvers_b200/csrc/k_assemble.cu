@@ -128,6 +128,8 @@ hs_status launch_rbf_assemble(hs_ctx ctx, double* A, const double* X, int d, con
     const int64_t T = total_blocks(nb);
     HS_REQUIRE(T < (1LL << 31), "too many blocks");
     const size_t smem = (size_t)2 * bsz * d * sizeof(double);
+    prof_begin(ctx, s, HS_KERNEL_ASSEMBLE);
+    ctx->launches += 1;
     if (bsz % 2 == 0 && smem <= 200 * 1024) {
         if (smem > 48 * 1024)
             HS_CUDA(cudaFuncSetAttribute(rbf_assemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -136,6 +138,7 @@ hs_status launch_rbf_assemble(hs_ctx ctx, double* A, const double* X, int d, con
         rbf_assemble_odd_kernel<<<(unsigned)T, 256, 0, s>>>(A, X, ctx->N, d, bsz, nb, ard, wdev, sf2, sn2, iso_scale);
     }
     HS_CHECK_LAUNCH("rbf_assemble");
+    prof_end(ctx, s, HS_KERNEL_ASSEMBLE, (double)T * bsz * bsz * (3.0 * d + 2.0), (double)T * bsz * bsz * 8.0);
     return HS_OK;
 }
 

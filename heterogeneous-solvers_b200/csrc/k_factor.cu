@@ -359,7 +359,8 @@ hs_status set_attrs() {
     return HS_OK;
 }
 
-hs_status launch_trsm_args(const TrsmArgs& ta, int items, cudaStream_t s) {
+hs_status launch_trsm_args(hs_ctx ctx, const TrsmArgs& ta, int items, cudaStream_t s) {
+    ctx->launches += 1;
     HS_REQUIRE(ta.n <= 256, "TRSM supports triangles up to 256");
     const size_t smem = trsm_smem(ta.n);
     trsm_kernel<<<items * ta.slabs, 256, smem, s>>>(ta);
@@ -369,6 +370,7 @@ hs_status launch_trsm_args(const TrsmArgs& ta, int items, cudaStream_t s) {
 
 hs_status potrf_small(hs_ctx ctx, double* blk, int ld, int n, int valid, long long row_base, cudaStream_t s) {
     const size_t smem = (size_t)n * (n + 1) * sizeof(double);
+    ctx->launches += 1;
     potrf_smem_kernel<<<1, 512, smem, s>>>(blk, ld, n, valid, ctx->d_info, row_base);
     HS_CHECK_LAUNCH("potrf");
     return HS_OK;
@@ -376,7 +378,7 @@ hs_status potrf_small(hs_ctx ctx, double* blk, int ld, int n, int valid, long lo
 
 }  // namespace
 
-hs_status launch_potrf(hs_ctx ctx, double* A, int blockID, int blockRow, cudaStream_t s) {
+static hs_status potrf_impl(hs_ctx ctx, double* A, int blockID, int blockRow, cudaStream_t s) {
     hs_status st = set_attrs();
     if (st != HS_OK) return st;
     const int bsz = ctx->bsz;
@@ -395,8 +397,9 @@ hs_status launch_potrf(hs_ctx ctx, double* A, int blockID, int blockRow, cudaStr
         double* A22 = A21 + n1;
         if (valid > n1) {
             TrsmArgs ta{blk, bsz, n1, A21, bsz, 0, n2 / kTrsmRows, n2, 0};
-            st = launch_trsm_args(ta, 1, s);
+            st = launch_trsm_args(ctx, ta, 1, s);
             if (st != HS_OK) return st;
+            ctx->launches += 1;
             tile_update_kernel<<<1, 256, kTileSmem, s>>>(A22, bsz, A21, A21, bsz, n1, 1);
             HS_CHECK_LAUNCH("potrf syrk");
             st = potrf_small(ctx, A22, bsz, n2, valid - n1, row_base + n1, s);
@@ -405,13 +408,23 @@ hs_status launch_potrf(hs_ctx ctx, double* A, int blockID, int blockRow, cudaStr
             st = potrf_small(ctx, A22, bsz, n2, 0, row_base + n1, s);
         }
         if (st != HS_OK) return st;
+        ctx->launches += 1;
         zero_tile_kernel<<<16, 256, 0, s>>>(blk + n1, bsz, min(valid, n1), n2);
         HS_CHECK_LAUNCH("potrf zero");
         return HS_OK;
     }
+    ctx->launches += 1;
     potrf_global_kernel<<<1, 1024, 0, s>>>(blk, bsz, valid, ctx->d_info, row_base);
     HS_CHECK_LAUNCH("potrf");
     return HS_OK;
+}
+
+hs_status launch_potrf(hs_ctx ctx, double* A, int blockID, int blockRow, cudaStream_t s) {
+    const double n = ctx->bsz;
+    prof_begin(ctx, s, HS_KERNEL_POTRF);
+    hs_status st = potrf_impl(ctx, A, blockID, blockRow, s);
+    prof_end(ctx, s, HS_KERNEL_POTRF, n * n * n / 3.0, 2.0 * n * n * 8.0);
+    return st;
 }
 
 hs_status launch_trsm(hs_ctx ctx, double* A, int blockID, int blockRow, int blockStart, int blockCount,
@@ -424,7 +437,11 @@ hs_status launch_trsm(hs_ctx ctx, double* A, int blockID, int blockRow, int bloc
     const size_t bb = (size_t)bsz * bsz;
     TrsmArgs ta{A + (size_t)blockID * bb, bsz, bsz, A, bsz, (int64_t)blockID + (blockStart - blockRow),
                 (bsz + kTrsmRows - 1) / kTrsmRows, bsz, (int64_t)bb};
-    return launch_trsm_args(ta, blockCount, s);
+    const double n = bsz;
+    prof_begin(ctx, s, HS_KERNEL_TRSM);
+    st = launch_trsm_args(ctx, ta, blockCount, s);
+    prof_end(ctx, s, HS_KERNEL_TRSM, blockCount * n * n * n, (2.0 * blockCount + 1.0) * n * n * 8.0);
+    return st;
 }
 
 hs_status launch_update(hs_ctx ctx, double* A, int blockID, int blockRow, int syrkStart, int syrkCount,
@@ -450,18 +467,31 @@ hs_status launch_update(hs_ctx ctx, double* A, int blockID, int blockRow, int sy
     const int64_t total = pairs + (syrkCount > 0 ? syrkCount : 0);
     if (total <= 0) return HS_OK;
     a.totalPairs = total;
+    // algorithmic work: 2 bsz^3 per GEMM pair, bsz^2 (bsz + 1) per SYRK block;
+    // bytes: read + write of every output block plus the panel column once
+    const double n = ctx->bsz;
+    const int64_t syrkN = syrkCount > 0 ? syrkCount : 0;
+    const double flops = (double)pairs * 2.0 * n * n * n + (double)syrkN * n * n * (n + 1.0);
+    const int64_t panel = (gemmCount > 0 ? gemmCount + 1 : 0) > syrkN ? (gemmCount + 1) : syrkN;
+    const double bytes = ((double)pairs * 2.0 + (double)syrkN * 2.0 + (double)panel) * n * n * 8.0;
     if (ctx->bsz % BM == 0) {
         a.tilesPerSide = ctx->bsz / BM;
         const int64_t grid = total * a.tilesPerSide * a.tilesPerSide;
         HS_REQUIRE(grid < (1LL << 31), "trailing update too large for one launch");
+        prof_begin(ctx, s, HS_KERNEL_UPDATE);
+        ctx->launches += 1;
         update_dmma_kernel<<<(unsigned)grid, 256, kTileSmem, s>>>(a);
         HS_CHECK_LAUNCH("update_dmma");
+        prof_end(ctx, s, HS_KERNEL_UPDATE, flops, bytes);
     } else {
         const int64_t bb = (int64_t)ctx->bsz * ctx->bsz;
         dim3 grid((unsigned)((bb + 255) / 256), (unsigned)(total < 65535 ? total : 65535),
                   (unsigned)((total + 65534) / 65535));
+        prof_begin(ctx, s, HS_KERNEL_UPDATE);
+        ctx->launches += 1;
         update_scalar_kernel<<<grid, 256, 0, s>>>(a);
         HS_CHECK_LAUNCH("update_scalar");
+        prof_end(ctx, s, HS_KERNEL_UPDATE, flops, bytes);
     }
     return HS_OK;
 }

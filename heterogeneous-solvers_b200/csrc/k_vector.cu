@@ -36,8 +36,43 @@ __global__ void vec_kernel(const double* __restrict__ x, const double* __restric
     }
 }
 
+// reference-order forms: no contraction, the reference's operand order
+template <int OP>
+__global__ void vec_kernel_ref(const double* __restrict__ x, const double* __restrict__ y, double alpha,
+                               double* __restrict__ out, int64_t first, int64_t len) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < len; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = first + t;
+        double v;
+        if (OP == 0) v = __dmul_rn(x[i], alpha);
+        else if (OP == 1) v = __dadd_rn(x[i], y[i]);
+        else if (OP == 2) v = __dsub_rn(x[i], y[i]);
+        else v = __dadd_rn(x[i], __dmul_rn(y[i], alpha));
+        out[i] = v;
+    }
+}
+
 // ------------------------------------------------------------------ dot
 constexpr int kDotBlocks = 512;
+
+// VectorOperations.cpp:187-238: ceil(len/chunks) elements per chunk summed
+// from zero, then the chunk sums in order; one thread per chunk
+__global__ void dot_refseq_chunks(const double* __restrict__ x, const double* __restrict__ y, int64_t first,
+                                  int64_t len, int chunks, double* __restrict__ part) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= chunks) return;
+    const int64_t per = (len + chunks - 1) / chunks;
+    const int64_t s = (int64_t)c * per + first;
+    const int64_t e = (s + per < first + len) ? s + per : first + len;
+    double v = 0.0;
+    for (int64_t i = s; i < e; ++i) v = __dadd_rn(v, __dmul_rn(x[i], y[i]));
+    part[c] = v;
+}
+
+__global__ void dot_refseq_final(const double* __restrict__ part, int chunks, double* __restrict__ out) {
+    double v = 0.0;
+    for (int c = 0; c < chunks; ++c) v = __dadd_rn(v, part[c]);
+    *out = v;
+}
 
 __device__ __forceinline__ double block_reduce_sum(double v, double* sh) {
     // fixed-order tree: warp butterfly, then the 8 warp sums in order
@@ -230,6 +265,35 @@ __global__ void __launch_bounds__(kThreads) symv_reduce(const double* __restrict
     }
 }
 
+// reference-order SYMV (MatrixVectorOperations.cpp:194-280): one thread per
+// row, one running sum over the stored blocks j <= i row-wise and then the
+// blocks j > i column-wise, products and sums rounded separately
+__global__ void symv_refseq_kernel(const double* __restrict__ A, const double* __restrict__ b,
+                                   double* __restrict__ result, int bsz, int nb, int bi0, int bj0, int nbi, int nbj,
+                                   int reset) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nbi * bsz) return;
+    const int64_t i = t + (int64_t)bi0 * bsz;
+    const int iIn = (int)(i % bsz);
+    const int bi = (int)(i / bsz);
+    const size_t bb = (size_t)bsz * bsz;
+    double v = 0.0;
+    if (!reset) v = __dadd_rn(v, result[i]);
+    int bj = bj0;
+    const int last = bj0 + nbj - 1;
+    for (; bj <= (bi < last ? bi : last); ++bj) {
+        const double* row = A + (size_t)block_id(bi, bj, nb) * bb + (size_t)iIn * bsz;
+        const double* bv = b + (size_t)bj * bsz;
+        for (int j = 0; j < bsz; ++j) v = __dadd_rn(v, __dmul_rn(row[j], bv[j]));
+    }
+    for (; bj < bj0 + nbj; ++bj) {
+        const double* blk = A + (size_t)block_id(bj, bi, nb) * bb;
+        const double* bv = b + (size_t)bj * bsz;
+        for (int j = 0; j < bsz; ++j) v = __dadd_rn(v, __dmul_rn(blk[(size_t)j * bsz + iIn], bv[j]));
+    }
+    result[i] = v;
+}
+
 // ------------------------------------------------------------------ column update
 template <int BSZ>
 __global__ void __launch_bounds__(kThreads) column_update_kernel(const double* __restrict__ A, double* __restrict__ b,
@@ -332,9 +396,36 @@ hs_status launch_dot(hs_ctx ctx, const double* x, const double* y, double* resul
     if (st != HS_OK) return st;
     double* partial = static_cast<double*>(ctx->scratch);
     const int g = dot_blocks(len);
+    prof_begin(ctx, s, HS_KERNEL_VECTOR);
+    ctx->launches += 2;
     dot_stage1<<<g, kThreads, 0, s>>>(x, y, first, len, partial);
     dot_stage2<<<1, kThreads, 0, s>>>(partial, g, result);
     HS_CHECK_LAUNCH("dot");
+    prof_end(ctx, s, HS_KERNEL_VECTOR, 2.0 * len, 16.0 * len);
+    return HS_OK;
+}
+
+hs_status launch_symv_refseq(hs_ctx ctx, const double* A, const double* b, double* result, int bi0, int bj0,
+                             int nbi, int nbj, int reset, cudaStream_t s) {
+    const int64_t rows = (int64_t)nbi * ctx->bsz;
+    if (rows <= 0) return HS_OK;
+    ctx->launches += 1;
+    symv_refseq_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(A, b, result, ctx->bsz, ctx->nb, bi0, bj0, nbi,
+                                                                     nbj, reset);
+    HS_CHECK_LAUNCH("symv_refseq");
+    return HS_OK;
+}
+
+hs_status launch_dot_refseq(hs_ctx ctx, const double* x, const double* y, double* result, int64_t first,
+                            int64_t len, int chunks, cudaStream_t s) {
+    hs_status st = ensure_scratch(ctx, kSmallScratch);
+    if (st != HS_OK) return st;
+    HS_REQUIRE(chunks <= kMaxPartials, "too many chunks");
+    double* part = static_cast<double*>(ctx->scratch);
+    ctx->launches += 2;
+    dot_refseq_chunks<<<(chunks + 127) / 128, 128, 0, s>>>(x, y, first, len, chunks, part);
+    dot_refseq_final<<<1, 1, 0, s>>>(part, chunks, result);
+    HS_CHECK_LAUNCH("dot_refseq");
     return HS_OK;
 }
 
@@ -347,7 +438,19 @@ hs_status launch_symv(hs_ctx ctx, const double* A, const double* b, double* resu
     if (st != HS_OK) return st;
     double* small = static_cast<double*>(ctx->scratch);
     double* P = reinterpret_cast<double*>(static_cast<char*>(ctx->scratch) + kSmallScratch);
+    // algorithmic bytes: every stored block the rectangle touches, read once, plus the vectors
+    int64_t stored = 0;
+    for (int I = bi0; I < bi0 + nbi; ++I) {
+        const int lo = bj0, hi = bj0 + nbj;  // J range
+        for (int J = lo; J < hi; ++J) {
+            const bool mirrored = J > I && J >= bi0 && J < bi0 + nbi && I >= bj0 && I < bj0 + nbj;
+            if (!mirrored) ++stored;
+        }
+    }
+    const double bb = (double)bsz * bsz;
+    prof_begin(ctx, s, HS_KERNEL_SYMV);
     if (nbj > 0) {
+        ctx->launches += 1;
         const int64_t grid = (int64_t)nbi * nbj;
         if (bsz == 256)
             symv_partials<256><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
@@ -362,9 +465,12 @@ hs_status launch_symv(hs_ctx ctx, const double* A, const double* b, double* resu
     if (rg64 > kMaxPartials) rg64 = kMaxPartials;
     const unsigned rg = (unsigned)rg64;
     double* wpart = small;
+    ctx->launches += dot_with ? 2 : 1;
     symv_reduce<<<rg, kThreads, 0, s>>>(P, result, bsz, bi0, nbi, nbj, reset, dot_with, wpart);
     if (dot_with) dot_stage2<<<1, kThreads, 0, s>>>(wpart, (int)rg, dot_out);
     HS_CHECK_LAUNCH("symv_reduce");
+    prof_end(ctx, s, HS_KERNEL_SYMV, 2.0 * (double)nbi * nbj * bb,
+             (double)stored * bb * 8.0 + 8.0 * ((double)nbj * bsz + 2.0 * nbi * bsz));
     return HS_OK;
 }
 
@@ -373,6 +479,8 @@ hs_status launch_column_update(hs_ctx ctx, const double* A, double* b, int block
     if (blockCount <= 0) return HS_OK;
     const int bsz = ctx->bsz;
     HS_REQUIRE(bsz <= 1024, "matrixBlockSize > 1024 is not supported by the column update");
+    prof_begin(ctx, s, HS_KERNEL_COLUPD);
+    ctx->launches += 1;
     if (bsz == 256)
         column_update_kernel<256><<<blockCount, kThreads, 0, s>>>(A, b, bsz, ctx->nb, blockStart, blockRow, blockID,
                                                                   transposed);
@@ -383,6 +491,8 @@ hs_status launch_column_update(hs_ctx ctx, const double* A, double* b, int block
         column_update_kernel<0><<<blockCount, kThreads, 0, s>>>(A, b, bsz, ctx->nb, blockStart, blockRow, blockID,
                                                                 transposed);
     HS_CHECK_LAUNCH("column_update");
+    prof_end(ctx, s, HS_KERNEL_COLUPD, 2.0 * blockCount * (double)bsz * bsz,
+             (double)blockCount * bsz * bsz * 8.0 + 24.0 * blockCount * bsz);
     return HS_OK;
 }
 
@@ -393,8 +503,11 @@ hs_status launch_trsv(hs_ctx ctx, const double* A, double* b, int blockRow, int 
     HS_REQUIRE(smem <= 200 * 1024, "matrixBlockSize too large for the block triangular solve");
     if (smem > 48 * 1024) HS_CUDA(cudaFuncSetAttribute(trsv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        (int)smem));
+    prof_begin(ctx, s, HS_KERNEL_TRSV);
+    ctx->launches += 1;
     trsv_kernel<<<1, kThreads, smem, s>>>(A, b, bsz, ctx->N, blockRow, blockID, transposed, nullptr);
     HS_CHECK_LAUNCH("trsv");
+    prof_end(ctx, s, HS_KERNEL_TRSV, (double)bsz * bsz, (double)bsz * bsz * 4.0 + 16.0 * bsz);
     return HS_OK;
 }
 
@@ -403,6 +516,17 @@ hs_status launch_vec(hs_ctx ctx, int op, const double* x, const double* y, doubl
     if (len <= 0) return HS_OK;
     int64_t g = (len + kThreads - 1) / kThreads;
     if (g > 8 * (int64_t)ctx->num_sms) g = 8 * (int64_t)ctx->num_sms;
+    ctx->launches += 1;
+    if (ctx->ref_chunks > 0) {
+        switch (op) {
+            case 0: vec_kernel_ref<0><<<(unsigned)g, kThreads, 0, s>>>(x, y, alpha, out, first, len); break;
+            case 1: vec_kernel_ref<1><<<(unsigned)g, kThreads, 0, s>>>(x, y, alpha, out, first, len); break;
+            case 2: vec_kernel_ref<2><<<(unsigned)g, kThreads, 0, s>>>(x, y, alpha, out, first, len); break;
+            default: vec_kernel_ref<3><<<(unsigned)g, kThreads, 0, s>>>(x, y, alpha, out, first, len); break;
+        }
+        HS_CHECK_LAUNCH("vector op");
+        return HS_OK;
+    }
     switch (op) {
         case 0: vec_kernel<0><<<(unsigned)g, kThreads, 0, s>>>(x, y, alpha, out, first, len); break;
         case 1: vec_kernel<1><<<(unsigned)g, kThreads, 0, s>>>(x, y, alpha, out, first, len); break;

@@ -54,8 +54,9 @@ int hs_abi_version(void);
 const char* hs_last_error(void);
 const char* hs_status_string(hs_status s);
 
-/* Create a context on `device`.  `stream` is a cudaStream_t (NULL: the context
- * creates and owns a non-blocking stream). */
+/* Create a context on `device`.  `stream` is the caller's cudaStream_t on which
+ * every call of this context is ordered; NULL selects the CUDA default stream.
+ * The context never destroys the caller's stream. */
 hs_status hs_ctx_create(int device, void* stream, hs_ctx* out);
 hs_status hs_ctx_destroy(hs_ctx ctx);
 hs_status hs_ctx_set_stream(hs_ctx ctx, void* stream);
@@ -66,6 +67,44 @@ hs_status hs_sync(hs_ctx ctx);
  * SymmetricMatrix.cpp:11-19, RightHandSide.cpp:8-15 */
 int64_t hs_packed_matrix_size(int64_t N, int matrixBlockSize);
 int64_t hs_padded_vector_size(int64_t N, int matrixBlockSize);
+
+/* Instrumentation.  With profiling on, every launch of the kernels below is
+ * bracketed by CUDA events on the stream it is launched on; hs_ctx_read_profile
+ * synchronises, folds the finished pairs into per-kernel totals and returns
+ * them (launches, summed device ms, algorithmic flops and bytes of those
+ * launches).  hs_ctx_launch_count counts every kernel launched through the
+ * context since its creation. */
+typedef enum hs_kernel_id {
+    HS_KERNEL_UPDATE = 0,    /* SYRK + GEMM trailing update (FP64) */
+    HS_KERNEL_POTRF = 1,
+    HS_KERNEL_TRSM = 2,
+    HS_KERNEL_SYMV = 3,      /* symmetric block matvec, both phases */
+    HS_KERNEL_TRSV = 4,
+    HS_KERNEL_COLUPD = 5,
+    HS_KERNEL_ASSEMBLE = 6,
+    HS_KERNEL_VECTOR = 7,    /* vector ops, dots, CG updates */
+    HS_KERNEL_COUNT = 8
+} hs_kernel_id;
+typedef struct hs_kernel_profile {
+    int64_t launches;
+    double ms;
+    double flops;
+    double bytes;
+} hs_kernel_profile;
+hs_status hs_ctx_set_profiling(hs_ctx ctx, int enable);
+hs_status hs_ctx_read_profile(hs_ctx ctx, int kernel, hs_kernel_profile* out);
+hs_status hs_ctx_reset_profile(hs_ctx ctx);
+int64_t hs_ctx_launch_count(hs_ctx ctx);
+
+/* Reference accumulation order.  cpu_chunks > 0 makes hs_symv_block, hs_dot_block,
+ * the vector updates and hs_cg_solve follow the arithmetic of the reference's CPU
+ * path exactly: one running sum per matrix row in block order
+ * (MatrixVectorOperations.cpp:194-280), multiplies and adds rounded separately,
+ * dot products summed in `cpu_chunks` sequential chunks and then in chunk order
+ * (VectorOperations.cpp:187-238, whose chunk count is the CPU's core count).
+ * CG then reproduces the reference's iterates bit for bit; it is a parity mode,
+ * far slower than the default (0: fused, tree-reduced kernels). */
+hs_status hs_ctx_set_reference_order(hs_ctx ctx, int cpu_chunks);
 
 /* ------------------------------------------------------------------ operators */
 /* MatrixOperations::cholesky / cholesky_GPU / cholesky_optimizedGPU
