@@ -76,6 +76,7 @@ SIGNATURES = {
     "hs_syrk_diag": [_P, _P, _I, _I, _I, _I, _I],
     "hs_gemm_trailing": [_P, _P, _I, _I, _I, _I, _I],
     "hs_symv_block": [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I],
+    "hs_symv_block_noalloc": [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I],
     "hs_trsv_block": [_P, _P, _P, _I, _I, _I],
     "hs_column_update": [_P, _P, _P, _I, _I, _I, _I, _I, _I],
     "hs_scale_block": [_P, _P, _D, _P, _I, _I],

@@ -150,6 +150,8 @@ hs_status launch_dot(hs_ctx ctx, const double* x, const double* y, double* resul
                      cudaStream_t s);
 hs_status launch_vec(hs_ctx ctx, int op, const double* x, const double* y, double alpha, double* out,
                      int64_t first, int64_t len, cudaStream_t s);
+hs_status launch_symv_partials_at(hs_ctx ctx, const double* A, const double* b, double* result, int bi0, int bj0,
+                                  int nbi, int nbj, int reset, double* P, cudaStream_t s);
 // reference-order forms (ctx->ref_chunks > 0)
 hs_status launch_symv_refseq(hs_ctx ctx, const double* A, const double* b, double* result, int bi0, int bj0,
                              int nbi, int nbj, int reset, cudaStream_t s);

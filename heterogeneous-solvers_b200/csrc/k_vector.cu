@@ -474,6 +474,32 @@ hs_status launch_symv(hs_ctx ctx, const double* A, const double* b, double* resu
     return HS_OK;
 }
 
+// the two matvec kernels with a caller-provided partial-sum buffer P of at
+// least nbi * nbj * bsz doubles; allocates nothing (hs_symv_block_noalloc)
+hs_status launch_symv_partials_at(hs_ctx ctx, const double* A, const double* b, double* result, int bi0, int bj0,
+                                  int nbi, int nbj, int reset, double* P, cudaStream_t s) {
+    if (nbi <= 0) return HS_OK;
+    const int bsz = ctx->bsz;
+    if (nbj > 0) {
+        const int64_t grid = (int64_t)nbi * nbj;
+        ctx->launches += 1;
+        if (bsz == 256)
+            symv_partials<256><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
+        else if (bsz == 128)
+            symv_partials<128><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
+        else
+            symv_partials<0><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
+        HS_CHECK_LAUNCH("symv_partials");
+    }
+    const int64_t rows = (int64_t)nbi * bsz;
+    int64_t rg64 = (rows + kThreads - 1) / kThreads;
+    if (rg64 > kMaxPartials) rg64 = kMaxPartials;
+    ctx->launches += 1;
+    symv_reduce<<<(unsigned)rg64, kThreads, 0, s>>>(P, result, bsz, bi0, nbi, nbj, reset, nullptr, nullptr);
+    HS_CHECK_LAUNCH("symv_reduce");
+    return HS_OK;
+}
+
 hs_status launch_column_update(hs_ctx ctx, const double* A, double* b, int blockStart, int blockCount, int blockRow,
                                int blockID, int transposed, cudaStream_t s) {
     if (blockCount <= 0) return HS_OK;

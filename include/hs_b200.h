@@ -144,6 +144,22 @@ hs_status hs_gemm_trailing(hs_ctx ctx, double* A, int blockID, int blockRow, int
 hs_status hs_symv_block(hs_ctx ctx, const double* A, const double* b, double* result, int blockStart_i,
                         int blockStart_j, int blockCount_i, int blockCount_j, int blockCountXY, int reset);
 
+/* No counterpart in the reference.  The same product as hs_symv_block, for callers
+ * that cannot let the library allocate device memory (an application whose own
+ * allocator already holds the free memory, or a latency-critical loop that cannot
+ * afford the device-wide synchronisation of cudaMalloc/cudaFree).  Its partial sums
+ * live in a fixed device array of HS_SYMV_NOALLOC_MAX_DOUBLES doubles (16 MiB) that
+ * every GPU loading the library holds until the process exits; no call allocates or
+ * frees anything.  A rectangle needing more than that
+ * (blockCount_i * blockCount_j * matrixBlockSize doubles) is rejected with
+ * HS_ERR_INVALID_ARG.  All calls on a device share the array, so calls whose
+ * kernels can overlap on that device race on it: order them on one stream.  The
+ * first call on each device looks up the array's device address (with that device
+ * current); make that first call before any stream capture starts. */
+#define HS_SYMV_NOALLOC_MAX_DOUBLES (2 * 1024 * 1024)
+hs_status hs_symv_block_noalloc(hs_ctx ctx, const double* A, const double* b, double* result, int blockStart_i,
+                                int blockStart_j, int blockCount_i, int blockCount_j, int blockCountXY, int reset);
+
 /* MatrixVectorOperations::triangularSolveBlockVector (MatrixVectorOperations.hpp:81;
  * .cpp:282-335): b_blockRow <- L^-1 b_blockRow (transposed: L^-T). */
 hs_status hs_trsv_block(hs_ctx ctx, const double* A, double* b, int blockRow, int blockID, int transposed);
