@@ -40,6 +40,14 @@ class SolveReport(ctypes.Structure):
                 ("factor_ms", ctypes.c_double), ("solve_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
 
 
+class MixedReport(ctypes.Structure):
+    _fields_ = [("refinement_steps", ctypes.c_int64), ("pcg_iterations", ctypes.c_int64),
+                ("fallback_pcg", ctypes.c_int), ("reserved", ctypes.c_int), ("backward_error", ctypes.c_double),
+                ("initial_backward_error", ctypes.c_double), ("norm_k_fro", ctypes.c_double),
+                ("logdet", ctypes.c_double), ("factor_ms", ctypes.c_double), ("refine_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double)]
+
+
 class KernelProfile(ctypes.Structure):
     _fields_ = [("launches", ctypes.c_int64), ("ms", ctypes.c_double), ("flops", ctypes.c_double),
                 ("bytes", ctypes.c_double)]
@@ -89,6 +97,8 @@ SIGNATURES = {
     "hs_cholesky_solve": [_P, _P, _P],
     "hs_cg_solve": [_P, _P, _P, _P, _D, _I64, ctypes.POINTER(_I64), ctypes.POINTER(_D), ctypes.POINTER(_D)],
     "hs_gp_solve_host": [_P, _P, _P, _I, _P, _I, _D, _D, _I, _D, _I64, _P, ctypes.POINTER(SolveReport)],
+    "hs_mixed_solve": [_P, _P, _P, _P, _I, _D, _I, ctypes.POINTER(MixedReport)],
+    "hs_cholesky_logdet": [_P, _P, ctypes.POINTER(_D)],
 }
 _RESTYPES = {"hs_abi_version": _I, "hs_last_error": ctypes.c_char_p, "hs_status_string": ctypes.c_char_p,
              "hs_packed_matrix_size": _I64, "hs_padded_vector_size": _I64, "hs_ctx_launch_count": _I64}

@@ -16,14 +16,17 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import HSError, NoConvergenceError, NotSPDError, SolveReport, call
+from ._lib import HSError, MixedReport, NoConvergenceError, NotSPDError, SolveReport, call
 
 __all__ = [
     "Context", "SymmetricMatrix", "RightHandSide", "MatrixOperations", "MatrixMatrixOperations",
     "MatrixVectorOperations", "VectorOperations", "Cholesky", "TriangularSystemSolver", "CG",
     "MatrixGenerator", "MatrixParser", "HSError", "NotSPDError", "NoConvergenceError", "block_id",
-    "packed_size", "padded_size", "gp_solve_host",
+    "packed_size", "padded_size", "gp_solve_host", "MixedPrecisionSolver", "cholesky_logdet", "PRECISIONS",
 ]
+
+# hs_precision
+PRECISIONS = {"fp64": 0, "tf32x3": 1, "bf16x3": 2}
 
 
 def block_id(i, j, nb):
@@ -389,6 +392,49 @@ class CG:
         if status != 4:  # reaching iMax is reported but, as in the reference, not an exception
             _lib.check(status)
         return self
+
+
+def cholesky_logdet(ctx, L):
+    """log|K| = 2 sum log diag(L) of a packed device factor from Cholesky."""
+    out = ctypes.c_double()
+    call("hs_cholesky_logdet", ctx.handle, _dptr(L, ctx), ctypes.byref(out))
+    return out.value
+
+
+class MixedPrecisionSolver:
+    """Mixed-precision solve of K x = b (no reference counterpart).
+
+    The factor runs in FP32 with the panel TRSM and SYRK/GEMM trailing updates
+    on the tensor cores as split products ("tf32x3": three TF32 products per
+    FP32 product) and every diagonal-block POTRF in FP64; FP64 iterative
+    refinement then drives the backward error ||b - K x|| / (||K||_F ||x||)
+    below ``tol``, continuing as CG preconditioned by the low-precision factor
+    when refinement stalls.  K (packed, device) is left unchanged.
+    """
+
+    def __init__(self, A, ctx, precision="tf32x3"):
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        self.A = A
+        self.ctx = ctx
+        self.precision = precision
+        self.report = None
+
+    def solve(self, b, tol=1e-14, max_steps=30, out=None):
+        """b: padded RHS (device tensor or RightHandSide); returns x (device)."""
+        ctx = self.ctx
+        ctx.set_problem(self.A.N, self.A.blockSize)
+        K = _to_device(self.A.matrixData, ctx)
+        bd = b.rightHandSideData if isinstance(b, RightHandSide) else b
+        bd = _to_device(bd, ctx)
+        x = out if out is not None else torch.empty_like(bd)
+        rep = MixedReport()
+        status = _lib.load().hs_mixed_solve(ctx.handle, _dptr(K, ctx), _dptr(bd, ctx), _dptr(x, ctx),
+                                            PRECISIONS[self.precision], float(tol), int(max_steps),
+                                            ctypes.byref(rep))
+        self.report = {f: getattr(rep, f) for f, _ in MixedReport._fields_ if f != "reserved"}
+        _lib.check(status)
+        return x
 
 
 class MatrixGenerator:

@@ -59,6 +59,8 @@ hs_status ensure_work(hs_ctx ctx, size_t bytes) {
 
 __global__ void set_i64_kernel(long long* p, long long v) { *p = v; }
 
+void set_i64_dev(long long* p, long long v, cudaStream_t s) { set_i64_kernel<<<1, 1, 0, s>>>(p, v); }
+
 static cudaEvent_t pool_get(hs_ctx ctx) {
     if (!ctx->prof_pool.empty()) {
         cudaEvent_t e = ctx->prof_pool.back();

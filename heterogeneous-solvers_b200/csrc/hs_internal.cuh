@@ -80,6 +80,7 @@ hs_status cuda_fail(cudaError_t e, const char* what);
     } while (0)
 
 hs_status require_ctx(hs_ctx ctx, const char* fn);
+void set_i64_dev(long long* p, long long v, cudaStream_t s);
 
 // per-kernel timing around one launch (no-ops unless ctx->profiling)
 void prof_begin(hs_ctx ctx, cudaStream_t s, int kernel);

@@ -1,0 +1,388 @@
+// hs_mixed.cu — mixed-precision solve: 3xTF32 tensor-core factor (k_mixed.cu),
+// FP64 iterative refinement to a backward-error target, and conjugate gradients
+// preconditioned by the low-precision factor when refinement stalls; plus the
+// log-determinant of a factor.
+//
+// No reference counterpart (new form).  Residuals r = b - K x use the FP64
+// packed K and the FP64 matvec; the triangular solves apply the FP32 factor
+// with FP64 arithmetic (FP64 diagonal blocks, FP32 off-diagonal blocks).
+#include <chrono>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "hs_internal.cuh"
+#include "hs_mixed.cuh"
+
+namespace hs {
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ double cta_sum2(double v, double* sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += sh[i];
+    return s;
+}
+
+// r = b - r (r holds K x on entry), partial sums of r.r and x.x
+__global__ void residual2_kernel(const double* __restrict__ b, double* __restrict__ r, const double* __restrict__ x,
+                                 int64_t n, double* __restrict__ part) {
+    __shared__ double sh[32];
+    double rr = 0.0, xx = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = b[i] - r[i];
+        r[i] = v;
+        rr += v * v;
+        xx += x[i] * x[i];
+    }
+    const double s1 = cta_sum2(rr, sh);
+    __syncthreads();
+    const double s2 = cta_sum2(xx, sh);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = s1;
+        part[2 * blockIdx.x + 1] = s2;
+    }
+}
+
+__global__ void sum_pairs_kernel(const double* __restrict__ part, int n, double* __restrict__ out) {
+    __shared__ double sh[32];
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        a += part[2 * i];
+        b += part[2 * i + 1];
+    }
+    const double s1 = cta_sum2(a, sh);
+    __syncthreads();
+    const double s2 = cta_sum2(b, sh);
+    if (threadIdx.x == 0) {
+        out[0] = s1;
+        out[1] = s2;
+    }
+}
+
+// squared Frobenius norm of the packed symmetric matrix (off-diagonal blocks twice)
+__global__ void fro2_kernel(const double* __restrict__ A, int bsz, int nb, int64_t T, double* __restrict__ part) {
+    __shared__ double sh[32];
+    double acc = 0.0;
+    const int64_t bb = (int64_t)bsz * bsz;
+    for (int64_t blk = blockIdx.x; blk < T; blk += gridDim.x) {
+        int bi, bj;
+        block_coords(blk, nb, &bi, &bj);
+        const double w = (bi == bj) ? 1.0 : 2.0;
+        double s = 0.0;
+        for (int64_t e = threadIdx.x; e < bb; e += blockDim.x) {
+            const double v = A[blk * bb + e];
+            s += v * v;
+        }
+        acc += w * s;
+    }
+    const double t = cta_sum2(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void sum_kernel(const double* __restrict__ part, int n, double* __restrict__ out) {
+    __shared__ double sh[32];
+    double a = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a += part[i];
+    const double s = cta_sum2(a, sh);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// sum of log(diag) over the valid rows of the diagonal blocks (blocks at `ids`
+// or, when ids == nullptr, nb consecutive blocks)
+__global__ void logdiag_kernel(const double* __restrict__ L, int bsz, int nb, int64_t N, int consecutive,
+                               double* __restrict__ out) {
+    __shared__ double sh[32];
+    double acc = 0.0;
+    const int64_t bb = (int64_t)bsz * bsz;
+    for (int64_t i = threadIdx.x; i < N; i += blockDim.x) {
+        const int k = (int)(i / bsz), r = (int)(i % bsz);
+        const int64_t id = consecutive ? k : block_id(k, k, nb);
+        acc += log(L[id * bb + (int64_t)r * bsz + r]);
+    }
+    const double s = cta_sum2(acc, sh);
+    if (threadIdx.x == 0) *out = 2.0 * s;
+}
+
+// x += d
+__global__ void add_kernel(double* __restrict__ x, const double* __restrict__ d, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] += d[i];
+}
+
+int grid_n(int64_t n, int sms) {
+    int64_t g = (n + kThreads - 1) / kThreads;
+    if (g > 4LL * sms) g = 4LL * sms;
+    return (int)(g < 1 ? 1 : g);
+}
+
+struct Dev {
+    void* p = nullptr;
+    ~Dev() {
+        if (p) cudaFree(p);
+    }
+};
+
+}  // namespace
+
+// b <- (L L^T)^-1 b with the mixed factor: FP64 diagonal blocks, FP32 off-diagonal blocks
+hs_status mixed_apply(hs_ctx ctx, const MixedWork& w, double* b, cudaStream_t s) {
+    const int nb = ctx->nb;
+    const int64_t T = total_blocks(nb);
+    for (int j = 0; j < nb; ++j) {
+        const int right = nb - j;
+        const int blockID = (int)(T - (int64_t)right * (right + 1) / 2);
+        hs_status st = launch_trsv(ctx, w.Ld, b, j, j, 0, s);
+        if (st != HS_OK) return st;
+        if (j < nb - 1) {
+            st = launch_column_update_f32(ctx, w.A32, b, j + 1, nb - (j + 1), j, blockID, 0, s);
+            if (st != HS_OK) return st;
+        }
+    }
+    for (int j = nb - 1; j >= 0; --j) {
+        const int right = nb - j;
+        const int blockID = (int)(T - (int64_t)right * (right + 1) / 2);
+        hs_status st = launch_trsv(ctx, w.Ld, b, j, j, 1, s);
+        if (st != HS_OK) return st;
+        if (j > 0) {
+            st = launch_column_update_f32(ctx, w.A32, b, 0, j, j, blockID, 1, s);
+            if (st != HS_OK) return st;
+        }
+    }
+    return HS_OK;
+}
+
+}  // namespace hs
+
+using namespace hs;
+
+extern "C" {
+
+hs_status hs_cholesky_logdet(hs_ctx ctx, const double* L, double* logdet) {
+    hs_status st = require_ctx(ctx, "hs_cholesky_logdet");
+    if (st != HS_OK) return st;
+    if (!L || !logdet) {
+        set_error("hs_cholesky_logdet: null pointer");
+        return HS_ERR_INVALID_ARG;
+    }
+    st = ensure_scratch(ctx, kSmallScratch);
+    if (st != HS_OK) return st;
+    double* out = reinterpret_cast<double*>(static_cast<char*>(ctx->scratch) + kScalarOffset) + 8;
+    ctx->launches += 1;
+    logdiag_kernel<<<1, 1024, 0, ctx->stream>>>(L, ctx->bsz, ctx->nb, ctx->N, 0, out);
+    HS_CHECK_LAUNCH("logdet");
+    HS_CUDA(cudaMemcpyAsync(logdet, out, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HS_OK;
+}
+
+hs_status hs_mixed_solve(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,
+                         int max_steps, hs_mixed_report* rep) {
+    hs_status st = require_ctx(ctx, "hs_mixed_solve");
+    if (st != HS_OK) return st;
+    if (!K || !b || !x) {
+        set_error("hs_mixed_solve: null pointer");
+        return HS_ERR_INVALID_ARG;
+    }
+    if (precision != HS_PRECISION_TF32X3) {
+        set_error("hs_mixed_solve: only HS_PRECISION_TF32X3 is implemented");
+        return HS_ERR_UNSUPPORTED;
+    }
+    if (!(tol > 0.0) || max_steps < 1) {
+        set_error("hs_mixed_solve: tol must be > 0 and max_steps >= 1");
+        return HS_ERR_INVALID_ARG;
+    }
+    cudaStream_t s = ctx->stream;
+    const int nb = ctx->nb, bsz = ctx->bsz;
+    const int64_t n = (int64_t)nb * bsz;
+    const auto t0 = std::chrono::steady_clock::now();
+    hs_mixed_report R{};
+    // workspace: factor + 5 vectors
+    Dev ws, vec;
+    HS_CUDA(cudaMalloc(&ws.p, mixed_workspace_bytes(ctx->N, bsz)));
+    HS_CUDA(cudaMalloc(&vec.p, (size_t)5 * n * sizeof(double)));
+    double* r = static_cast<double*>(vec.p);
+    double* d = r + n;
+    double* p = d + n;
+    double* q = p + n;
+    double* z = q + n;
+    MixedWork w;
+    st = mixed_bind(ctx, ws.p, &w);
+    if (st != HS_OK) return st;
+    st = ensure_scratch(ctx, kSmallScratch + (size_t)nb * nb * bsz * sizeof(double));
+    if (st != HS_OK) return st;
+    double* part = static_cast<double*>(ctx->scratch);
+    double* scal = reinterpret_cast<double*>(static_cast<char*>(ctx->scratch) + kScalarOffset) + 16;
+    volatile double* h = ctx->h_pinned;
+    const int g = grid_n(n, ctx->num_sms);
+
+    // ||K||_F
+    {
+        const int64_t T = total_blocks(nb);
+        const int fg = (int)(T < 1024 ? T : 1024);
+        ctx->launches += 2;
+        fro2_kernel<<<fg, kThreads, 0, s>>>(K, bsz, nb, T, part);
+        sum_kernel<<<1, kThreads, 0, s>>>(part, fg, scal);
+        HS_CHECK_LAUNCH("fro2");
+        HS_CUDA(cudaMemcpyAsync((void*)(h + 8), scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        HS_CUDA(cudaStreamSynchronize(s));
+        R.norm_k_fro = std::sqrt(h[8]);
+    }
+    // factor (a non-positive FP64 pivot of the FP32 matrix is recorded in ctx->d_info)
+    cudaEvent_t e0, e1, e2;
+    HS_CUDA(cudaEventCreate(&e0));
+    HS_CUDA(cudaEventCreate(&e1));
+    HS_CUDA(cudaEventCreate(&e2));
+    HS_CUDA(cudaEventRecord(e0, s));
+    ctx->launches += 1;
+    {
+        long long* info = ctx->d_info;
+        set_i64_dev(info, INT64_MAX, s);
+    }
+    st = mixed_factor(ctx, K, w, s);
+    if (st != HS_OK) return st;
+    HS_CUDA(cudaEventRecord(e1, s));
+    HS_CUDA(cudaStreamSynchronize(s));
+    st = mixed_check_error(ctx, w);
+    if (st != HS_OK) return st;
+    int64_t info = -1;
+    st = hs_ctx_take_info(ctx, &info);
+    if (st != HS_OK) return st;
+    if (info >= 0) {
+        set_error("hs_mixed_solve: the FP32 factor met a non-positive pivot at row " + std::to_string(info) +
+                  " (matrix too ill-conditioned for the low-precision factor)");
+        return HS_ERR_NOT_SPD;
+    }
+    // log|K| from the FP64 diagonal blocks
+    ctx->launches += 1;
+    logdiag_kernel<<<1, 1024, 0, s>>>(w.Ld, bsz, nb, ctx->N, 1, scal + 2);
+    HS_CHECK_LAUNCH("logdet");
+
+    auto residual = [&](double* rnorm, double* xnorm) -> hs_status {
+        // r = b - K x, ||r||, ||x||
+        hs_status s2 = launch_symv(ctx, K, x, r, 0, 0, nb, nb, 1, nullptr, nullptr, s);
+        if (s2 != HS_OK) return s2;
+        ctx->launches += 2;
+        residual2_kernel<<<g, kThreads, 0, s>>>(b, r, x, n, part);
+        sum_pairs_kernel<<<1, kThreads, 0, s>>>(part, g, scal + 4);
+        HS_CHECK_LAUNCH("residual");
+        HS_CUDA(cudaMemcpyAsync((void*)(h + 10), scal + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        HS_CUDA(cudaStreamSynchronize(s));
+        *rnorm = std::sqrt(h[10]);
+        *xnorm = std::sqrt(h[11]);
+        return HS_OK;
+    };
+    // x0 = M^-1 b
+    HS_CUDA(cudaMemcpyAsync(x, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    st = mixed_apply(ctx, w, x, s);
+    if (st != HS_OK) return st;
+    double rn = 0, xn = 0, prev = INFINITY;
+    int stalls = 0;
+    bool converged = false;
+    int steps = 0;
+    for (; steps < max_steps; ++steps) {
+        st = residual(&rn, &xn);
+        if (st != HS_OK) return st;
+        R.backward_error = rn / (R.norm_k_fro * xn);
+        if (steps == 0) R.initial_backward_error = R.backward_error;
+        if (R.backward_error <= tol) {
+            converged = true;
+            break;
+        }
+        if (rn > 0.5 * prev) {
+            if (++stalls >= 2) break;
+        } else {
+            stalls = 0;
+        }
+        prev = rn;
+        // d = M^-1 r; x += d
+        HS_CUDA(cudaMemcpyAsync(d, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        st = mixed_apply(ctx, w, d, s);
+        if (st != HS_OK) return st;
+        ctx->launches += 1;
+        add_kernel<<<g, kThreads, 0, s>>>(x, d, n);
+        HS_CHECK_LAUNCH("refine add");
+    }
+    R.refinement_steps = steps;
+    if (!converged) {
+        // conjugate gradients preconditioned by the low-precision factor, from the current x
+        R.fallback_pcg = 1;
+        st = residual(&rn, &xn);  // r = b - K x
+        if (st != HS_OK) return st;
+        HS_CUDA(cudaMemcpyAsync(z, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        st = mixed_apply(ctx, w, z, s);
+        if (st != HS_OK) return st;
+        HS_CUDA(cudaMemcpyAsync(p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        st = launch_dot(ctx, r, z, scal + 6, 0, n, s);
+        if (st != HS_OK) return st;
+        HS_CUDA(cudaMemcpyAsync((void*)(h + 12), scal + 6, sizeof(double), cudaMemcpyDeviceToHost, s));
+        HS_CUDA(cudaStreamSynchronize(s));
+        double rho = h[12];
+        const int max_pcg = 50 * max_steps + 200;
+        int it = 0;
+        for (; it < max_pcg; ++it) {
+            st = launch_symv(ctx, K, p, q, 0, 0, nb, nb, 1, p, scal + 7, s);  // q = K p, p.q
+            if (st != HS_OK) return st;
+            HS_CUDA(cudaMemcpyAsync((void*)(h + 13), scal + 7, sizeof(double), cudaMemcpyDeviceToHost, s));
+            HS_CUDA(cudaStreamSynchronize(s));
+            const double alpha = rho / h[13];
+            if ((st = launch_vec(ctx, 3, x, p, alpha, x, 0, n, s)) != HS_OK) return st;
+            if ((st = launch_vec(ctx, 3, r, q, -alpha, r, 0, n, s)) != HS_OK) return st;
+            if ((it + 1) % 10 == 0) {
+                st = residual(&rn, &xn);  // true residual keeps r honest
+                if (st != HS_OK) return st;
+            } else {
+                if ((st = launch_dot(ctx, r, r, scal + 8, 0, n, s)) != HS_OK) return st;
+                if ((st = launch_dot(ctx, x, x, scal + 9, 0, n, s)) != HS_OK) return st;
+                HS_CUDA(cudaMemcpyAsync((void*)(h + 14), scal + 8, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+                HS_CUDA(cudaStreamSynchronize(s));
+                rn = std::sqrt(h[14]);
+                xn = std::sqrt(h[15]);
+            }
+            R.backward_error = rn / (R.norm_k_fro * xn);
+            if (R.backward_error <= tol) {
+                converged = true;
+                ++it;
+                break;
+            }
+            HS_CUDA(cudaMemcpyAsync(z, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            if ((st = mixed_apply(ctx, w, z, s)) != HS_OK) return st;
+            if ((st = launch_dot(ctx, r, z, scal + 6, 0, n, s)) != HS_OK) return st;
+            HS_CUDA(cudaMemcpyAsync((void*)(h + 12), scal + 6, sizeof(double), cudaMemcpyDeviceToHost, s));
+            HS_CUDA(cudaStreamSynchronize(s));
+            const double rho_new = h[12];
+            const double beta = rho_new / rho;
+            rho = rho_new;
+            if ((st = launch_vec(ctx, 3, z, p, beta, p, 0, n, s)) != HS_OK) return st;
+        }
+        R.pcg_iterations = it;
+    }
+    HS_CUDA(cudaEventRecord(e2, s));
+    HS_CUDA(cudaMemcpyAsync((void*)(h + 16), scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
+    HS_CUDA(cudaStreamSynchronize(s));
+    R.logdet = h[16];
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    R.factor_ms = ms;
+    cudaEventElapsedTime(&ms, e1, e2);
+    R.refine_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    R.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (rep) *rep = R;
+    if (!converged) {
+        set_error("hs_mixed_solve: backward error " + std::to_string(R.backward_error) + " above the target " +
+                  std::to_string(tol) + " after refinement and preconditioned CG");
+        return HS_ERR_REFINEMENT_STALLED;
+    }
+    return HS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,34 @@
+// hs_mixed.cuh — internals shared by the mixed-precision factor (k_mixed.cu)
+// and its refinement / preconditioned-CG drivers (hs_mixed.cu).
+#pragma once
+
+#include <cuda.h>
+
+#include "hs_internal.cuh"
+
+namespace hs {
+
+// device workspace of one mixed-precision factorization
+struct MixedWork {
+    float* A32 = nullptr;   // packed FP32 copy of K, overwritten by L (off-diagonal blocks used by the solves)
+    float* LO = nullptr;    // low parts: panel blocks 0..nb-1, slots nb / nb+1 = L_kk^-1 hi / lo
+    double* Ld = nullptr;   // FP64 diagonal blocks of L (nb blocks)
+    double* S = nullptr;    // FP64 scratch block (POTRF)
+    double* Y = nullptr;    // FP64 scratch block (L_kk^-T)
+    int* err = nullptr;     // tensor-core tile timeout flag
+    CUtensorMap mA128, mAB, mL128, mLB;
+};
+
+size_t mixed_workspace_bytes(int64_t N, int bsz);
+hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w);
+hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s);
+hs_status mixed_check_error(hs_ctx ctx, const MixedWork& w);
+
+// TRSM of `items` bsz x bsz FP64 blocks stored contiguously at B against the
+// lower triangle L (bsz x bsz): B <- B L^-T
+hs_status launch_trsm_on(hs_ctx ctx, const double* L, int n, double* B, int items, cudaStream_t s);
+// column update reading FP32 blocks (accumulation in FP64)
+hs_status launch_column_update_f32(hs_ctx ctx, const float* A32, double* b, int blockStart, int blockCount,
+                                   int blockRow, int blockID, int transposed, cudaStream_t s);
+
+}  // namespace hs

@@ -14,6 +14,7 @@
 // result is C - sum_k a_ik b_jk accumulated in k order.  Other block sizes use
 // a scalar fallback with the reference's accumulation order.
 #include "hs_internal.cuh"
+#include "hs_mixed.cuh"
 
 namespace hs {
 namespace {
@@ -442,6 +443,13 @@ hs_status launch_trsm(hs_ctx ctx, double* A, int blockID, int blockRow, int bloc
     st = launch_trsm_args(ctx, ta, blockCount, s);
     prof_end(ctx, s, HS_KERNEL_TRSM, blockCount * n * n * n, (2.0 * blockCount + 1.0) * n * n * 8.0);
     return st;
+}
+
+hs_status launch_trsm_on(hs_ctx ctx, const double* L, int n, double* B, int items, cudaStream_t s) {
+    hs_status st = set_attrs();
+    if (st != HS_OK) return st;
+    TrsmArgs ta{L, n, n, B, n, 0, (n + kTrsmRows - 1) / kTrsmRows, n, (int64_t)n * n};
+    return launch_trsm_args(ctx, ta, items, s);
 }
 
 hs_status launch_update(hs_ctx ctx, double* A, int blockID, int blockRow, int syrkStart, int syrkCount,

@@ -1,0 +1,441 @@
+// k_mixed.cu — mixed-precision blocked Cholesky: FP32 factor whose panel TRSM
+// and SYRK/GEMM trailing updates run on the 5th-generation tensor cores
+// (tcgen05, kind::tf32) as 3xTF32 split products with FP32 accumulation in
+// TMEM, while every diagonal-block POTRF runs in FP64.
+//
+// No reference counterpart (the reference factors in FP64 or FP32 only,
+// src/utility/Configuration.hpp:14-19); the block structure is the reference's
+// right-looking algorithm (src/solver/cholesky/Cholesky.cpp:446-471).
+//
+// Split products: an FP32 operand a is read by the tensor core as TF32
+// (its top 19 bits), a_hi; a_lo = a - a_hi is exact in FP32 and kept in a
+// second buffer.  a*b ~ a_hi*b_hi + a_hi*b_lo + a_lo*b_hi: three MMAs per
+// k-step, accumulated in FP32, relative error ~2^-21 instead of TF32's 2^-11.
+//
+// Kernel structure (one 128 x bsz output tile per CTA, 4 warps):
+//   thread 0   TMA producer: A_hi, A_lo (128 x 32 FP32) and B_hi, B_lo
+//              (bsz x 32 FP32) per K slab, 128-byte swizzle, 2-stage ring
+//   thread 32  MMA issuer: 3 x 4 tcgen05.mma (K = 8 each) per slab, commit to
+//              the stage's "empty" barrier and finally to "done"
+//   all warps  epilogue: TMEM -> registers (warp w owns lanes 32w..32w+31 =
+//              tile rows), C -= D (update) or L = D, L_lo = D - tf32(D) (TRSM)
+// Every mbarrier wait is bounded (2 s); on expiry the CTA records an error in
+// the context's flag word, frees its TMEM and returns.
+#include <cudaTypedefs.h>
+
+#include "hs_internal.cuh"
+#include "hs_mixed.cuh"
+#include "tc_common.cuh"
+
+namespace hs {
+namespace {
+
+using namespace tc;
+
+constexpr int kTcThreads = 128;
+constexpr int kSlab = 32;               // K elements (FP32) per stage = 128 bytes
+constexpr uint64_t kWaitNs = 2000000000ull;
+
+enum { MODE_UPDATE = 0, MODE_TRSM = 1 };
+
+struct TcArgs {
+    float* A32;        // packed FP32 working matrix
+    float* LO;         // low parts: panel blocks 0..m-1, slot nb = L_kk^-T hi, nb+1 = lo
+    int64_t blockID;   // id of the diagonal block of column k
+    int k, nb;
+    int64_t gemmPairs, pairBase;  // MODE_UPDATE: GEMM pairs c < r, rows k+2..
+    int syrkStart;
+    int64_t totalPairs;
+    int* err;          // error flag (timeouts)
+};
+
+template <int BSZ>
+struct TcSmem {
+    static constexpr int kTiles = BSZ / 128;               // 128-row tiles per block
+    static constexpr int kABytes = 128 * kSlab * 4;        // 16 KB
+    static constexpr int kBBytes = BSZ * kSlab * 4;        // 16 / 32 KB
+    static constexpr int kStage = 2 * kABytes + 2 * kBBytes;
+    static constexpr int kStages = 2;
+    static constexpr int kBytes = kStages * kStage + 1024 /* barriers, slot */ + 1024 /* alignment */;
+};
+
+template <int BSZ, int MODE>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    tc_tile_kernel(const __grid_constant__ CUtensorMap mA128, const __grid_constant__ CUtensorMap mAB,
+                   const __grid_constant__ CUtensorMap mL128, const __grid_constant__ CUtensorMap mLB, TcArgs a) {
+    using SM = TcSmem<BSZ>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + SM::kStages * SM::kStage);
+    uint64_t* empty = full + SM::kStages;
+    uint64_t* done = empty + SM::kStages;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const size_t bb = (size_t)BSZ * BSZ;
+
+    // ---- tile decode
+    const int ti = (int)(blockIdx.x % SM::kTiles);
+    const int64_t item = blockIdx.x / SM::kTiles;
+    int r, c;
+    if (MODE == MODE_TRSM) {
+        r = a.k + 1 + (int)item;
+        c = a.k;
+    } else if (item < a.gemmPairs) {
+        const int64_t t = item + a.pairBase;
+        const int u = tri_root(t);
+        r = a.k + 1 + (u + 1);
+        c = a.k + 1 + (int)(t - (int64_t)u * (u + 1) / 2);
+    } else {
+        r = c = a.syrkStart + (int)(item - a.gemmPairs);
+    }
+    // operand coordinates: (column, row, block) in the TMA maps
+    const int blkA = (int)(a.blockID + (r - a.k));  // panel block of row r
+    const int gA = r - a.k - 1;                     // its low-part slot
+    const int blkB = (MODE == MODE_TRSM) ? a.nb : (int)(a.blockID + (c - a.k));
+    const int gB = (MODE == MODE_TRSM) ? a.nb + 1 : c - a.k - 1;
+
+    if (tid == 0) {
+        for (int s = 0; s < SM::kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        fence_barrier_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(tslot, BSZ);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t taddr = *tslot;
+    const uint64_t deadline = globaltimer_ns() + kWaitNs;
+    bool ok = true;
+    constexpr int kSlabs = BSZ / kSlab;
+
+    if (tid == 0) {
+        // ---- producer
+        for (int kc = 0; kc < kSlabs && ok; ++kc) {
+            const int s = kc % SM::kStages, use = kc / SM::kStages;
+            if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, deadline)) { ok = false; break; }
+            uint8_t* st = smem + s * SM::kStage;
+            mbar_arrive_expect_tx(&full[s], SM::kStage);
+            tma_load_3d(st, &mA128, &full[s], kc * kSlab, ti * 128, blkA);
+            tma_load_3d(st + SM::kABytes, &mL128, &full[s], kc * kSlab, ti * 128, gA);
+            if (MODE == MODE_TRSM) {
+                tma_load_3d(st + 2 * SM::kABytes, &mLB, &full[s], kc * kSlab, 0, blkB);
+            } else {
+                tma_load_3d(st + 2 * SM::kABytes, &mAB, &full[s], kc * kSlab, 0, blkB);
+            }
+            tma_load_3d(st + 2 * SM::kABytes + SM::kBBytes, &mLB, &full[s], kc * kSlab, 0, gB);
+        }
+        if (!ok) atomicExch(a.err, 1);
+    } else if (tid == 32) {
+        // ---- MMA issuer
+        constexpr uint32_t idesc = umma_idesc(kFmtTF32, kFmtTF32, 128, BSZ);
+        for (int kc = 0; kc < kSlabs; ++kc) {
+            const int s = kc % SM::kStages, use = kc / SM::kStages;
+            if (!mbar_wait(&full[s], use & 1, deadline)) { ok = false; break; }
+            tc_fence_after();
+            const uint32_t base = smem_u32(smem + s * SM::kStage);
+            const uint32_t aHi = base, aLo = base + SM::kABytes;
+            const uint32_t bHi = base + 2 * SM::kABytes, bLo = bHi + SM::kBBytes;
+#pragma unroll
+            for (int ks = 0; ks < kSlab / 8; ++ks) {
+                const uint32_t off = ks * 32;  // 8 TF32 = 32 bytes along K
+                const uint64_t dAh = umma_desc_sw128(aHi + off), dAl = umma_desc_sw128(aLo + off);
+                const uint64_t dBh = umma_desc_sw128(bHi + off), dBl = umma_desc_sw128(bLo + off);
+                umma_tf32(taddr, dAh, dBh, idesc, (kc | ks) != 0);
+                umma_tf32(taddr, dAh, dBl, idesc, 1);
+                umma_tf32(taddr, dAl, dBh, idesc, 1);
+            }
+            umma_commit(&empty[s]);
+        }
+        if (ok) umma_commit(done);
+        else atomicExch(a.err, 1);
+    }
+    __syncwarp();
+
+    // ---- epilogue: all 4 warps, thread = tile row
+    int wok = 0;
+    if (lane == 0) wok = mbar_wait(done, 0, deadline) ? 1 : 0;
+    const bool done_ok = __shfl_sync(0xffffffffu, wok, 0) != 0;
+    __syncwarp();
+    tc_fence_after();
+    if (!done_ok) {
+        if (lane == 0) atomicExch(a.err, 1);
+    } else {
+        const int row = warp * 32 + lane;
+        float* outp;
+        float* lop = nullptr;
+        if (MODE == MODE_TRSM) {
+            outp = a.A32 + (size_t)blkA * bb + (size_t)(ti * 128 + row) * BSZ;
+            lop = a.LO + (size_t)gA * bb + (size_t)(ti * 128 + row) * BSZ;
+        } else {
+            outp = a.A32 + (size_t)block_id(r, c, a.nb) * bb + (size_t)(ti * 128 + row) * BSZ;
+        }
+#pragma unroll 1
+        for (int j = 0; j < BSZ / 32; ++j) {
+            uint32_t v[32];
+            tmem_ld_32x32b_x32(taddr + ((uint32_t)(warp * 32) << 16) + j * 32, v);
+            tmem_ld_wait();
+            float4* o4 = reinterpret_cast<float4*>(outp + j * 32);
+            if (MODE == MODE_UPDATE) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    float4 cv = o4[q];
+                    cv.x -= __uint_as_float(v[4 * q + 0]);
+                    cv.y -= __uint_as_float(v[4 * q + 1]);
+                    cv.z -= __uint_as_float(v[4 * q + 2]);
+                    cv.w -= __uint_as_float(v[4 * q + 3]);
+                    o4[q] = cv;
+                }
+            } else {
+                float4* l4 = reinterpret_cast<float4*>(lop + j * 32);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const float x0 = __uint_as_float(v[4 * q + 0]), x1 = __uint_as_float(v[4 * q + 1]);
+                    const float x2 = __uint_as_float(v[4 * q + 2]), x3 = __uint_as_float(v[4 * q + 3]);
+                    o4[q] = make_float4(x0, x1, x2, x3);
+                    l4[q] = make_float4(x0 - tf32_trunc(x0), x1 - tf32_trunc(x1), x2 - tf32_trunc(x2),
+                                        x3 - tf32_trunc(x3));
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(taddr, BSZ);
+}
+
+// ------------------------------------------------------------------ helpers
+__global__ void f64_to_f32_kernel(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
+    const int64_t n2 = n / 2;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = __ldcs(reinterpret_cast<const double2*>(in) + i);
+        reinterpret_cast<float2*>(out)[i] = make_float2((float)v.x, (float)v.y);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) out[n - 1] = (float)in[n - 1];
+}
+
+// lo[i] = a[i] - tf32(a[i]) over n floats
+__global__ void lo_part_kernel(const float* __restrict__ a, float* __restrict__ lo, int64_t n4) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+        const float4 v = reinterpret_cast<const float4*>(a)[i];
+        reinterpret_cast<float4*>(lo)[i] =
+            make_float4(v.x - tf32_trunc(v.x), v.y - tf32_trunc(v.y), v.z - tf32_trunc(v.z), v.w - tf32_trunc(v.w));
+    }
+}
+
+// S (FP64, bsz x bsz) = A32 diagonal block; T (FP64) = identity
+__global__ void diag_in_kernel(const float* __restrict__ blk, double* __restrict__ S, double* __restrict__ I,
+                               int bsz) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < bsz * bsz; e += gridDim.x * blockDim.x) {
+        S[e] = (double)blk[e];
+        I[e] = (e / bsz == e % bsz) ? 1.0 : 0.0;
+    }
+}
+
+// after POTRF(S) and Y = I L^-T (= (L^-1)^T): A32 diagonal block = float(L),
+// Ldiag64[k] = L, LO[nb] = hi of L^-1 (row-major, i.e. Y transposed), LO[nb+1] = lo
+__global__ void diag_out_kernel(const double* __restrict__ S, const double* __restrict__ Y, float* __restrict__ blk,
+                                double* __restrict__ Ld, float* __restrict__ invHi, float* __restrict__ invLo,
+                                int bsz) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < bsz * bsz; e += gridDim.x * blockDim.x) {
+        const int i = e / bsz, j = e % bsz;
+        blk[e] = (float)S[e];
+        Ld[e] = S[e];
+        const float y = (float)Y[(size_t)j * bsz + i];  // (L^-1)[i][j] = Y[j][i]
+        invHi[e] = y;
+        invLo[e] = y - tf32_trunc(y);
+    }
+}
+
+__global__ void set_int_kernel(int* p, int v) { *p = v; }
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+hs_status get_encoder() {
+    if (g_encode) return HS_OK;
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    HS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !fn) {
+        set_error("cuTensorMapEncodeTiled is not available from the driver");
+        return HS_ERR_UNSUPPORTED;
+    }
+    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    return HS_OK;
+}
+
+// 3-D FP32 map over `blocks` blocks of bsz x bsz, box = 32 columns x box_rows rows x 1 block
+hs_status make_map(CUtensorMap* m, float* base, int bsz, int64_t blocks, int box_rows) {
+    hs_status st = get_encoder();
+    if (st != HS_OK) return st;
+    cuuint64_t dims[3] = {(cuuint64_t)bsz, (cuuint64_t)bsz, (cuuint64_t)blocks};
+    cuuint64_t strides[2] = {(cuuint64_t)bsz * 4, (cuuint64_t)bsz * bsz * 4};
+    cuuint32_t box[3] = {(cuuint32_t)kSlab, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+        return HS_ERR_CUDA;
+    }
+    return HS_OK;
+}
+
+template <int BSZ>
+hs_status tc_launch(hs_ctx ctx, int mode, const MixedWork& w, TcArgs a, int64_t items, cudaStream_t s) {
+    using SM = TcSmem<BSZ>;
+    const int64_t grid = items * SM::kTiles;
+    if (grid <= 0) return HS_OK;
+    HS_REQUIRE(grid < (1LL << 31), "too many tiles");
+    ctx->launches += 1;
+    if (mode == MODE_TRSM)
+        tc_tile_kernel<BSZ, MODE_TRSM><<<(unsigned)grid, kTcThreads, SM::kBytes, s>>>(w.mA128, w.mAB, w.mL128,
+                                                                                     w.mLB, a);
+    else
+        tc_tile_kernel<BSZ, MODE_UPDATE><<<(unsigned)grid, kTcThreads, SM::kBytes, s>>>(w.mA128, w.mAB, w.mL128,
+                                                                                       w.mLB, a);
+    HS_CHECK_LAUNCH("tc_tile_kernel");
+    return HS_OK;
+}
+
+bool g_tc_attr[64][2] = {};
+
+template <int BSZ>
+hs_status tc_attrs() {
+    int dev = 0;
+    HS_CUDA(cudaGetDevice(&dev));
+    const int slot = BSZ == 256 ? 1 : 0;
+    if (dev < 64 && g_tc_attr[dev][slot]) return HS_OK;
+    HS_CUDA(cudaFuncSetAttribute(tc_tile_kernel<BSZ, MODE_TRSM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TcSmem<BSZ>::kBytes));
+    HS_CUDA(cudaFuncSetAttribute(tc_tile_kernel<BSZ, MODE_UPDATE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TcSmem<BSZ>::kBytes));
+    if (dev < 64) g_tc_attr[dev][slot] = true;
+    return HS_OK;
+}
+
+int grid_for_elems(int64_t n, int num_sms) {
+    int64_t g = (n + 255) / 256;
+    if (g > 8LL * num_sms) g = 8LL * num_sms;
+    return (int)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+size_t mixed_workspace_bytes(int64_t N, int bsz) {
+    const int64_t nb = (N + bsz - 1) / bsz;
+    const size_t bb = (size_t)bsz * bsz;
+    const size_t T = (size_t)(nb * (nb + 1) / 2);
+    size_t bytes = 0;
+    bytes += T * bb * 4;                 // A32 / L32
+    bytes += (size_t)(nb + 2) * bb * 4;  // LO
+    bytes += (size_t)nb * bb * 8;        // Ldiag64
+    bytes += 2 * bb * 8;                 // S, I/Y
+    bytes += 1024;                       // flags
+    return bytes;
+}
+
+hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
+    const int bsz = ctx->bsz, nb = ctx->nb;
+    const size_t bb = (size_t)bsz * bsz;
+    const size_t T = total_blocks(nb);
+    char* p = static_cast<char*>(ws);
+    w->A32 = reinterpret_cast<float*>(p);
+    p += T * bb * 4;
+    w->LO = reinterpret_cast<float*>(p);
+    p += (size_t)(nb + 2) * bb * 4;
+    w->Ld = reinterpret_cast<double*>(p);
+    p += (size_t)nb * bb * 8;
+    w->S = reinterpret_cast<double*>(p);
+    p += bb * 8;
+    w->Y = reinterpret_cast<double*>(p);
+    p += bb * 8;
+    w->err = reinterpret_cast<int*>(p);
+    hs_status st = make_map(&w->mA128, w->A32, bsz, (int64_t)T, 128);
+    if (st == HS_OK) st = make_map(&w->mAB, w->A32, bsz, (int64_t)T, bsz);
+    if (st == HS_OK) st = make_map(&w->mL128, w->LO, bsz, nb + 2, 128);
+    if (st == HS_OK) st = make_map(&w->mLB, w->LO, bsz, nb + 2, bsz);
+    return st;
+}
+
+hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s) {
+    const int bsz = ctx->bsz, nb = ctx->nb;
+    HS_REQUIRE(bsz == 128 || bsz == 256, "the mixed-precision factor supports matrixBlockSize 128 or 256");
+    hs_status st = bsz == 256 ? tc_attrs<256>() : tc_attrs<128>();
+    if (st != HS_OK) return st;
+    const size_t bb = (size_t)bsz * bsz;
+    const int64_t T = total_blocks(nb);
+    ctx->launches += 2;
+    set_int_kernel<<<1, 1, 0, s>>>(w.err, 0);
+    f64_to_f32_kernel<<<grid_for_elems(T * (int64_t)bb / 2, ctx->num_sms), 256, 0, s>>>(K64, w.A32, T * (int64_t)bb);
+    HS_CHECK_LAUNCH("f64_to_f32");
+    // the factor works on a temporary context view whose "matrix" is the FP64 scratch block S
+    for (int k = 0; k < nb; ++k) {
+        const int right = nb - k;
+        const int64_t blockID = T - (int64_t)right * (right + 1) / 2;
+        float* dblk = w.A32 + (size_t)blockID * bb;
+        // diagonal block in FP64: POTRF, then Y = L^-T by TRSM on the identity
+        ctx->launches += 1;
+        diag_in_kernel<<<64, 256, 0, s>>>(dblk, w.S, w.Y, bsz);
+        st = launch_potrf(ctx, w.S, 0, k, s);  // block 0 of the scratch, guard rows of block row k
+        if (st != HS_OK) return st;
+        st = launch_trsm_on(ctx, w.S, bsz, w.Y, 1, s);
+        if (st != HS_OK) return st;
+        ctx->launches += 1;
+        diag_out_kernel<<<64, 256, 0, s>>>(w.S, w.Y, dblk, w.Ld + (size_t)k * bb, w.LO + (size_t)nb * bb,
+                                           w.LO + (size_t)(nb + 1) * bb, bsz);
+        HS_CHECK_LAUNCH("mixed diag");
+        const int m = nb - k - 1;
+        if (m == 0) break;
+        // low parts of the raw panel, TRSM-as-GEMM with L^-T (writes L and its low part)
+        ctx->launches += 1;
+        lo_part_kernel<<<grid_for_elems((int64_t)m * bb / 4, ctx->num_sms), 256, 0, s>>>(dblk + bb, w.LO,
+                                                                                          (int64_t)m * bb / 4);
+        HS_CHECK_LAUNCH("lo_part");
+        TcArgs a{};
+        a.A32 = w.A32;
+        a.LO = w.LO;
+        a.blockID = blockID;
+        a.k = k;
+        a.nb = nb;
+        a.err = w.err;
+        prof_begin(ctx, s, HS_KERNEL_TRSM);
+        st = bsz == 256 ? tc_launch<256>(ctx, MODE_TRSM, w, a, m, s) : tc_launch<128>(ctx, MODE_TRSM, w, a, m, s);
+        if (st != HS_OK) return st;
+        prof_end(ctx, s, HS_KERNEL_TRSM, (double)m * 2.0 * bsz * bb, 4.0 * m * bb * 4.0);
+        // trailing update: GEMM pairs for rows k+2.., SYRK blocks k+1.. (as full blocks)
+        const int64_t g0 = 1, g1 = m;  // rows r' = r - k - 1 in [1, m)
+        a.pairBase = g0 * (g0 - 1) / 2;
+        a.gemmPairs = g1 * (g1 - 1) / 2 - a.pairBase;
+        a.syrkStart = k + 1;
+        a.totalPairs = a.gemmPairs + m;
+        prof_begin(ctx, s, HS_KERNEL_UPDATE);
+        st = bsz == 256 ? tc_launch<256>(ctx, MODE_UPDATE, w, a, a.totalPairs, s)
+                        : tc_launch<128>(ctx, MODE_UPDATE, w, a, a.totalPairs, s);
+        if (st != HS_OK) return st;
+        const double n3 = (double)bsz * bb;
+        prof_end(ctx, s, HS_KERNEL_UPDATE, (double)a.gemmPairs * 2.0 * n3 + (double)m * bsz * bsz * (bsz + 1.0),
+                 ((double)a.totalPairs * 2.0 + 2.0 * m) * bb * 4.0);
+    }
+    return HS_OK;
+}
+
+hs_status mixed_check_error(hs_ctx ctx, const MixedWork& w) {
+    int e = 0;
+    HS_CUDA(cudaMemcpy(&e, w.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        set_error("mixed-precision factor: a tensor-core tile gave up waiting for its operands (timeout)");
+        return HS_ERR_TIMEOUT;
+    }
+    (void)ctx;
+    return HS_OK;
+}
+
+}  // namespace hs

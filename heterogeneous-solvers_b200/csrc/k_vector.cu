@@ -15,6 +15,7 @@
 // second kernel sums the slots of an output block row in a fixed order, so the
 // result is bitwise reproducible without atomics.
 #include "hs_internal.cuh"
+#include "hs_mixed.cuh"
 
 namespace hs {
 namespace {
@@ -111,7 +112,29 @@ __global__ void dot_stage2(const double* __restrict__ partial, int n, double* __
 //   colOut[c] = sum_r M[r][c] * xr[r]      (column part)
 // Fast path for bsz in {128, 256}: 8 warps own bsz/8 consecutive rows each,
 // lane l owns bsz/32 consecutive columns loaded with 16-byte streaming loads.
-template <int BSZ>
+// CPL consecutive elements of one row as doubles, 16-byte streaming loads
+template <int CPL>
+__device__ __forceinline__ void load_row(const double* p, double (&a)[CPL]) {
+#pragma unroll
+    for (int j = 0; j < CPL / 2; ++j) {
+        const double2 v = __ldcs(reinterpret_cast<const double2*>(p) + j);
+        a[2 * j] = v.x;
+        a[2 * j + 1] = v.y;
+    }
+}
+template <int CPL>
+__device__ __forceinline__ void load_row(const float* p, double (&a)[CPL]) {
+#pragma unroll
+    for (int j = 0; j < CPL / 4; ++j) {
+        const float4 v = __ldcs(reinterpret_cast<const float4*>(p) + j);
+        a[4 * j] = v.x;
+        a[4 * j + 1] = v.y;
+        a[4 * j + 2] = v.z;
+        a[4 * j + 3] = v.w;
+    }
+}
+
+template <int BSZ, typename T = double>
 struct BlockApply {
     static constexpr int CPL = BSZ / 32;  // columns per lane
     static constexpr int RPW = BSZ / 8;   // rows per warp
@@ -137,7 +160,7 @@ struct BlockApply {
     }
 
     // mode bit 1: row part, bit 2: column part.  colOut / rowOut get "=" semantics.
-    __device__ static void run(const double* __restrict__ M, const double* __restrict__ xc,
+    __device__ static void run(const T* __restrict__ M, const double* __restrict__ xc,
                                const double* __restrict__ xr, double* __restrict__ rowOut,
                                double* __restrict__ colOut, int mode, double* smem /* 8*BSZ */) {
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -152,14 +175,8 @@ struct BlockApply {
         const double xrl = ((mode & 2) && lane < RPW) ? xr[r0 + lane] : 0.0;
 #pragma unroll
         for (int rr = 0; rr < RPW; ++rr) {
-            const double2* rowp = reinterpret_cast<const double2*>(M + (size_t)(r0 + rr) * BSZ + c0);
             double a[CPL];
-#pragma unroll
-            for (int j = 0; j < CPL / 2; ++j) {
-                const double2 v = __ldcs(rowp + j);
-                a[2 * j] = v.x;
-                a[2 * j + 1] = v.y;
-            }
+            load_row<CPL>(M + (size_t)(r0 + rr) * BSZ + c0, a);
             double acc = 0.0;
 #pragma unroll
             for (int j = 0; j < CPL; ++j) acc = fma(a[j], xcv[j], acc);
@@ -314,6 +331,28 @@ __global__ void __launch_bounds__(kThreads) column_update_kernel(const double* _
     }
     __syncthreads();
     for (int r = threadIdx.x; r < bsz; r += blockDim.x) bi[r] -= out[r];
+}
+
+// block-column update reading FP32 blocks (mixed-precision solves), FP64 sums
+template <int BSZ>
+__global__ void __launch_bounds__(kThreads) column_update_f32_kernel(const float* __restrict__ A,
+                                                                     double* __restrict__ b, int nb, int blockStart,
+                                                                     int blockRow, int64_t blockID, int transposed) {
+    __shared__ double smem[8 * BSZ];
+    __shared__ double out[BSZ];
+    const int g = blockIdx.x;
+    const size_t bb = (size_t)BSZ * BSZ;
+    const double* b0 = b + (size_t)blockRow * BSZ;
+    double* bi = b + (size_t)(blockStart + g) * BSZ;
+    if (!transposed) {
+        const float* M = A + (size_t)(blockID + (blockStart - blockRow + g)) * bb;
+        BlockApply<BSZ, float>::run(M, b0, nullptr, out, nullptr, 1, smem);
+    } else {
+        const float* M = A + (size_t)block_id(blockRow, blockStart + g, nb) * bb;
+        BlockApply<BSZ, float>::run(M, nullptr, b0, nullptr, out, 2, smem);
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < BSZ; r += blockDim.x) bi[r] -= out[r];
 }
 
 // ------------------------------------------------------------------ TRSV
@@ -519,6 +558,25 @@ hs_status launch_column_update(hs_ctx ctx, const double* A, double* b, int block
     HS_CHECK_LAUNCH("column_update");
     prof_end(ctx, s, HS_KERNEL_COLUPD, 2.0 * blockCount * (double)bsz * bsz,
              (double)blockCount * bsz * bsz * 8.0 + 24.0 * blockCount * bsz);
+    return HS_OK;
+}
+
+hs_status launch_column_update_f32(hs_ctx ctx, const float* A32, double* b, int blockStart, int blockCount,
+                                   int blockRow, int blockID, int transposed, cudaStream_t s) {
+    if (blockCount <= 0) return HS_OK;
+    const int bsz = ctx->bsz;
+    HS_REQUIRE(bsz == 128 || bsz == 256, "FP32 column update supports matrixBlockSize 128 or 256");
+    prof_begin(ctx, s, HS_KERNEL_COLUPD);
+    ctx->launches += 1;
+    if (bsz == 256)
+        column_update_f32_kernel<256><<<blockCount, kThreads, 0, s>>>(A32, b, ctx->nb, blockStart, blockRow, blockID,
+                                                                     transposed);
+    else
+        column_update_f32_kernel<128><<<blockCount, kThreads, 0, s>>>(A32, b, ctx->nb, blockStart, blockRow, blockID,
+                                                                     transposed);
+    HS_CHECK_LAUNCH("column_update_f32");
+    prof_end(ctx, s, HS_KERNEL_COLUPD, 2.0 * blockCount * (double)bsz * bsz,
+             (double)blockCount * bsz * bsz * 4.0 + 24.0 * blockCount * bsz);
     return HS_OK;
 }
 

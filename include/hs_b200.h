@@ -224,6 +224,41 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
                            int n_ell, double sf2, double sn2, int algorithm, double epsilon, int64_t iMax,
                            double* x_host, hs_solve_report* report);
 
+/* ------------------------------------------------------------------ mixed precision
+ * No reference counterpart (new form).  hs_mixed_solve factors K (packed FP64,
+ * device, left unchanged) in FP32 with the panel TRSM and the SYRK/GEMM trailing
+ * updates on the tensor cores (tcgen05 kind::tf32, 3xTF32 split products, FP32
+ * accumulation) and every diagonal-block POTRF in FP64, then refines
+ * x <- x + (L L^T)^-1 (b - K x) with FP64 residuals until the backward error
+ * ||b - K x|| / (||K||_F ||x||) <= tol.  When refinement stops contracting it
+ * continues with conjugate gradients preconditioned by the FP32 factor.  b and x
+ * are device vectors of hs_padded_vector_size doubles.  Allocates its own
+ * workspace (FP32 factor: half the packed matrix).  Returns
+ * HS_ERR_REFINEMENT_STALLED when neither reaches tol, HS_ERR_NOT_SPD when the
+ * FP32 factor meets a non-positive pivot. */
+typedef enum hs_precision {
+    HS_PRECISION_FP64 = 0,
+    HS_PRECISION_TF32X3 = 1,
+    HS_PRECISION_BF16X3 = 2
+} hs_precision;
+typedef struct hs_mixed_report {
+    int64_t refinement_steps;
+    int64_t pcg_iterations;
+    int fallback_pcg;
+    int reserved;
+    double backward_error;   /* ||b - K x|| / (||K||_F ||x||) at exit */
+    double initial_backward_error; /* the same for x0 = (L L^T)^-1 b, before any refinement */
+    double norm_k_fro;
+    double logdet;           /* log|K| = 2 sum log diag(L) from the FP64 diagonal blocks */
+    double factor_ms, refine_ms, total_ms;
+} hs_mixed_report;
+hs_status hs_mixed_solve(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,
+                         int max_steps, hs_mixed_report* report);
+
+/* log|K| = 2 sum_i log L_ii of a factor from hs_cholesky_factor (packed, device);
+ * *logdet is a host pointer. */
+hs_status hs_cholesky_logdet(hs_ctx ctx, const double* L, double* logdet);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,102 @@
+"""GPU suite: the mixed-precision form (3xTF32 tensor-core factor, FP64
+diagonal POTRF, FP64 iterative refinement, PCG fallback) against dense FP64
+LAPACK and the plain FP64 path, on seeded RBF systems."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import oracle_lib as ol
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(hs, ctx, N, bsz, d, ell, sn2, seed=5):
+    rng = np.random.default_rng(seed)
+    X = rng.random((N, d))
+    y = np.sin(X.sum(axis=1)) + 0.1 * rng.standard_normal(N)
+    ctx.set_problem(N, bsz)
+    A = hs.SymmetricMatrix(N, bsz, device="cuda:0")
+    hs.MatrixGenerator.assemble(ctx, A.matrixData, X, ell, 1.0, sn2)
+    b = torch.zeros(hs.padded_size(N, bsz), dtype=torch.float64, device="cuda:0")
+    b[:N] = torch.from_numpy(y)
+    return A, b, X, y
+
+
+@pytest.mark.parametrize("N,bsz,d,ell,sn2", [
+    (1000, 128, 8, 0.5, 1e-2), (700, 256, 16, 1.0, 1e-2), (1024, 256, 8, 0.5, 1e-1), (300, 128, 8, 0.5, 1e-2),
+    (2048, 256, 16, 1.0, 1e-2),
+])
+def test_mixed_solve_reaches_fp64_backward_error(hs, ctx, N, bsz, d, ell, sn2):
+    A, b, X, y = _system(hs, ctx, N, bsz, d, ell, sn2)
+    solver = hs.MixedPrecisionSolver(A, ctx, "tf32x3")
+    x = solver.solve(b, tol=1e-14, max_steps=30)
+    rep = solver.report
+    Kd = A.to_dense()
+    x_ref = np.linalg.solve(Kd, y)
+    xg = x.cpu().numpy()
+    assert np.all(xg[N:] == 0.0), "padding of x must stay zero"
+    xg = xg[:N]
+    bwd = np.linalg.norm(y - Kd @ xg) / (np.linalg.norm(Kd, "fro") * np.linalg.norm(xg))
+    rel = np.linalg.norm(xg - x_ref) / np.linalg.norm(x_ref)
+    print(f"N={N} bsz={bsz} sn2={sn2}: steps {rep['refinement_steps']} pcg {rep['pcg_iterations']} "
+          f"bwd0 {rep['initial_backward_error']:.2e} bwd {rep['backward_error']:.2e} (host {bwd:.2e}) "
+          f"x rel {rel:.2e}")
+    assert rep["backward_error"] <= 1e-14
+    assert bwd <= 2e-14
+    # 3xTF32 products give an FP32-accurate factor: the unrefined solution's backward
+    # error is ~1e-7; a plain TF32 product (10-bit mantissa) would leave ~1e-4
+    assert rep["initial_backward_error"] <= 1e-5
+    cond = np.linalg.cond(Kd)
+    assert rel <= max(1e-12, 50 * cond * 1e-16)
+    sign, logdet_ref = np.linalg.slogdet(Kd)
+    assert sign > 0
+    assert abs(rep["logdet"] - logdet_ref) <= 1e-4 * abs(logdet_ref) + 1e-3
+
+
+def test_mixed_leaves_matrix_unchanged(hs, ctx):
+    A, b, _, _ = _system(hs, ctx, 600, 128, 8, 0.5, 1e-2)
+    before = A.matrixData.clone()
+    hs.MixedPrecisionSolver(A, ctx).solve(b)
+    torch.cuda.synchronize()
+    assert torch.equal(before, A.matrixData)
+
+
+def test_mixed_matches_fp64_path(hs, ctx):
+    """The mixed solve and the FP64 factor + solve agree to the FP64 accuracy of the system."""
+    A, b, _, y = _system(hs, ctx, 1536, 256, 8, 0.5, 1e-2, seed=9)
+    x_mixed = hs.MixedPrecisionSolver(A, ctx).solve(b).cpu().numpy()
+    L = A.matrixData.clone()
+    info = ctypes.c_int64(-2)
+    hs._lib.call("hs_cholesky_factor", ctx.handle, ctypes.c_void_p(L.data_ptr()), ctypes.byref(info))
+    assert info.value == -1
+    x64 = b.clone()
+    hs._lib.call("hs_cholesky_solve", ctx.handle, ctypes.c_void_p(L.data_ptr()), ctypes.c_void_p(x64.data_ptr()))
+    x64 = x64.cpu().numpy()
+    rel = np.linalg.norm(x_mixed - x64) / np.linalg.norm(x64)
+    assert rel <= 1e-10, rel
+
+
+@pytest.mark.parametrize("N,bsz", [(1000, 128), (700, 256)])
+def test_logdet_of_fp64_factor(hs, ctx, N, bsz):
+    A, _, _, _ = _system(hs, ctx, N, bsz, 8, 0.5, 1e-2)
+    Kd = A.to_dense()
+    chol = hs.Cholesky(A, ctx).solve_heterogeneous()
+    ld = hs.cholesky_logdet(ctx, chol.A_gpu)
+    ref = np.linalg.slogdet(Kd)[1]
+    assert abs(ld - ref) <= 1e-11 * abs(ref)
+
+
+def test_mixed_ill_conditioned_falls_back_or_converges(hs, ctx):
+    """sn2 = 1e-6: the FP32 factor is a poor approximation; the solve must still
+    reach the backward-error target (refinement, then PCG with the factor)."""
+    A, b, _, y = _system(hs, ctx, 1024, 128, 8, 0.5, 1e-6)
+    solver = hs.MixedPrecisionSolver(A, ctx)
+    x = solver.solve(b, tol=1e-14, max_steps=30)
+    rep = solver.report
+    print("ill-conditioned:", rep)
+    Kd = A.to_dense()
+    xg = x.cpu().numpy()[:1024]
+    bwd = np.linalg.norm(y - Kd @ xg) / (np.linalg.norm(Kd, "fro") * np.linalg.norm(xg))
+    assert bwd <= 2e-14
