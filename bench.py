@@ -2,15 +2,18 @@
 """Benchmark of the blocked SPD solve path for GP kernel matrices.
 
 One step = RBF assembly of the packed kernel matrix from device-resident
-inputs, the FP64 blocked Cholesky factor and the forward/back substitution,
-at N = 131072, d = 16, l = 1, sf2 = 1, sn2 = 1e-2, matrix_bsz = 256 (68.85 GB
+inputs and the mixed-precision solve (3xTF32 tensor-core factor with FP64
+diagonal POTRF, FP64 iterative refinement to backward error <= 1e-14), at
+N = 131072, d = 16, l = 1, sf2 = 1, sn2 = 1e-2, matrix_bsz = 256 (68.85 GB
 packed FP64 matrix, larger than L2, so no flush is needed between steps).
+The FP64 factor + solve of the same system is timed in the same run (the
+comparison at equal error), with both backward errors.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints one JSON line on rank 0.  `value` is whole-job throughput in solves/s
 (N independent replicas under torchrun: the path does not shard).  `e2e` is
-the same metric through hs_gp_solve_host with pinned host buffers.  The
+the same metric through hs_gp_solve_host (algorithm 2) with pinned host buffers.  The
 reference arm (--impl reference) times the CPU restatement of the reference's
 CPU path (or its sources compiled through oracle/ref_build.py when present) on
 a bounded sample and extrapolates by N^3.
@@ -42,6 +45,13 @@ def load_package():
     return mod
 
 
+def bench_config(N, world=1):
+    """The workload both arms run: one GP system solved to FP64 accuracy."""
+    return {"workload": f"{WORKLOAD}: solve K x = y (RBF kernel matrix assembled from X) to FP64 backward error",
+            "N": N, "d": 16, "bsz": 256, "lengthscale": 1.0, "sf2": 1.0, "sn2": 1e-2,
+            "l2": "inputs larger than L2 (packed K 68.85 GB at N=131072)", "parallelism": f"replicas x{world}"}
+
+
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -53,6 +63,8 @@ def parse_args():
     ap.add_argument("--cpu-sample-n", type=int, default=8192)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
+    ap.add_argument("--tol", type=float, default=1e-14, help="backward-error target of the mixed solve")
     return ap.parse_args()
 
 
@@ -154,18 +166,21 @@ def run_reference_arm(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_full * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{WORKLOAD}: RBF assembly + FP64 blocked Cholesky factor + solve", "N": N,
-                       "d": 16, "bsz": 256},
+            "config": dict(bench_config(N), implementation="the reference's CPU path (init_gpu_perc=0): "
+                                                          "FP64 blocked Cholesky factor + forward/back solve"),
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------------ GPU arm
-def measure_fp64_peak(torch, device):
-    """cuBLAS DGEMM 8192^3 (torch.matmul float64), best of 5: the FP64 peak."""
-    a = torch.randn(8192, 8192, dtype=torch.float64, device=device)
-    b = torch.randn(8192, 8192, dtype=torch.float64, device=device)
+def measure_gemm_peak(torch, device, dtype, tf32=False):
+    """cuBLAS GEMM 8192^3 through torch.matmul, best of 5, in TFLOP/s (FP64, or
+    FP32 inputs on the TF32 tensor-core path when ``tf32``)."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = tf32
+    a = torch.randn(8192, 8192, dtype=dtype, device=device)
+    b = torch.randn(8192, 8192, dtype=dtype, device=device)
     for _ in range(2):
         torch.matmul(a, b)
     best = 0.0
@@ -176,6 +191,7 @@ def measure_fp64_peak(torch, device):
         e1.record()
         e1.synchronize()
         best = max(best, 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    torch.backends.cuda.matmul.allow_tf32 = prev
     del a, b
     torch.cuda.empty_cache()
     return best
@@ -189,6 +205,8 @@ def main():
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
         return
+
+    import ctypes
 
     import numpy as np
     import torch
@@ -206,34 +224,58 @@ def main():
     N = args.n or cfg["N"]
     bsz, d = cfg["bsz"], cfg["d"]
     X, y = wl.gp_inputs(N, d, cfg["seed"] + rank)
+    dev = f"cuda:{device}"
     ctx = hs.Context(device=device)
     ctx.set_problem(N, bsz)
+    nb = ctx.blockCountXY
     n_pad = hs.padded_size(N, bsz)
-    Xd = torch.from_numpy(X).to(f"cuda:{device}")
-    bd = torch.zeros(n_pad, dtype=torch.float64, device=f"cuda:{device}")
-    bd[:N] = torch.from_numpy(y).to(f"cuda:{device}")
-    A = torch.empty(hs.packed_size(N, bsz), dtype=torch.float64, device=f"cuda:{device}")
+    Xd = torch.from_numpy(X).to(dev)
+    bd = torch.zeros(n_pad, dtype=torch.float64, device=dev)
+    bd[:N] = torch.from_numpy(y).to(dev)
+    A = torch.empty(hs.packed_size(N, bsz), dtype=torch.float64, device=dev)
     xd = torch.empty_like(bd)
     lib = hs._lib.load()
-    import ctypes
 
     def P(t):
         return ctypes.c_void_p(t.data_ptr())
 
     info = ctypes.c_int64()
+    mrep = hs._lib.MixedReport()
 
-    def step():
+    def assemble():
         hs.MatrixGenerator.assemble(ctx, A, Xd, cfg["lengthscale"], cfg["sf2"], cfg["sn2"])
+
+    def step_mixed():
+        assemble()
+        hs._lib.check(lib.hs_mixed_solve(ctx.handle, P(A), P(bd), P(xd), hs.PRECISIONS["tf32x3"], args.tol,
+                                         30, ctypes.byref(mrep)))
+
+    def step_fp64(x_out):
+        assemble()
         hs._lib.check(lib.hs_cholesky_factor(ctx.handle, P(A), ctypes.byref(info)))
-        xd.copy_(bd)
-        hs._lib.check(lib.hs_cholesky_solve(ctx.handle, P(A), P(xd)))
+        x_out.copy_(bd)
+        hs._lib.check(lib.hs_cholesky_solve(ctx.handle, P(A), P(x_out)))
+
+    def k_fro():
+        blocks = A.view(-1, bsz * bsz)
+        diag_ids = torch.tensor([hs.block_id(k, k, nb) for k in range(nb)], device=A.device)
+        sq_all = (blocks * blocks).sum(dim=1)
+        return float(torch.sqrt(2.0 * sq_all.sum() - sq_all[diag_ids].sum()).item())
+
+    def backward_error(x):
+        """||y - K x|| / (||K||_F ||x||) with K re-assembled in A."""
+        assemble()
+        r = torch.empty_like(bd)
+        hs.MatrixVectorOperations.matrixVectorBlock(ctx, A, x, r, 0, 0, nb, nb, nb)
+        res = torch.linalg.norm(r - bd).item()
+        return res / (k_fro() * torch.linalg.norm(x).item())
 
     for _ in range(args.warmup):
-        step()
+        step_mixed()
     torch.cuda.synchronize()
-    fp64_peak = measure_fp64_peak(torch, device)
+    tf32_peak = measure_gemm_peak(torch, device, torch.float32, tf32=True)
 
-    # ---------------- timed region (device-resident inputs)
+    # ---------------- timed region: mixed-precision solve (device-resident inputs)
     sampler = ClockSampler(device)
     if world > 1:
         dist.barrier()
@@ -245,15 +287,16 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
-        step()
+        step_mixed()
     e1.record()
     torch.cuda.synchronize()
     clocks = sampler.stop()
     launches = ctx.launch_count() - launches0
     ctx.set_profiling(False)
     t_ms = e0.elapsed_time(e1)
-    prof = {k: ctx.read_profile(k) for k in ("update", "potrf", "trsm", "assemble", "trsv", "colupd")}
-    t_max = torch.tensor([t_ms], dtype=torch.float64, device=f"cuda:{device}")
+    kernels = ("update", "potrf", "trsm", "assemble", "trsv", "colupd", "symv", "vector")
+    prof = {k: ctx.read_profile(k) for k in kernels}
+    t_max = torch.tensor([t_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
     t_max_ms = float(t_max.item())
@@ -261,23 +304,47 @@ def main():
         dist.barrier()
     ms_per_step = t_max_ms / args.steps
     value = world * args.steps / (t_max_ms * 1e-3)
+    mixed_report = {f: getattr(mrep, f) for f, _ in hs._lib.MixedReport._fields_ if f != "reserved"}
+    x_mixed = xd.clone()
+    bwd_mixed = backward_error(x_mixed)
 
-    # ---------------- size-independent checks on the last step's result
-    x_host = xd[:N].cpu().numpy()
-    hs.MatrixGenerator.assemble(ctx, A, Xd, cfg["lengthscale"], cfg["sf2"], cfg["sn2"])
-    r = torch.empty_like(bd)
-    nb = ctx.blockCountXY
-    hs.MatrixVectorOperations.matrixVectorBlock(ctx, A, xd, r, 0, 0, nb, nb, nb)
-    res = torch.linalg.norm(r - bd).item()
-    blocks = A.view(-1, bsz * bsz)
-    diag_ids = torch.tensor([hs.block_id(k, k, nb) for k in range(nb)], device=A.device)
-    sq_all = (blocks * blocks).sum(dim=1)
-    k_fro = float(torch.sqrt(2.0 * sq_all.sum() - sq_all[diag_ids].sum()).item())
-    backward_error = res / (k_fro * float(np.linalg.norm(x_host)) + float(np.linalg.norm(y)))
+    # ---------------- FP64 factor + solve on the same system (the comparison at equal error)
+    fp64 = None
+    if not args.no_fp64:
+        x64 = torch.empty_like(bd)
+        # load the FP64 kernels on a small system, then time one full step
+        ctx_s = hs.Context(device=device, N=4096, matrixBlockSize=bsz)
+        As = torch.empty(hs.packed_size(4096, bsz), dtype=torch.float64, device=dev)
+        hs.MatrixGenerator.assemble(ctx_s, As, Xd[:4096], cfg["lengthscale"], cfg["sf2"], cfg["sn2"])
+        lib.hs_cholesky_factor(ctx_s.handle, P(As), ctypes.byref(info))
+        ctx_s.close()
+        del As
+        torch.cuda.synchronize()
+        ctx.reset_profile()
+        ctx.set_profiling(True)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        step_fp64(x64)
+        f1.record()
+        torch.cuda.synchronize()
+        ctx.set_profiling(False)
+        upd64 = ctx.read_profile("update")
+        fp64_ms = f0.elapsed_time(f1)
+        logdet64 = hs.cholesky_logdet(ctx, A)
+        bwd64 = backward_error(x64)
+        fp64 = {"ms_per_step": fp64_ms, "solves_per_s": 1e3 / fp64_ms, "backward_error": bwd64,
+                "factor_tflops_whole": (N ** 3 / 3) / (fp64_ms * 1e-3) / 1e12,
+                "update_dmma_tflops": upd64["flops"] / (upd64["ms"] * 1e-3) / 1e12 if upd64["ms"] else None,
+                "speedup_mixed_vs_fp64": fp64_ms / ms_per_step}
+        fp64["mixed_x_rel_diff"] = float((torch.linalg.norm(x_mixed - x64) / torch.linalg.norm(x64)).item())
+        fp64["mixed_logdet_rel_diff"] = abs(mixed_report["logdet"] - logdet64) / abs(logdet64)
+        fp64["logdet"] = logdet64
+        del x64
 
     # ---------------- CG matvec roofline: a bounded number of CG iterations on K
     cg_info = None
     if args.cg_iters > 0:
+        assemble()
         x_cg = torch.empty_like(bd)
         it, dn, d0 = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
         ctx.reset_profile()
@@ -297,7 +364,7 @@ def main():
                    "matvec_frac_of_hbm": None}
         del x_cg
 
-    # ---------------- e2e through the host-buffer API
+    # ---------------- e2e through the host-buffer API (mixed precision, algorithm 2)
     e2e = None
     if not args.no_e2e:
         del A
@@ -305,27 +372,28 @@ def main():
         Xh = torch.from_numpy(X).pin_memory()
         yh = torch.from_numpy(y).pin_memory()
         xh = torch.empty(N, dtype=torch.float64).pin_memory()
-        hs.gp_solve_host(ctx, Xh, yh, cfg["lengthscale"], cfg["sf2"], cfg["sn2"], out=xh)  # warm-up
+        kw = dict(algorithm="mixed", epsilon=args.tol, iMax=30, out=xh)
+        hs.gp_solve_host(ctx, Xh, yh, cfg["lengthscale"], cfg["sf2"], cfg["sn2"], **kw)  # warm-up
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            _, rep = hs.gp_solve_host(ctx, Xh, yh, cfg["lengthscale"], cfg["sf2"], cfg["sn2"], out=xh)
+            _, rep = hs.gp_solve_host(ctx, Xh, yh, cfg["lengthscale"], cfg["sf2"], cfg["sn2"], **kw)
         torch.cuda.synchronize()
-        t_e2e = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=f"cuda:{device}")
+        t_e2e = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
         if world > 1:
             dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
         e2e = {"value": world * args.steps / float(t_e2e.item()), "unit": "solves/s",
                "h2d_bytes_per_step": int(X.nbytes + y.nbytes), "d2h_bytes_per_step": int(N * 8),
-               "report_ms": {"assemble+h2d": rep.assemble_ms, "factor": rep.factor_ms, "solve": rep.solve_ms,
+               "report_ms": {"assemble+h2d": rep.assemble_ms, "factor+refine": rep.factor_ms,
                              "total": rep.total_ms}}
 
-    # ---------------- roofline of the dominant kernel (FP64 trailing update)
+    # ---------------- roofline of the dominant kernel (tensor-core trailing update)
     upd = prof["update"]
-    achieved = upd["flops"] / (upd["ms"] * 1e-3) / 1e12 if upd["ms"] else None
+    useful = upd["flops"] / (upd["ms"] * 1e-3) / 1e12 if upd["ms"] else None
     traffic = None
-    tfile = ROOT / "profiles" / "update_dmma_traffic.json"
+    tfile = ROOT / "profiles" / "update_tc_traffic.json"
     if tfile.exists() and upd["launches"]:
         tj = json.loads(tfile.read_text())
         traffic = tj["dram_bytes_per_flop"] * upd["flops"] / upd["launches"]
@@ -348,24 +416,27 @@ def main():
     if rank == 0:
         phases = {k: {"launches": v["launches"], "ms_per_step": v["ms"] / args.steps,
                       "tflops": v["flops"] / (v["ms"] * 1e-3) / 1e12 if v["ms"] else None}
-                  for k, v in prof.items()}
+                  for k, v in prof.items() if v["launches"]}
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64",
+            "vs_baseline": None, "dtype": "f32 (3xTF32 tensor-core factor) + f64 refinement",
             "data": f"synthetic: X~U[0,1]^({N}x{d}) seed {cfg['seed']}+rank, y=sin(sum_k x_k)+N(0,0.1^2)",
-            "config": {"workload": f"{WORKLOAD}: RBF assembly + FP64 blocked Cholesky factor + forward/back solve",
-                       "N": N, "d": d, "bsz": bsz, "lengthscale": cfg["lengthscale"], "sf2": cfg["sf2"],
-                       "sn2": cfg["sn2"], "l2": "inputs larger than L2 (packed K 68.85 GB at N=131072)",
-                       "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                         "frac": achieved / fp64_peak if achieved else None, "traffic": traffic,
-                         "kernel": "update_dmma_kernel (FP64 SYRK+GEMM trailing update, DMMA)",
-                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is absent from "
-                                        "MEASURED_PEAKS.json)"},
+            "config": dict(bench_config(N, world), implementation=(
+                "RBF assembly + mixed-precision Cholesky (3xTF32 tensor-core TRSM/SYRK/GEMM, FP64 POTRF) + "
+                f"FP64 iterative refinement to backward error <= {args.tol:g}")),
+            "roofline": {"bound": "tensor", "achieved": useful,
+                         "peak": tf32_peak / 3.0 if useful else None, "unit": "TFLOP/s",
+                         "frac": useful / (tf32_peak / 3.0) if useful else None, "traffic": traffic,
+                         "kernel": "tc_tile_kernel<256, update> (3xTF32 SYRK+GEMM trailing update, tcgen05)",
+                         "peak_source": "cuBLAS TF32 GEMM 8192^3 measured in this run, divided by the 3 TF32 "
+                                        "products of one split FP32 product (TF32 is absent from "
+                                        "MEASURED_PEAKS.json)",
+                         "tf32_gemm_peak": tf32_peak,
+                         "issued_tf32_tflops": 3 * useful if useful else None},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-            "phases": phases, "factor_tflops_whole": (N ** 3 / 3) / (ms_per_step * 1e-3) / 1e12,
-            "backward_error": backward_error, "cg": cg_info,
+            "phases": phases, "mixed": mixed_report, "backward_error": bwd_mixed, "fp64": fp64,
+            "cg": cg_info,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -69,6 +69,7 @@ SIGNATURES = {
     "hs_ctx_create": [_I, _P, ctypes.POINTER(_P)],
     "hs_ctx_destroy": [_P],
     "hs_ctx_set_stream": [_P, _P],
+    "hs_ctx_release_buffers": [_P],
     "hs_ctx_set_problem": [_P, _I64, _I],
     "hs_sync": [_P],
     "hs_packed_matrix_size": [_I64, _I],

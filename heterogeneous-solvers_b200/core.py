@@ -519,10 +519,16 @@ class MatrixParser:
         return b
 
 
+# hs_gp_solve_host algorithms
+_ALGORITHMS = {"cholesky": 0, "cg": 1, "mixed": 2}
+
+
 def gp_solve_host(ctx, X, y, lengthscale=1.0, signal_variance=1.0, noise_variance=0.01, algorithm="cholesky",
                   epsilon=1e-10, iMax=100000, out=None):
     """End-to-end GP solve through host buffers (hs_gp_solve_host): host X
-    (N x d) and y (N) in, host x = K^-1 y out, plus the phase report.  X, y
+    (N x d) and y (N) in, host x = K^-1 y out, plus the phase report.
+    ``algorithm`` is "cholesky", "cg" or "mixed" (for "mixed", ``epsilon`` is
+    the backward-error target and ``iMax`` the refinement step limit).  X, y
     and ``out`` may be CPU torch tensors (pinned memory gives asynchronous
     copies) or numpy arrays."""
 
@@ -543,6 +549,6 @@ def gp_solve_host(ctx, X, y, lengthscale=1.0, signal_variance=1.0, noise_varianc
     x, xp = host(out if out is not None else np.empty(N, dtype=np.float64))
     rep = SolveReport()
     call("hs_gp_solve_host", ctx.handle, Xp, yp, d, ell.ctypes.data_as(ctypes.c_void_p), int(ell.size),
-         float(signal_variance), float(noise_variance), 0 if algorithm == "cholesky" else 1, float(epsilon),
+         float(signal_variance), float(noise_variance), _ALGORITHMS[algorithm], float(epsilon),
          int(iMax), xp, ctypes.byref(rep))
     return x, rep

@@ -57,6 +57,17 @@ hs_status ensure_work(hs_ctx ctx, size_t bytes) {
     return HS_OK;
 }
 
+hs_status ensure_mixed(hs_ctx ctx, size_t bytes) {
+    if (ctx->mixed_bytes >= bytes) return HS_OK;
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->mixed) HS_CUDA(cudaFree(ctx->mixed));
+    ctx->mixed = nullptr;
+    ctx->mixed_bytes = 0;
+    HS_CUDA(cudaMalloc(&ctx->mixed, bytes));
+    ctx->mixed_bytes = bytes;
+    return HS_OK;
+}
+
 __global__ void set_i64_kernel(long long* p, long long v) { *p = v; }
 
 void set_i64_dev(long long* p, long long v, cudaStream_t s) { set_i64_kernel<<<1, 1, 0, s>>>(p, v); }
@@ -208,9 +219,26 @@ hs_status hs_ctx_destroy(hs_ctx ctx) {
     for (auto e : ctx->prof_pool) cudaEventDestroy(e);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->work) cudaFree(ctx->work);
+    if (ctx->mixed) cudaFree(ctx->mixed);
     if (ctx->d_info) cudaFree(ctx->d_info);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     delete ctx;
+    return HS_OK;
+}
+
+hs_status hs_ctx_release_buffers(hs_ctx ctx) {
+    if (!ctx) {
+        set_error("hs_ctx_release_buffers: null context");
+        return HS_ERR_INVALID_ARG;
+    }
+    HS_CUDA(cudaSetDevice(ctx->device));
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->side) HS_CUDA(cudaStreamSynchronize(ctx->side));
+    if (ctx->scratch) HS_CUDA(cudaFree(ctx->scratch));
+    if (ctx->work) HS_CUDA(cudaFree(ctx->work));
+    if (ctx->mixed) HS_CUDA(cudaFree(ctx->mixed));
+    ctx->scratch = ctx->work = ctx->mixed = nullptr;
+    ctx->scratch_bytes = ctx->work_bytes = ctx->mixed_bytes = 0;
     return HS_OK;
 }
 

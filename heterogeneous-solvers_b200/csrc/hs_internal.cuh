@@ -25,6 +25,10 @@ struct hs_ctx_s {
     // grow-only device work vectors of the solver drivers (CG r/d/q, ...)
     void* work = nullptr;
     size_t work_bytes = 0;
+    // grow-only workspace of the mixed-precision factor (FP32 factor, split
+    // parts, FP64 diagonal blocks, refinement vectors)
+    void* mixed = nullptr;
+    size_t mixed_bytes = 0;
 
     // device word holding the smallest failing pivot row (INT64_MAX = none)
     long long* d_info = nullptr;
@@ -89,6 +93,7 @@ void prof_end(hs_ctx ctx, cudaStream_t s, int kernel, double flops, double bytes
 // the old buffer is released after a stream sync)
 hs_status ensure_scratch(hs_ctx ctx, size_t bytes);
 hs_status ensure_work(hs_ctx ctx, size_t bytes);
+hs_status ensure_mixed(hs_ctx ctx, size_t bytes);
 
 // scratch layout: [0, 32 KB) reduction partials, [32 KB, 48 KB) solver scalars,
 // [56 KB, 64 KB) small constants; matvec partial blocks start at 64 KB

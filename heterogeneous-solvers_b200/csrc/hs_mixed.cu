@@ -122,13 +122,6 @@ int grid_n(int64_t n, int sms) {
     return (int)(g < 1 ? 1 : g);
 }
 
-struct Dev {
-    void* p = nullptr;
-    ~Dev() {
-        if (p) cudaFree(p);
-    }
-};
-
 }  // namespace
 
 // b <- (L L^T)^-1 b with the mixed factor: FP64 diagonal blocks, FP32 off-diagonal blocks
@@ -158,38 +151,19 @@ hs_status mixed_apply(hs_ctx ctx, const MixedWork& w, double* b, cudaStream_t s)
     return HS_OK;
 }
 
-}  // namespace hs
 
-using namespace hs;
-
-extern "C" {
-
-hs_status hs_cholesky_logdet(hs_ctx ctx, const double* L, double* logdet) {
-    hs_status st = require_ctx(ctx, "hs_cholesky_logdet");
-    if (st != HS_OK) return st;
-    if (!L || !logdet) {
-        set_error("hs_cholesky_logdet: null pointer");
-        return HS_ERR_INVALID_ARG;
+namespace {
+struct Events {
+    cudaEvent_t e[3] = {};
+    ~Events() {
+        for (auto& v : e)
+            if (v) cudaEventDestroy(v);
     }
-    st = ensure_scratch(ctx, kSmallScratch);
-    if (st != HS_OK) return st;
-    double* out = reinterpret_cast<double*>(static_cast<char*>(ctx->scratch) + kScalarOffset) + 8;
-    ctx->launches += 1;
-    logdiag_kernel<<<1, 1024, 0, ctx->stream>>>(L, ctx->bsz, ctx->nb, ctx->N, 0, out);
-    HS_CHECK_LAUNCH("logdet");
-    HS_CUDA(cudaMemcpyAsync(logdet, out, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    HS_CUDA(cudaStreamSynchronize(ctx->stream));
-    return HS_OK;
-}
+};
+}  // namespace
 
-hs_status hs_mixed_solve(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,
-                         int max_steps, hs_mixed_report* rep) {
-    hs_status st = require_ctx(ctx, "hs_mixed_solve");
-    if (st != HS_OK) return st;
-    if (!K || !b || !x) {
-        set_error("hs_mixed_solve: null pointer");
-        return HS_ERR_INVALID_ARG;
-    }
+hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,
+                           int max_steps, hs_mixed_report* out) {
     if (precision != HS_PRECISION_TF32X3) {
         set_error("hs_mixed_solve: only HS_PRECISION_TF32X3 is implemented");
         return HS_ERR_UNSUPPORTED;
@@ -202,18 +176,19 @@ hs_status hs_mixed_solve(hs_ctx ctx, const double* K, const double* b, double* x
     const int nb = ctx->nb, bsz = ctx->bsz;
     const int64_t n = (int64_t)nb * bsz;
     const auto t0 = std::chrono::steady_clock::now();
-    hs_mixed_report R{};
-    // workspace: factor + 5 vectors
-    Dev ws, vec;
-    HS_CUDA(cudaMalloc(&ws.p, mixed_workspace_bytes(ctx->N, bsz)));
-    HS_CUDA(cudaMalloc(&vec.p, (size_t)5 * n * sizeof(double)));
-    double* r = static_cast<double*>(vec.p);
+    hs_mixed_report& R = *out;
+    R = hs_mixed_report{};
+    // workspace (kept by the context): factor + 5 vectors
+    const size_t fbytes = (mixed_workspace_bytes(ctx->N, bsz) + 255) & ~size_t(255);
+    hs_status st = ensure_mixed(ctx, fbytes + (size_t)5 * n * sizeof(double));
+    if (st != HS_OK) return st;
+    double* r = reinterpret_cast<double*>(static_cast<char*>(ctx->mixed) + fbytes);
     double* d = r + n;
     double* p = d + n;
     double* q = p + n;
     double* z = q + n;
     MixedWork w;
-    st = mixed_bind(ctx, ws.p, &w);
+    st = mixed_bind(ctx, ctx->mixed, &w);
     if (st != HS_OK) return st;
     st = ensure_scratch(ctx, kSmallScratch + (size_t)nb * nb * bsz * sizeof(double));
     if (st != HS_OK) return st;
@@ -221,6 +196,8 @@ hs_status hs_mixed_solve(hs_ctx ctx, const double* K, const double* b, double* x
     double* scal = reinterpret_cast<double*>(static_cast<char*>(ctx->scratch) + kScalarOffset) + 16;
     volatile double* h = ctx->h_pinned;
     const int g = grid_n(n, ctx->num_sms);
+    Events ev;
+    for (auto& e : ev.e) HS_CUDA(cudaEventCreate(&e));
 
     // ||K||_F
     {
@@ -235,19 +212,12 @@ hs_status hs_mixed_solve(hs_ctx ctx, const double* K, const double* b, double* x
         R.norm_k_fro = std::sqrt(h[8]);
     }
     // factor (a non-positive FP64 pivot of the FP32 matrix is recorded in ctx->d_info)
-    cudaEvent_t e0, e1, e2;
-    HS_CUDA(cudaEventCreate(&e0));
-    HS_CUDA(cudaEventCreate(&e1));
-    HS_CUDA(cudaEventCreate(&e2));
-    HS_CUDA(cudaEventRecord(e0, s));
+    HS_CUDA(cudaEventRecord(ev.e[0], s));
     ctx->launches += 1;
-    {
-        long long* info = ctx->d_info;
-        set_i64_dev(info, INT64_MAX, s);
-    }
+    set_i64_dev(ctx->d_info, INT64_MAX, s);
     st = mixed_factor(ctx, K, w, s);
     if (st != HS_OK) return st;
-    HS_CUDA(cudaEventRecord(e1, s));
+    HS_CUDA(cudaEventRecord(ev.e[1], s));
     HS_CUDA(cudaStreamSynchronize(s));
     st = mixed_check_error(ctx, w);
     if (st != HS_OK) return st;
@@ -347,9 +317,15 @@ hs_status hs_mixed_solve(hs_ctx ctx, const double* K, const double* b, double* x
             }
             R.backward_error = rn / (R.norm_k_fro * xn);
             if (R.backward_error <= tol) {
-                converged = true;
-                ++it;
-                break;
+                // confirm with the true residual before stopping
+                st = residual(&rn, &xn);
+                if (st != HS_OK) return st;
+                R.backward_error = rn / (R.norm_k_fro * xn);
+                if (R.backward_error <= tol) {
+                    converged = true;
+                    ++it;
+                    break;
+                }
             }
             HS_CUDA(cudaMemcpyAsync(z, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
             if ((st = mixed_apply(ctx, w, z, s)) != HS_OK) return st;
@@ -363,26 +339,60 @@ hs_status hs_mixed_solve(hs_ctx ctx, const double* K, const double* b, double* x
         }
         R.pcg_iterations = it;
     }
-    HS_CUDA(cudaEventRecord(e2, s));
+    HS_CUDA(cudaEventRecord(ev.e[2], s));
     HS_CUDA(cudaMemcpyAsync((void*)(h + 16), scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
     HS_CUDA(cudaStreamSynchronize(s));
     R.logdet = h[16];
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventElapsedTime(&ms, ev.e[0], ev.e[1]);
     R.factor_ms = ms;
-    cudaEventElapsedTime(&ms, e1, e2);
+    cudaEventElapsedTime(&ms, ev.e[1], ev.e[2]);
     R.refine_ms = ms;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(e2);
     R.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    if (rep) *rep = R;
     if (!converged) {
         set_error("hs_mixed_solve: backward error " + std::to_string(R.backward_error) + " above the target " +
                   std::to_string(tol) + " after refinement and preconditioned CG");
         return HS_ERR_REFINEMENT_STALLED;
     }
     return HS_OK;
+}
+
+}  // namespace hs
+
+using namespace hs;
+
+extern "C" {
+
+hs_status hs_cholesky_logdet(hs_ctx ctx, const double* L, double* logdet) {
+    hs_status st = require_ctx(ctx, "hs_cholesky_logdet");
+    if (st != HS_OK) return st;
+    if (!L || !logdet) {
+        set_error("hs_cholesky_logdet: null pointer");
+        return HS_ERR_INVALID_ARG;
+    }
+    st = ensure_scratch(ctx, kSmallScratch);
+    if (st != HS_OK) return st;
+    double* out = reinterpret_cast<double*>(static_cast<char*>(ctx->scratch) + kScalarOffset) + 8;
+    ctx->launches += 1;
+    logdiag_kernel<<<1, 1024, 0, ctx->stream>>>(L, ctx->bsz, ctx->nb, ctx->N, 0, out);
+    HS_CHECK_LAUNCH("logdet");
+    HS_CUDA(cudaMemcpyAsync(logdet, out, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HS_OK;
+}
+
+hs_status hs_mixed_solve(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,
+                         int max_steps, hs_mixed_report* rep) {
+    hs_status st = require_ctx(ctx, "hs_mixed_solve");
+    if (st != HS_OK) return st;
+    if (!K || !b || !x) {
+        set_error("hs_mixed_solve: null pointer");
+        return HS_ERR_INVALID_ARG;
+    }
+    hs_mixed_report R{};
+    st = mixed_solve_impl(ctx, K, b, x, precision, tol, max_steps, &R);
+    if (rep) *rep = R;
+    return st;
 }
 
 }  // extern "C"

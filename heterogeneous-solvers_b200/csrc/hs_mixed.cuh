@@ -23,6 +23,9 @@ size_t mixed_workspace_bytes(int64_t N, int bsz);
 hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w);
 hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s);
 hs_status mixed_check_error(hs_ctx ctx, const MixedWork& w);
+// the mixed-precision solve behind hs_mixed_solve (workspace kept by the context)
+hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,
+                           int max_steps, hs_mixed_report* out);
 
 // TRSM of `items` bsz x bsz FP64 blocks stored contiguously at B against the
 // lower triangle L (bsz x bsz): B <- B L^-T

@@ -13,6 +13,7 @@
 #include <string>
 
 #include "hs_internal.cuh"
+#include "hs_mixed.cuh"
 
 namespace hs {
 namespace {
@@ -309,8 +310,8 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
         set_error("hs_gp_solve_host: null pointer");
         return HS_ERR_INVALID_ARG;
     }
-    if (algorithm != 0 && algorithm != 1) {
-        set_error("hs_gp_solve_host: algorithm must be 0 (cholesky) or 1 (cg)");
+    if (algorithm < 0 || algorithm > 2) {
+        set_error("hs_gp_solve_host: algorithm must be 0 (cholesky), 1 (cg) or 2 (mixed precision + refinement)");
         return HS_ERR_INVALID_ARG;
     }
     const int64_t N = ctx->N;
@@ -359,10 +360,17 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
         HS_E2E(cudaMemcpyAsync(xd, bd, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         st = solve_driver(ctx, Ad, xd);
         if (st != HS_OK) { cleanup(); return st; }
-    } else {
+    } else if (algorithm == 1) {
         HS_E2E(cudaEventRecord(ev[2], s));
         st = cg_driver(ctx, Ad, bd, xd, epsilon, iMax, &iters, nullptr, nullptr);
         if (st != HS_OK && st != HS_ERR_NO_CONVERGENCE) { cleanup(); return st; }
+    } else {
+        // mixed precision: epsilon is the backward-error target, iMax the refinement step limit
+        hs_mixed_report mr{};
+        st = mixed_solve_impl(ctx, Ad, bd, xd, HS_PRECISION_TF32X3, epsilon, (int)iMax, &mr);
+        if (st != HS_OK) { cleanup(); return st; }
+        iters = mr.refinement_steps + mr.pcg_iterations;
+        HS_E2E(cudaEventRecord(ev[2], s));
     }
     HS_E2E(cudaEventRecord(ev[3], s));
     HS_E2E(cudaMemcpyAsync(x_host, xd, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -60,6 +60,13 @@ const char* hs_status_string(hs_status s);
 hs_status hs_ctx_create(int device, void* stream, hs_ctx* out);
 hs_status hs_ctx_destroy(hs_ctx ctx);
 hs_status hs_ctx_set_stream(hs_ctx ctx, void* stream);
+/* The context keeps grow-only device buffers between calls (reduction partials,
+ * matvec partial sums, solver work vectors, the mixed-precision workspace);
+ * this frees them all (after synchronising the stream).  They are allocated
+ * again by the next call that needs them.  No reference counterpart (the
+ * reference's solvers free their device copies in their destructors,
+ * Cholesky.cpp:18-22). */
+hs_status hs_ctx_release_buffers(hs_ctx ctx);
 /* conf::N and conf::matrixBlockSize (Configuration.hpp:22, :33).  Sets nb. */
 hs_status hs_ctx_set_problem(hs_ctx ctx, int64_t N, int matrixBlockSize);
 hs_status hs_sync(hs_ctx ctx);
@@ -213,8 +220,11 @@ hs_status hs_cg_solve(hs_ctx ctx, const double* A, const double* b, double* x, d
 
 /* End-to-end GP solve through host buffers, the path of GaussianProcess::start's
  * solve (src/gaussianProcess/GaussianProcess.cpp:20-40) and main.cpp:201-249:
- * X_host (N x d), y_host (N) -> RBF assembly -> factor + solve (algorithm 0) or
- * CG (algorithm 1) -> x_host (N).  Device buffers are allocated inside. */
+ * X_host (N x d), y_host (N) -> RBF assembly -> factor + solve (algorithm 0),
+ * CG (algorithm 1: epsilon, iMax as in hs_cg_solve) or the mixed-precision solve
+ * (algorithm 2, no reference counterpart: epsilon = backward-error target, iMax =
+ * refinement step limit; report->factor_ms then covers factor and refinement) ->
+ * x_host (N).  Device buffers are allocated inside. */
 typedef struct hs_solve_report {
     int64_t info;            /* factor: -1 or failing row */
     int64_t iterations;      /* CG iterations (algorithm 1) */

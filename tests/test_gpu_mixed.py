@@ -100,3 +100,24 @@ def test_mixed_ill_conditioned_falls_back_or_converges(hs, ctx):
     xg = x.cpu().numpy()[:1024]
     bwd = np.linalg.norm(y - Kd @ xg) / (np.linalg.norm(Kd, "fro") * np.linalg.norm(xg))
     assert bwd <= 2e-14
+
+
+def test_gp_solve_host_mixed(hs):
+    """hs_gp_solve_host, algorithm 2: host X, y in, host x out, through the mixed solve."""
+    N, bsz, d = 900, 128, 8
+    rng = np.random.default_rng(21)
+    X = rng.random((N, d))
+    y = np.sin(X.sum(axis=1)) + 0.1 * rng.standard_normal(N)
+    with hs.Context(device=0) as c:
+        c.set_problem(N, bsz)
+        x, rep = hs.gp_solve_host(c, X, y, 0.5, 1.0, 1e-2, algorithm="mixed", epsilon=1e-14, iMax=30)
+        A = hs.SymmetricMatrix(N, bsz, device="cuda:0")
+        hs.MatrixGenerator.assemble(c, A.matrixData, X, 0.5, 1.0, 1e-2)
+        Kd = A.to_dense()
+        hs._lib.call("hs_ctx_release_buffers", c.handle)
+        # a call after the release allocates again
+        x2, _ = hs.gp_solve_host(c, X, y, 0.5, 1.0, 1e-2, algorithm="mixed", epsilon=1e-14, iMax=30)
+    bwd = np.linalg.norm(y - Kd @ x) / (np.linalg.norm(Kd, "fro") * np.linalg.norm(x))
+    assert bwd <= 2e-14
+    assert rep.iterations >= 1
+    np.testing.assert_array_equal(x, x2)
