@@ -48,13 +48,19 @@ class MixedReport(ctypes.Structure):
                 ("total_ms", ctypes.c_double)]
 
 
+class GpReport(ctypes.Structure):
+    _fields_ = [("factor_ms", ctypes.c_double), ("adjoint_ms", ctypes.c_double), ("grad_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double), ("data_fit", ctypes.c_double), ("logdet", ctypes.c_double)]
+
+
 class KernelProfile(ctypes.Structure):
     _fields_ = [("launches", ctypes.c_int64), ("ms", ctypes.c_double), ("flops", ctypes.c_double),
                 ("bytes", ctypes.c_double)]
 
 
 # hs_kernel_id
-KERNEL_IDS = {"update": 0, "potrf": 1, "trsm": 2, "symv": 3, "trsv": 4, "colupd": 5, "assemble": 6, "vector": 7}
+KERNEL_IDS = {"update": 0, "potrf": 1, "trsm": 2, "symv": 3, "trsv": 4, "colupd": 5, "assemble": 6, "vector": 7,
+              "adjoint": 8, "grad": 9}
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -100,6 +106,8 @@ SIGNATURES = {
     "hs_gp_solve_host": [_P, _P, _P, _I, _P, _I, _D, _D, _I, _D, _I64, _P, ctypes.POINTER(SolveReport)],
     "hs_mixed_solve": [_P, _P, _P, _P, _I, _D, _I, ctypes.POINTER(MixedReport)],
     "hs_cholesky_logdet": [_P, _P, ctypes.POINTER(_D)],
+    "hs_cholesky_adjoint": [_P, _P, _P],
+    "hs_gp_nlml_grad": [_P, _P, _P, _I, _P, _I, ctypes.POINTER(_D), _P, ctypes.POINTER(GpReport)],
 }
 _RESTYPES = {"hs_abi_version": _I, "hs_last_error": ctypes.c_char_p, "hs_status_string": ctypes.c_char_p,
              "hs_packed_matrix_size": _I64, "hs_padded_vector_size": _I64, "hs_ctx_launch_count": _I64}

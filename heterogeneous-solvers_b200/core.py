@@ -16,13 +16,14 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import HSError, MixedReport, NoConvergenceError, NotSPDError, SolveReport, call
+from ._lib import GpReport, HSError, MixedReport, NoConvergenceError, NotSPDError, SolveReport, call
 
 __all__ = [
     "Context", "SymmetricMatrix", "RightHandSide", "MatrixOperations", "MatrixMatrixOperations",
     "MatrixVectorOperations", "VectorOperations", "Cholesky", "TriangularSystemSolver", "CG",
     "MatrixGenerator", "MatrixParser", "HSError", "NotSPDError", "NoConvergenceError", "block_id",
     "packed_size", "padded_size", "gp_solve_host", "MixedPrecisionSolver", "cholesky_logdet", "PRECISIONS",
+    "cholesky_adjoint", "gp_nlml_grad", "GaussianProcessNLML",
 ]
 
 # hs_precision
@@ -435,6 +436,61 @@ class MixedPrecisionSolver:
         self.report = {f: getattr(rep, f) for f, _ in MixedReport._fields_ if f != "reserved"}
         _lib.check(status)
         return x
+
+
+def cholesky_adjoint(ctx, L, Abar):
+    """Reverse-mode blocked Cholesky: on entry ``Abar`` (packed, device) holds
+    the adjoint of a scalar with respect to the lower blocks of the factor
+    ``L``; on exit it holds the adjoint with respect to the lower entries of
+    A = L L^T.  FP64 tensor-core products; L is not modified."""
+    call("hs_cholesky_adjoint", ctx.handle, _dptr(L, ctx), _dptr(Abar, ctx))
+    return Abar
+
+
+def gp_nlml_grad(ctx, X, y, theta, n_ell=None):
+    """GP negative log marginal likelihood and its gradient with respect to
+    theta = [log l_1..log l_n_ell, log sf2, log sn2] (FP64 factor, reverse-mode
+    Cholesky and an on-the-fly dK/dtheta contraction).  X (N x d) and y (N)
+    may be host or device float64 arrays; returns (nlml, grad ndarray, report)."""
+    Xd = X if isinstance(X, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(X, dtype=np.float64))
+    yd = y if isinstance(y, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(y, dtype=np.float64))
+    Xd = _to_device(Xd.to(torch.float64), ctx).contiguous()
+    yd = _to_device(yd.to(torch.float64), ctx).contiguous()
+    if Xd.dim() != 2 or Xd.shape[0] != ctx.N or yd.numel() != ctx.N:
+        raise ValueError("X must be N x d and y of length N (N of the context)")
+    th = np.ascontiguousarray(np.asarray(theta, dtype=np.float64).ravel())
+    if n_ell is None:
+        n_ell = th.size - 2
+    if th.size != n_ell + 2:
+        raise ValueError("theta must hold n_ell + 2 values")
+    nlml = ctypes.c_double()
+    grad = np.zeros(n_ell + 2)
+    rep = GpReport()
+    call("hs_gp_nlml_grad", ctx.handle, _dptr(Xd, ctx), _dptr(yd, ctx), int(Xd.shape[1]),
+         th.ctypes.data_as(ctypes.c_void_p), int(n_ell), ctypes.byref(nlml), grad.ctypes.data_as(ctypes.c_void_p),
+         ctypes.byref(rep))
+    return nlml.value, grad, {f: getattr(rep, f) for f, _ in GpReport._fields_}
+
+
+class GaussianProcessNLML(torch.autograd.Function):
+    """torch.autograd.Function over hs_gp_nlml_grad: forward returns the NLML
+    of theta (a float64 tensor of n_ell + 2 log-parameters), backward returns
+    the library's analytic gradient times the incoming gradient.
+
+        nlml = GaussianProcessNLML.apply(theta, X, y, ctx)
+    """
+
+    @staticmethod
+    def forward(fctx, theta, X, y, ctx):
+        th = theta.detach().to("cpu", torch.float64).numpy()
+        value, grad, _ = gp_nlml_grad(ctx, X, y, th)
+        fctx.save_for_backward(torch.from_numpy(grad).to(theta.device, theta.dtype))
+        return torch.tensor(value, dtype=theta.dtype, device=theta.device)
+
+    @staticmethod
+    def backward(fctx, g):
+        (grad,) = fctx.saved_tensors
+        return g * grad, None, None, None
 
 
 class MatrixGenerator:

@@ -1,0 +1,370 @@
+// k_adjoint.cu — reverse-mode (adjoint) blocked Cholesky on the FP64 tensor
+// cores, and the kernels of the GP marginal-likelihood gradient.
+//
+// No reference counterpart (new form).  The reverse sweep undoes the
+// right-looking factor of src/solver/cholesky/Cholesky.cpp:446-471 block
+// column by block column, k = nb-1 .. 0.  With Abar the adjoint of the lower
+// entries of A (initially the adjoint Lbar of the factor), P the panel rows
+// r > k of column k and D = L_kk:
+//   (i)   Lbar_P -= (Abar + Abar^T)_trailing * L_P      (trailing block SYMM)
+//   (ii)  Abar_P  = Lbar_P * D^-1                        (reverse of the TRSM)
+//   (iii) Dbar   -= tril(sum_r Abar_rk^T L_rk)          (the TRSM's use of D)
+//   (iv)  Abar_kk = tril_h(D^-T (H + H^T) D^-1),  H = tril_h(D^T Dbar)
+// where tril_h keeps the lower triangle with the diagonal halved.  (iv) is
+// the level-3 form of the reverse of an unblocked Cholesky (I. Murray,
+// "Differentiation of the Cholesky decomposition", 2016): from A = L L^T,
+// L^-1 dA L^-T = X + X^T with X = L^-1 dL lower triangular, so dL =
+// L tril_h(L^-1 dA L^-T), and tr(Lbar^T dL) = tr(sym(H) L^-1 dA L^-T) with
+// H = tril_h(L^T Lbar).  Every product runs on the FP64 tensor pipe
+// (mma.sync m8n8k4 f64) in the chained tile kernel below.
+#include <cmath>
+
+#include "hs_gp.cuh"
+
+namespace hs {
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4;
+constexpr int SPAD = 20;   // row pitch (doubles) of K-contiguous operand rows
+constexpr int LDT = 136;   // row pitch (doubles) of M/N-contiguous operand rows
+constexpr int kStageA = BM * SPAD;  // >= BK * LDT
+constexpr int kStage = 2 * kStageA;
+constexpr int kChainSmem = STAGES * kStage * (int)sizeof(double);  // 160 KB
+static_assert(BK * LDT <= kStageA, "stage layout");
+
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+        : "+d"(d[0]), "+d"(d[1])
+        : "d"(a), "d"(b));
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// One element of a product chain: op(A) op(B), both bsz x bsz row-major blocks.
+struct Elem {
+    const double* A;
+    const double* B;
+    int ta, tb;  // 1: the operand enters transposed
+};
+
+__device__ __forceinline__ Elem chain_elem(const ChainArgs& a, int item, int64_t q) {
+    const int64_t bb = (int64_t)a.bsz * a.bsz;
+    Elem e;
+    if (a.mode == CHAIN_SYMM) {
+        // output Lbar_rk, r = k+1+item; chain over c = k+1..r (Abar_rc L_ck) then
+        // c = r..nb-1 (Abar_cr^T L_ck): the symmetric trailing adjoint times the panel
+        const int k = a.k, r = k + 1 + item;
+        if (q < r - k) {
+            const int c = k + 1 + (int)q;
+            e.A = a.Abar + block_id(r, c, a.nb) * bb;
+            e.B = a.L + block_id(c, k, a.nb) * bb;
+            e.ta = 0;
+        } else {
+            const int c = r + (int)(q - (r - k));
+            e.A = a.Abar + block_id(c, r, a.nb) * bb;
+            e.B = a.L + block_id(c, k, a.nb) * bb;
+            e.ta = 1;
+        }
+        e.tb = 0;
+    } else {
+        // strided list: element q of item: A0 + item*sAi + q*sAq, B0 + item*sBi + q*sBq
+        e.A = a.A0 + item * a.sAi + q * a.sAq;
+        e.B = a.B0 + item * a.sBi + q * a.sBq;
+        e.ta = a.ta;
+        e.tb = a.tb;
+    }
+    return e;
+}
+
+// One CTA = one 128 x 128 tile of one output block, accumulating the chain
+// elements [q0, q1) of its item; 8 warps of 64 x 32, K streamed in 16-wide
+// slabs through a 4-stage cp.async ring.  Operands that enter transposed are
+// staged with the M (or N) index contiguous, the others with K contiguous.
+__global__ void __launch_bounds__(256, 1) chain_dmma_kernel(ChainArgs a) {
+    extern __shared__ __align__(16) double smem[];
+    const int tps = a.bsz / BM;
+    const int64_t idx = blockIdx.x;
+    const int split = (int)(idx % a.splits);
+    const int64_t rest = idx / a.splits;
+    const int tile = (int)(rest % (tps * tps));
+    const int item = (int)(rest / (tps * tps));
+    const int ti = tile / tps, tj = tile % tps;
+    const int64_t q0 = a.chain * split / a.splits, q1 = a.chain * (split + 1) / a.splits;
+    const int spb = a.bsz / BK;  // slabs per chain element
+    const int64_t nk = (q1 - q0) * spb;
+    const int bsz = a.bsz;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int wm = warp >> 2, wn = warp & 3;
+    const int g = lane >> 2, t = lane & 3;
+
+    double acc[8][4][2];
+#pragma unroll
+    for (int mi = 0; mi < 8; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+
+    auto load_stage = [&](int stage, int64_t kt) {
+        const Elem e = chain_elem(a, item, q0 + kt / spb);
+        const int kc = (int)(kt % spb) * BK;
+        double* As = smem + stage * kStage;
+        double* Bs = As + kStageA;
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) {
+            const int x = tid + 256 * qq;
+            if (!e.ta) {  // A_op[m][k] = A[ti*128+m][kc+k]: rows m, K contiguous
+                const int row = x >> 3, ch = x & 7;
+                cp_async16(As + row * SPAD + ch * 2, e.A + (size_t)(ti * BM + row) * bsz + kc + ch * 2);
+            } else {      // A_op[m][k] = A[kc+k][ti*128+m]: rows k, M contiguous
+                const int row = x >> 6, ch = x & 63;
+                cp_async16(As + row * LDT + ch * 2, e.A + (size_t)(kc + row) * bsz + ti * BM + ch * 2);
+            }
+            if (!e.tb) {  // B_op[k][n] = B[kc+k][tj*128+n]: rows k, N contiguous
+                const int row = x >> 6, ch = x & 63;
+                cp_async16(Bs + row * LDT + ch * 2, e.B + (size_t)(kc + row) * bsz + tj * BN + ch * 2);
+            } else {      // B_op[k][n] = B[tj*128+n][kc+k]: rows n, K contiguous
+                const int row = x >> 3, ch = x & 7;
+                cp_async16(Bs + row * SPAD + ch * 2, e.B + (size_t)(tj * BN + row) * bsz + kc + ch * 2);
+            }
+        }
+    };
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+        if (s < nk) load_stage(s, s);
+        cp_async_commit();
+    }
+    for (int64_t kt = 0; kt < nk; ++kt) {
+        cp_async_wait<STAGES - 2>();
+        __syncthreads();
+        {
+            const int64_t nx = kt + STAGES - 1;
+            if (nx < nk) load_stage((int)(nx % STAGES), nx);
+            cp_async_commit();
+        }
+        const Elem e = chain_elem(a, item, q0 + kt / spb);
+        const double* As = smem + (int)(kt % STAGES) * kStage;
+        const double* Bs = As + kStageA;
+#pragma unroll
+        for (int kk = 0; kk < BK / 4; ++kk) {
+            double av[8], bv[4];
+            if (!e.ta) {
+#pragma unroll
+                for (int mi = 0; mi < 8; ++mi) av[mi] = As[(wm * 64 + mi * 8 + g) * SPAD + kk * 4 + t];
+            } else {
+#pragma unroll
+                for (int mi = 0; mi < 8; ++mi) av[mi] = As[(kk * 4 + t) * LDT + wm * 64 + mi * 8 + g];
+            }
+            if (!e.tb) {
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(kk * 4 + t) * LDT + wn * 32 + ni * 8 + g];
+            } else {
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(wn * 32 + ni * 8 + g) * SPAD + kk * 4 + t];
+            }
+#pragma unroll
+            for (int mi = 0; mi < 8; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma884(acc[mi][ni], av[mi], bv[ni]);
+        }
+    }
+    cp_async_wait<0>();
+
+    // ---- epilogue
+    const int64_t bb = (int64_t)bsz * bsz;
+    double* C;
+    int epi = a.epi;
+    if (a.splits > 1) {
+        C = a.partial + ((int64_t)split * a.items + item) * bb;
+        epi = EPI_STORE;
+    } else if (a.mode == CHAIN_SYMM) {
+        C = a.Abar + block_id(a.k + 1 + item, a.k, a.nb) * bb;
+    } else {
+        C = a.C0 + item * a.sCi;
+    }
+    const double alpha = a.alpha;
+#pragma unroll
+    for (int mi = 0; mi < 8; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+            const int r = ti * BM + wm * 64 + mi * 8 + g;
+            const int c = tj * BN + wn * 32 + ni * 8 + 2 * t;
+            double* p = C + (size_t)r * bsz + c;
+            const double v0 = alpha * acc[mi][ni][0], v1 = alpha * acc[mi][ni][1];
+            if (epi == EPI_STORE) {
+                *reinterpret_cast<double2*>(p) = make_double2(v0, v1);
+            } else if (epi == EPI_ADD) {
+                double2 o = *reinterpret_cast<double2*>(p);
+                o.x += v0;
+                o.y += v1;
+                *reinterpret_cast<double2*>(p) = o;
+            } else if (epi == EPI_ADD_LOWER) {
+                if (c <= r) p[0] += v0;
+                if (c + 1 <= r) p[1] += v1;
+            } else {  // EPI_TRIL_HALF: lower triangle, diagonal halved, upper zero
+                p[0] = c < r ? v0 : (c == r ? 0.5 * v0 : 0.0);
+                p[1] = c + 1 < r ? v1 : (c + 1 == r ? 0.5 * v1 : 0.0);
+            }
+        }
+}
+
+// C (+)= sum over splits of the partial blocks, in split order
+__global__ void reduce_splits_kernel(const double* __restrict__ partial, int splits, int items, int64_t bb,
+                                     const ChainArgs a) {
+    const int item = blockIdx.y;
+    double* C;
+    if (a.mode == CHAIN_SYMM) C = a.Abar + block_id(a.k + 1 + item, a.k, a.nb) * bb;
+    else C = a.C0 + item * a.sCi;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < bb; e += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int sp = 0; sp < splits; ++sp) s += partial[((int64_t)sp * items + item) * bb + e];
+        const int r = (int)(e / a.bsz), c = (int)(e % a.bsz);
+        if (a.epi == EPI_STORE) C[e] = s;
+        else if (a.epi == EPI_ADD) C[e] += s;
+        else if (a.epi == EPI_ADD_LOWER) {
+            if (c <= r) C[e] += s;
+        } else {
+            C[e] = c < r ? s : (c == r ? 0.5 * s : 0.0);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ helpers
+// Abar = 0 except diag(Abar_kk) = 1 / L_ii for valid rows: the adjoint of
+// sum_i log L_ii with respect to L
+__global__ void zero_kernel(double* __restrict__ p, int64_t total) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
+        p[e] = 0.0;
+}
+__global__ void set_logdet_diag_kernel(const double* __restrict__ L, double* __restrict__ Abar, int bsz, int nb,
+                                       int64_t N) {
+    const int64_t bb = (int64_t)bsz * bsz;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(i / bsz), r = (int)(i % bsz);
+        const int64_t off = block_id(k, k, nb) * bb + (int64_t)r * bsz + r;
+        Abar[off] = 1.0 / L[off];
+    }
+}
+
+// Dp = D with unit diagonal on the rows >= valid (padding rows of the last
+// block): the padded factor is diag(L, I), so its diagonal blocks are invertible
+__global__ void pad_unit_diag_kernel(const double* __restrict__ D, double* __restrict__ Dp, int bsz, int valid) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < bsz * bsz; e += gridDim.x * blockDim.x) {
+        const int i = e / bsz, j = e % bsz;
+        Dp[e] = (i == j && i >= valid) ? 1.0 : D[e];
+    }
+}
+
+// zero the strict upper triangles of the diagonal blocks (the adjoint of a
+// lower-triangular factor has none)
+__global__ void zero_diag_upper_kernel(double* __restrict__ Abar, int bsz, int nb) {
+    const int64_t bb = (int64_t)bsz * bsz;
+    double* D = Abar + block_id(blockIdx.y, blockIdx.y, nb) * bb;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < bsz * bsz; e += gridDim.x * blockDim.x)
+        if (e % bsz > e / bsz) D[e] = 0.0;
+}
+
+__global__ void identity_kernel(double* __restrict__ Y, int bsz) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < bsz * bsz; e += gridDim.x * blockDim.x)
+        Y[e] = (e / bsz == e % bsz) ? 1.0 : 0.0;
+}
+
+// M = H + H^T with H = tril_h(G): M_ij = G_ij (i > j), G_ji (i < j), G_ii (i == j)
+__global__ void sym_tril_half_kernel(const double* __restrict__ G, double* __restrict__ M, int bsz) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < bsz * bsz; e += gridDim.x * blockDim.x) {
+        const int i = e / bsz, j = e % bsz;
+        M[e] = i >= j ? G[e] : G[(size_t)j * bsz + i];
+    }
+}
+
+int pick_splits(int64_t base_ctas, int64_t chain, int items, int64_t partial_blocks, int sms) {
+    int64_t s = (2LL * sms + base_ctas - 1) / base_ctas;
+    if (s > chain) s = chain;
+    if (s < 1) s = 1;
+    while (s > 1 && s * items > partial_blocks) --s;
+    return (int)s;
+}
+
+bool g_chain_attr[64] = {};
+
+hs_status chain_attrs() {
+    int dev = 0;
+    HS_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && g_chain_attr[dev]) return HS_OK;
+    HS_CUDA(cudaFuncSetAttribute(chain_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kChainSmem));
+    if (dev >= 0 && dev < 64) g_chain_attr[dev] = true;
+    return HS_OK;
+}
+
+}  // namespace
+
+hs_status launch_chain(hs_ctx ctx, ChainArgs a, double* partial, int64_t partial_blocks, cudaStream_t s) {
+    hs_status st = chain_attrs();
+    if (st != HS_OK) return st;
+    HS_REQUIRE(a.bsz == 128 || a.bsz == 256, "the tensor-core adjoint supports matrixBlockSize 128 or 256");
+    if (a.items <= 0 || a.chain <= 0) return HS_OK;
+    const int tps = a.bsz / BM;
+    const int64_t base = (int64_t)a.items * tps * tps;
+    a.splits = (partial && a.allow_split) ? pick_splits(base, a.chain, a.items, partial_blocks, ctx->num_sms) : 1;
+    a.partial = partial;
+    const int64_t grid = base * a.splits;
+    HS_REQUIRE(grid < (1LL << 31), "too many tiles");
+    const double n3 = (double)a.bsz * a.bsz * a.bsz;
+    prof_begin(ctx, s, HS_KERNEL_ADJOINT);
+    ctx->launches += 1;
+    chain_dmma_kernel<<<(unsigned)grid, 256, kChainSmem, s>>>(a);
+    HS_CHECK_LAUNCH("chain_dmma_kernel");
+    prof_end(ctx, s, HS_KERNEL_ADJOINT, 2.0 * n3 * (double)a.chain * a.items,
+             8.0 * (double)a.bsz * a.bsz * (2.0 * a.chain * a.items + 2.0 * a.items));
+    if (a.splits > 1) {
+        const int64_t bb = (int64_t)a.bsz * a.bsz;
+        ctx->launches += 1;
+        dim3 grid2((unsigned)((bb + 255) / 256 < 64 ? (bb + 255) / 256 : 64), (unsigned)a.items);
+        reduce_splits_kernel<<<grid2, 256, 0, s>>>(partial, a.splits, a.items, bb, a);
+        HS_CHECK_LAUNCH("reduce_splits");
+    }
+    return HS_OK;
+}
+
+hs_status launch_logdet_adjoint_init(hs_ctx ctx, const double* L, double* Abar, cudaStream_t s) {
+    const int64_t total = total_blocks(ctx->nb) * (int64_t)ctx->bsz * ctx->bsz;
+    ctx->launches += 2;
+    zero_kernel<<<4 * ctx->num_sms, 256, 0, s>>>(Abar, total);
+    set_logdet_diag_kernel<<<64, 256, 0, s>>>(L, Abar, ctx->bsz, ctx->nb, ctx->N);
+    HS_CHECK_LAUNCH("logdet adjoint init");
+    return HS_OK;
+}
+
+hs_status launch_pad_unit_diag(hs_ctx ctx, const double* D, double* Dp, int valid, cudaStream_t s) {
+    ctx->launches += 1;
+    pad_unit_diag_kernel<<<64, 256, 0, s>>>(D, Dp, ctx->bsz, valid);
+    HS_CHECK_LAUNCH("pad diag");
+    return HS_OK;
+}
+
+hs_status launch_zero_diag_upper(hs_ctx ctx, double* Abar, cudaStream_t s) {
+    ctx->launches += 1;
+    zero_diag_upper_kernel<<<dim3(16, ctx->nb), 256, 0, s>>>(Abar, ctx->bsz, ctx->nb);
+    HS_CHECK_LAUNCH("zero diag upper");
+    return HS_OK;
+}
+
+hs_status launch_identity(hs_ctx ctx, double* Y, cudaStream_t s) {
+    ctx->launches += 1;
+    identity_kernel<<<64, 256, 0, s>>>(Y, ctx->bsz);
+    HS_CHECK_LAUNCH("identity");
+    return HS_OK;
+}
+
+hs_status launch_sym_tril_half(hs_ctx ctx, const double* G, double* M, cudaStream_t s) {
+    ctx->launches += 1;
+    sym_tril_half_kernel<<<64, 256, 0, s>>>(G, M, ctx->bsz);
+    HS_CHECK_LAUNCH("sym tril half");
+    return HS_OK;
+}
+
+}  // namespace hs

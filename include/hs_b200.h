@@ -90,7 +90,9 @@ typedef enum hs_kernel_id {
     HS_KERNEL_COLUPD = 5,
     HS_KERNEL_ASSEMBLE = 6,
     HS_KERNEL_VECTOR = 7,    /* vector ops, dots, CG updates */
-    HS_KERNEL_COUNT = 8
+    HS_KERNEL_ADJOINT = 8,   /* reverse-mode Cholesky block products (FP64 DMMA) */
+    HS_KERNEL_GRAD = 9,      /* GP gradient contraction */
+    HS_KERNEL_COUNT = 10
 } hs_kernel_id;
 typedef struct hs_kernel_profile {
     int64_t launches;
@@ -268,6 +270,36 @@ hs_status hs_mixed_solve(hs_ctx ctx, const double* K, const double* b, double* x
 /* log|K| = 2 sum_i log L_ii of a factor from hs_cholesky_factor (packed, device);
  * *logdet is a host pointer. */
 hs_status hs_cholesky_logdet(hs_ctx ctx, const double* L, double* logdet);
+
+/* ------------------------------------------------------------------ differentiation
+ * No reference counterpart (new form).  Reverse-mode blocked Cholesky: with L
+ * the packed factor of A = L L^T (hs_cholesky_factor) and Abar holding, on
+ * entry, the adjoint Lbar of some scalar f with respect to the lower blocks of
+ * L (only the lower triangle of its diagonal blocks is read), Abar is
+ * overwritten by the adjoint of f with respect to the lower entries of A
+ * (entry (i,j), i >= j, of the packed storage: df = sum_{i>=j} Abar_ij dA_ij).
+ * Products run on the FP64 tensor cores; matrixBlockSize 128 or 256.  L is not
+ * modified.  Allocates a workspace of (nb + 132) blocks. */
+hs_status hs_cholesky_adjoint(hs_ctx ctx, const double* L, double* Abar);
+
+/* GP negative log marginal likelihood and its gradient.  X (N x d, row major)
+ * and y (N) are device arrays; theta (host) = [log l_1 .. log l_n_ell, log sf2,
+ * log sn2] with n_ell = 1 (isotropic) or d (ARD), K = sf2 exp(-1/2 sum_k
+ * (x_ik - x_jk)^2 / l_k^2) + sn2 I (hs_rbf_assemble's matrix).
+ *   *nlml = 1/2 y^T K^-1 y + 1/2 log|K| + N/2 log 2pi
+ *   grad[q] = dNLML/dtheta_q = 1/2 tr((K^-1 - alpha alpha^T) dK/dtheta_q)
+ * (host, n_ell + 2 values; may be NULL).  FP64 factor on the tensor cores,
+ * the gradient through hs_cholesky_adjoint of sum log L_ii and an on-the-fly
+ * contraction that recomputes dK/dtheta from X (nothing of size N^2 besides L
+ * and its adjoint is stored).  d <= 32; matrixBlockSize 128 or 256.  Returns
+ * HS_ERR_NOT_SPD when K(theta) has no Cholesky factor. */
+typedef struct hs_gp_report {
+    double factor_ms, adjoint_ms, grad_ms, total_ms;
+    double data_fit;   /* 1/2 y^T K^-1 y */
+    double logdet;     /* log|K| */
+} hs_gp_report;
+hs_status hs_gp_nlml_grad(hs_ctx ctx, const double* X, const double* y, int d, const double* theta, int n_ell,
+                          double* nlml, double* grad, hs_gp_report* report);
 
 #ifdef __cplusplus
 }
