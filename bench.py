@@ -65,6 +65,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
     ap.add_argument("--tol", type=float, default=1e-14, help="backward-error target of the mixed solve")
+    ap.add_argument("--lml-n", type=int, default=16384, help="N of the NLML+gradient leg (0: skip)")
+    ap.add_argument("--lml-steps", type=int, default=3)
     return ap.parse_args()
 
 
@@ -195,6 +197,46 @@ def measure_gemm_peak(torch, device, dtype, tf32=False):
     del a, b
     torch.cuda.empty_cache()
     return best
+
+
+def bench_lml(hs, torch, device, N, steps):
+    """NLML + gradient of an ARD RBF GP: X ~ U[0,1]^(N x 8), l_k ~ LogUniform[0.2, 2],
+    sf2 = 1, sn2 = 1e-3, y drawn from the GP prior plus noise (a dense FP64
+    Cholesky of K through torch draws it; not timed).  Times hs_gp_nlml_grad
+    (assembly, FP64 factor, solve, reverse-mode Cholesky, gradient contraction)."""
+    import numpy as np
+    d, bsz = 8, 256
+    rng = np.random.default_rng(4)
+    X = rng.random((N, d))
+    ell = np.exp(rng.uniform(np.log(0.2), np.log(2.0), d))
+    theta = np.concatenate([np.log(ell), [0.0, np.log(1e-3)]])
+    dev = f"cuda:{device}"
+    Xd = torch.from_numpy(X).to(dev)
+    Xs = Xd / torch.from_numpy(ell).to(dev)
+    K = torch.exp(-0.5 * torch.cdist(Xs, Xs).square()) + 1e-3 * torch.eye(N, dtype=torch.float64, device=dev)
+    z = torch.from_numpy(rng.standard_normal(N)).to(dev)
+    yd = torch.linalg.cholesky(K) @ z
+    del K, Xs
+    torch.cuda.empty_cache()
+    c = hs.Context(device=device, N=N, matrixBlockSize=bsz)
+    hs.gp_nlml_grad(c, Xd, yd, theta)  # warm-up
+    torch.cuda.synchronize()
+    c.reset_profile()
+    c.set_profiling(True)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        nlml, grad, rep = hs.gp_nlml_grad(c, Xd, yd, theta)
+    t_ms = (time.perf_counter() - t0) * 1e3 / steps
+    c.set_profiling(False)
+    adj = c.read_profile("adjoint")
+    c.close()
+    return {"workload": f"GP NLML + gradient, ARD RBF, N={N}, d={d}, bsz={bsz}, sn2=1e-3, y ~ GP prior",
+            "ms_per_call": t_ms, "nlml": nlml, "grad_norm": float(np.linalg.norm(grad)),
+            "phases_ms": {"assemble+factor": rep["factor_ms"], "solve+adjoint": rep["adjoint_ms"],
+                          "gradient": rep["grad_ms"]},
+            "adjoint_dmma_tflops": adj["flops"] / (adj["ms"] * 1e-3) / 1e12 if adj["ms"] else None,
+            "adjoint_launches_per_call": adj["launches"] / steps,
+            "useful_tflops_whole": (N ** 3 / 3 + 2 * N ** 3 / 3) / (t_ms * 1e-3) / 1e12}
 
 
 def main():
@@ -341,6 +383,11 @@ def main():
         fp64["logdet"] = logdet64
         del x64
 
+    # ---------------- GP NLML + gradient (ARD, d = 8) at N = 16384
+    lml = None
+    if args.lml_n > 0:
+        lml = bench_lml(hs, torch, ctx.device, args.lml_n, args.lml_steps)
+
     # ---------------- CG matvec roofline: a bounded number of CG iterations on K
     cg_info = None
     if args.cg_iters > 0:
@@ -428,7 +475,7 @@ def main():
             "roofline": {"bound": "tensor", "achieved": useful,
                          "peak": tf32_peak / 3.0 if useful else None, "unit": "TFLOP/s",
                          "frac": useful / (tf32_peak / 3.0) if useful else None, "traffic": traffic,
-                         "kernel": "tc_tile_kernel<256, update> (3xTF32 SYRK+GEMM trailing update, tcgen05)",
+                         "kernel": "tc_update_kernel<256> (3xTF32 SYRK+GEMM trailing update, tcgen05, persistent)",
                          "peak_source": "cuBLAS TF32 GEMM 8192^3 measured in this run, divided by the 3 TF32 "
                                         "products of one split FP32 product (TF32 is absent from "
                                         "MEASURED_PEAKS.json)",
@@ -436,7 +483,7 @@ def main():
                          "issued_tf32_tflops": 3 * useful if useful else None},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "phases": phases, "mixed": mixed_report, "backward_error": bwd_mixed, "fp64": fp64,
-            "cg": cg_info,
+            "lml_grad": lml, "cg": cg_info,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

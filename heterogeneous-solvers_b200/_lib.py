@@ -107,6 +107,9 @@ SIGNATURES = {
     "hs_mixed_solve": [_P, _P, _P, _P, _I, _D, _I, ctypes.POINTER(MixedReport)],
     "hs_cholesky_logdet": [_P, _P, ctypes.POINTER(_D)],
     "hs_cholesky_adjoint": [_P, _P, _P],
+    "hs_gp_test_kernel_matrix": [_P, _P, _P, _I64, _I, _P, _I, _D, _P],
+    "hs_matrix_vector_gp": [_P, _P, _P, _P, _I64, _I64],
+    "hs_gp_predict": [_P, _P, _P, _I64, _I, _P, _I, _D, _P, _P],
     "hs_gp_nlml_grad": [_P, _P, _P, _I, _P, _I, ctypes.POINTER(_D), _P, ctypes.POINTER(GpReport)],
 }
 _RESTYPES = {"hs_abi_version": _I, "hs_last_error": ctypes.c_char_p, "hs_status_string": ctypes.c_char_p,

@@ -23,7 +23,8 @@ __all__ = [
     "MatrixVectorOperations", "VectorOperations", "Cholesky", "TriangularSystemSolver", "CG",
     "MatrixGenerator", "MatrixParser", "HSError", "NotSPDError", "NoConvergenceError", "block_id",
     "packed_size", "padded_size", "gp_solve_host", "MixedPrecisionSolver", "cholesky_logdet", "PRECISIONS",
-    "cholesky_adjoint", "gp_nlml_grad", "GaussianProcessNLML",
+    "cholesky_adjoint", "gp_nlml_grad", "GaussianProcessNLML", "GaussianProcess", "gp_predict",
+    "UtilityFunctions", "fit_hyperparameters",
 ]
 
 # hs_precision
@@ -236,6 +237,11 @@ class MatrixVectorOperations:
     matrixVectorBlock_CPU = matrixVectorBlock
 
     @staticmethod
+    def matrixVectorGP(ctx, A, b, result, n, m):
+        """MatrixVectorOperations.cpp:379-395: result[i] = sum_k A[i*n+k] b[k], i < m."""
+        call("hs_matrix_vector_gp", ctx.handle, _dptr(A, ctx), _dptr(b, ctx), _dptr(result, ctx), int(n), int(m))
+
+    @staticmethod
     def triangularSolveBlockVector(ctx, A, b, blockRow, blockID, transposed):
         call("hs_trsv_block", ctx.handle, _dptr(A, ctx), _dptr(b, ctx), int(blockRow), int(blockID),
              int(bool(transposed)))
@@ -244,6 +250,11 @@ class MatrixVectorOperations:
     def matrixVectorColumnUpdate(ctx, A, b, blockStart, blockCount, blockRow, blockID, blockCountXY, transposed):
         call("hs_column_update", ctx.handle, _dptr(A, ctx), _dptr(b, ctx), int(blockStart), int(blockCount),
              int(blockRow), int(blockID), int(blockCountXY), int(bool(transposed)))
+
+
+def _dev_f64(x, ctx):
+    t = x if isinstance(x, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(x, dtype=np.float64))
+    return _to_device(t.to(torch.float64), ctx).contiguous()
 
 
 class VectorOperations:
@@ -472,6 +483,34 @@ def gp_nlml_grad(ctx, X, y, theta, n_ell=None):
     return nlml.value, grad, {f: getattr(rep, f) for f, _ in GpReport._fields_}
 
 
+def fit_hyperparameters(ctx, X, y, theta0, maxiter=30, n_ell=None, bounds=None):
+    """Fit theta = [log l_1..log l_n_ell, log sf2, log sn2] by L-BFGS (scipy's
+    L-BFGS-B) on the NLML and its analytic gradient (hs_gp_nlml_grad).  X and y
+    are copied to the device once.  Returns a dict with theta, nlml, the
+    number of L-BFGS iterations and function evaluations, and the wall time of
+    every NLML + gradient evaluation."""
+    from scipy.optimize import minimize
+
+    Xd = X if isinstance(X, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(X, dtype=np.float64))
+    yd = y if isinstance(y, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(y, dtype=np.float64))
+    Xd = _to_device(Xd.to(torch.float64), ctx).contiguous()
+    yd = _to_device(yd.to(torch.float64), ctx).contiguous()
+    th0 = np.asarray(theta0, dtype=np.float64).ravel()
+    n_ell = th0.size - 2 if n_ell is None else n_ell
+    evals = []
+
+    def fun(th):
+        t0 = time.perf_counter()
+        v, g, _ = gp_nlml_grad(ctx, Xd, yd, th, n_ell)
+        evals.append({"seconds": time.perf_counter() - t0, "nlml": v})
+        return v, g
+
+    res = minimize(fun, th0, jac=True, method="L-BFGS-B", bounds=bounds, options={"maxiter": int(maxiter)})
+    return {"theta": res.x, "nlml": float(res.fun), "iterations": int(res.nit), "evaluations": len(evals),
+            "eval_seconds": [e["seconds"] for e in evals], "nlml_trace": [e["nlml"] for e in evals],
+            "message": str(res.message)}
+
+
 class GaussianProcessNLML(torch.autograd.Function):
     """torch.autograd.Function over hs_gp_nlml_grad: forward returns the NLML
     of theta (a float64 tensor of n_ell + 2 log-parameters), backward returns
@@ -517,6 +556,21 @@ class MatrixGenerator:
              ell.ctypes.data_as(ctypes.c_void_p), int(ell.size), float(signal_variance), float(noise_variance))
 
     @staticmethod
+    def generateTestKernelMatrix(ctx, X, X_test, lengthscale=1.0, signal_variance=1.0, out=None):
+        """MatrixGenerator.cpp:163-213: K_star (N_test x N, row major, device)
+        with K_star[j, i] = sf2 exp(-|x_i - x*_j|^2 / (2 l^2)) (l scalar or ARD)."""
+        Xd, Xt = _dev_f64(X, ctx), _dev_f64(X_test, ctx)
+        if Xd.dim() != 2 or Xd.shape[0] != ctx.N or Xt.dim() != 2 or Xt.shape[1] != Xd.shape[1]:
+            raise ValueError("X must be N x d and X_test N_test x d")
+        ell = np.atleast_1d(np.asarray(lengthscale, dtype=np.float64))
+        K = out if out is not None else torch.empty((Xt.shape[0], Xd.shape[0]), dtype=torch.float64,
+                                                    device=f"cuda:{ctx.device}")
+        call("hs_gp_test_kernel_matrix", ctx.handle, _dptr(Xd, ctx), _dptr(Xt, ctx), int(Xt.shape[0]),
+             int(Xd.shape[1]), ell.ctypes.data_as(ctypes.c_void_p), int(ell.size), float(signal_variance),
+             _dptr(K, ctx))
+        return K
+
+    @staticmethod
     def generateSPDMatrix(ctx, series, N, matrixBlockSize, lengthscale=1.0, signal_variance=1.0,
                           noise_variance=0.01):
         """generateSPDMatrix (MatrixGenerator.cpp:73-162): the first N values of
@@ -532,6 +586,90 @@ class MatrixGenerator:
         MatrixGenerator.assemble(ctx, A.matrixData, MatrixGenerator.windowInputs(series[:N]), lengthscale,
                                  signal_variance, noise_variance)
         return A
+
+
+def gp_predict(ctx, X, X_test, alpha, lengthscale=1.0, signal_variance=1.0):
+    """Predictive mean K_star alpha with K_star recomputed on the fly (never
+    stored); alpha = K^-1 y of length N (padding beyond N is ignored)."""
+    Xd, Xt = _dev_f64(X, ctx), _dev_f64(X_test, ctx)
+    al = _dev_f64(alpha, ctx)
+    ell = np.atleast_1d(np.asarray(lengthscale, dtype=np.float64))
+    mean = torch.empty(Xt.shape[0], dtype=torch.float64, device=f"cuda:{ctx.device}")
+    call("hs_gp_predict", ctx.handle, _dptr(Xd, ctx), _dptr(Xt, ctx), int(Xt.shape[0]), int(Xd.shape[1]),
+         ell.ctypes.data_as(ctypes.c_void_p), int(ell.size), float(signal_variance), _dptr(al, ctx), _dptr(mean, ctx))
+    return mean
+
+
+class GaussianProcess:
+    """src/gaussianProcess/GaussianProcess.hpp:10-36: the prediction pipeline.
+
+    ``start()`` solves K alpha = y with the Cholesky factor + substitution or
+    with CG (GaussianProcess.cpp:20-40), then forms K_star from the training and
+    test inputs and returns K_star alpha (:42-54), as a host numpy array.
+    Inputs are the reference's one-value-per-line series files (or arrays),
+    windowed into 8 regressors (MatrixGenerator.cpp:76-99), or N x d arrays.
+    """
+
+    def __init__(self, A, train_y, path_train, path_test, ctx, algorithm="cholesky", lengthscale=1.0,
+                 signal_variance=1.0, N_test=None, fused=True):
+        self.A = A
+        self.train_y = train_y
+        self.path_train = path_train
+        self.path_test = path_test
+        self.ctx = ctx
+        self.algorithm = algorithm
+        self.lengthscale = lengthscale
+        self.signal_variance = signal_variance
+        self.N_test = N_test
+        self.fused = fused
+        self.result = None
+
+    @staticmethod
+    def _inputs(src, n=None):
+        """Series file / 1-D series -> 8-regressor window rows; N x d arrays as they are."""
+        a = np.loadtxt(src, dtype=np.float64, ndmin=1) if isinstance(src, (str, Path)) else np.asarray(
+            src, dtype=np.float64)
+        if n is not None and a.shape[0] < n:
+            raise ValueError("Not enough data available!")
+        a = a[:n] if n is not None else a
+        return MatrixGenerator.windowInputs(a) if a.ndim == 1 else a
+
+    def start(self):
+        ctx = self.ctx
+        N = self.A.N
+        if self.algorithm == "cg":
+            cg = CG(self.A, self.train_y, ctx).solveHeterogeneous()
+            alpha = cg.x.to(f"cuda:{ctx.device}")
+        elif self.algorithm == "cholesky":
+            chol = Cholesky(self.A, ctx).solve_heterogeneous()
+            TriangularSystemSolver(self.A, chol.A_gpu, self.train_y, ctx).solve()
+            alpha = _to_device(self.train_y.rightHandSideData, ctx)
+        else:
+            raise RuntimeError(f"Invalid algorithm: {self.algorithm}")
+        X = self._inputs(self.path_train, N)
+        Xt = self._inputs(self.path_test, self.N_test)
+        ctx.set_problem(N, self.A.blockSize)
+        if self.fused:
+            mean = gp_predict(ctx, X, Xt, alpha[:N].contiguous(), self.lengthscale, self.signal_variance)
+        else:
+            Ks = MatrixGenerator.generateTestKernelMatrix(ctx, X, Xt, self.lengthscale, self.signal_variance)
+            mean = torch.empty(Xt.shape[0], dtype=torch.float64, device=f"cuda:{ctx.device}")
+            MatrixVectorOperations.matrixVectorGP(ctx, Ks, alpha[:N].contiguous(), mean, N, Xt.shape[0])
+        self.result = mean.cpu().numpy()
+        return self.result
+
+
+class UtilityFunctions:
+    """src/utility/UtilityFunctions.hpp: output helpers."""
+
+    @staticmethod
+    def writeResult(path, x):
+        """UtilityFunctions.cpp:19-33: `x_result.txt` in `path`, every value with
+        20 fixed decimals followed by a space, then a newline."""
+        vals = x.detach().cpu().numpy() if isinstance(x, torch.Tensor) else np.asarray(x, dtype=np.float64)
+        out = Path(path) / "x_result.txt"
+        out.write_text("".join(f"{v:.20f} " for v in vals) + "\n")
+        return out
 
 
 class MatrixParser:

@@ -5,7 +5,8 @@
 //
 // No reference counterpart (new form).  Residuals r = b - K x use the FP64
 // packed K and the FP64 matvec; the triangular solves apply the FP32 factor
-// with FP64 arithmetic (FP64 diagonal blocks, FP32 off-diagonal blocks).
+// with FP64 arithmetic (FP32 off-diagonal blocks, FP64 inverses of the
+// diagonal blocks), one fused launch per block column and direction.
 #include <chrono>
 #include <cmath>
 #include <string>
@@ -124,33 +125,17 @@ int grid_n(int64_t n, int sms) {
 
 }  // namespace
 
-// b <- (L L^T)^-1 b with the mixed factor: FP64 diagonal blocks, FP32 off-diagonal blocks
+// b <- (L L^T)^-1 b with the mixed factor: FP32 off-diagonal blocks, FP64
+// inverse diagonal blocks; one launch per block column and direction
 hs_status mixed_apply(hs_ctx ctx, const MixedWork& w, double* b, cudaStream_t s) {
     const int nb = ctx->nb;
-    const int64_t T = total_blocks(nb);
-    for (int j = 0; j < nb; ++j) {
-        const int right = nb - j;
-        const int blockID = (int)(T - (int64_t)right * (right + 1) / 2);
-        hs_status st = launch_trsv(ctx, w.Ld, b, j, j, 0, s);
-        if (st != HS_OK) return st;
-        if (j < nb - 1) {
-            st = launch_column_update_f32(ctx, w.A32, b, j + 1, nb - (j + 1), j, blockID, 0, s);
-            if (st != HS_OK) return st;
-        }
-    }
-    for (int j = nb - 1; j >= 0; --j) {
-        const int right = nb - j;
-        const int blockID = (int)(T - (int64_t)right * (right + 1) / 2);
-        hs_status st = launch_trsv(ctx, w.Ld, b, j, j, 1, s);
-        if (st != HS_OK) return st;
-        if (j > 0) {
-            st = launch_column_update_f32(ctx, w.A32, b, 0, j, j, blockID, 1, s);
-            if (st != HS_OK) return st;
-        }
-    }
+    hs_status st;
+    for (int j = -1; j < nb - 1; ++j)
+        if ((st = launch_mixed_sweep(ctx, w.A32, w.Yinv, b, j, 1, s)) != HS_OK) return st;
+    for (int j = nb; j >= 1; --j)
+        if ((st = launch_mixed_sweep(ctx, w.A32, w.Yinv, b, j, 0, s)) != HS_OK) return st;
     return HS_OK;
 }
-
 
 namespace {
 struct Events {

@@ -13,8 +13,8 @@ struct MixedWork {
     float* A32 = nullptr;   // packed FP32 copy of K, overwritten by L (off-diagonal blocks used by the solves)
     float* LO = nullptr;    // low parts: panel blocks 0..nb-1, slots nb / nb+1 = L_kk^-1 hi / lo
     double* Ld = nullptr;   // FP64 diagonal blocks of L (nb blocks)
+    double* Yinv = nullptr; // FP64 inverse diagonal blocks, Y_k = L_kk^-T (nb blocks)
     double* S = nullptr;    // FP64 scratch block (POTRF)
-    double* Y = nullptr;    // FP64 scratch block (L_kk^-T)
     int* err = nullptr;     // tensor-core tile timeout flag
     CUtensorMap mA128, mAB, mL128, mLB;
 };
@@ -30,6 +30,9 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
 // TRSM of `items` bsz x bsz FP64 blocks stored contiguously at B against the
 // lower triangle L (bsz x bsz): B <- B L^-T
 hs_status launch_trsm_on(hs_ctx ctx, const double* L, int n, double* B, int items, cudaStream_t s);
+// one launch of a forward / backward sweep with the mixed factor (k_vector.cu)
+hs_status launch_mixed_sweep(hs_ctx ctx, const float* A32, const double* Y, double* b, int j, int forward,
+                             cudaStream_t s);
 // column update reading FP32 blocks (accumulation in FP64)
 hs_status launch_column_update_f32(hs_ctx ctx, const float* A32, double* b, int blockStart, int blockCount,
                                    int blockRow, int blockID, int transposed, cudaStream_t s);

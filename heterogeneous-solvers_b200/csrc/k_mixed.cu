@@ -210,6 +210,209 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (warp == 0) tmem_dealloc(taddr, BSZ);
 }
 
+// ------------------------------------------------------------------ persistent trailing update
+// The trailing update of block column k as one persistent launch: one CTA per
+// SM walks the 128 x BSZ output tiles in a grouped order (vertical strips of
+// kGroup block rows, column by column), so that the CTAs running at the same
+// time share panel blocks through L2.  Warp roles:
+//   warp 0 (one thread)  TMA producer: A_hi/A_lo/B_hi/B_lo slabs into a 2-stage
+//                        ring, plus an L2 prefetch of the tile's C rows
+//   warp 1 (one thread)  MMA issuer: 3 x 4 tcgen05.mma per slab into one of two
+//                        TMEM accumulators (2 x BSZ columns), so that the
+//                        epilogue of tile i overlaps the MMAs of tile i+1
+//   warps 2-5            epilogue: TMEM -> registers, C -= D, then free the
+//                        accumulator (one arrival per warp)
+constexpr int kGroup = 8;
+constexpr int kUpdThreads = 192;
+constexpr uint64_t kStepWaitNs = 2000000000ull;
+
+__host__ __device__ __forceinline__ int64_t tri64(int64_t n) { return n * (n + 1) / 2; }
+
+// pair p of the grouped enumeration of the m x m lower triangle -> (r', c')
+__device__ __forceinline__ void grouped_pair(int64_t p, int m, int* rr, int* cc) {
+    int lo = 0, hi = (m + kGroup - 1) / kGroup;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tri64((int64_t)mid * kGroup) <= p) lo = mid; else hi = mid - 1;
+    }
+    const int r0 = lo * kGroup;
+    const int r1 = min(r0 + kGroup, m), h = r1 - r0;
+    int64_t l = p - tri64(r0);
+    if (l < (int64_t)r0 * h) {
+        *rr = r0 + (int)(l % h);
+        *cc = (int)(l / h);
+        return;
+    }
+    l -= (int64_t)r0 * h;
+    int j = 0;
+    while (l >= h - j) {
+        l -= h - j;
+        ++j;
+    }
+    *rr = r0 + j + (int)l;
+    *cc = r0 + j;
+}
+
+template <int BSZ>
+__global__ void __launch_bounds__(kUpdThreads, 1)
+    tc_update_kernel(const __grid_constant__ CUtensorMap mA128, const __grid_constant__ CUtensorMap mAB,
+                     const __grid_constant__ CUtensorMap mL128, const __grid_constant__ CUtensorMap mLB, TcArgs a) {
+    using SM = TcSmem<BSZ>;
+    constexpr int kTiles = SM::kTiles;
+    constexpr int kSlabs = BSZ / kSlab;
+    constexpr uint32_t kAccCols = 2 * BSZ;  // two accumulators
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + SM::kStages * SM::kStage);
+    uint64_t* empty = full + SM::kStages;
+    uint64_t* tfull = empty + SM::kStages;
+    uint64_t* tempty = tfull + 2;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(tempty + 2);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m = a.nb - a.k - 1;
+    const int64_t ntiles = tri64(m) * kTiles;
+    const size_t bb = (size_t)BSZ * BSZ;
+
+    if (tid == 0) {
+        for (int s = 0; s < SM::kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 4);
+        }
+        fence_barrier_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(tslot, kAccCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t taddr = *tslot;
+    bool ok = true;
+
+    auto decode = [&](int64_t t, int* r, int* c, int* ti) {
+        int rr, cc;
+        grouped_pair(t / kTiles, m, &rr, &cc);
+        *ti = (int)(t % kTiles);
+        *r = a.k + 1 + rr;
+        *c = a.k + 1 + cc;
+    };
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- producer
+            uint32_t g = 0;
+            for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                int r, c, ti;
+                decode(t, &r, &c, &ti);
+                const int blkA = (int)(a.blockID + (r - a.k)), gA = r - a.k - 1;
+                const int blkB = (int)(a.blockID + (c - a.k)), gB = c - a.k - 1;
+                prefetch_l2(a.A32 + (size_t)block_id(r, c, a.nb) * bb + (size_t)ti * 128 * BSZ, 128 * BSZ * 4);
+                for (int kc = 0; kc < kSlabs; ++kc, ++g) {
+                    const uint32_t s = g % SM::kStages, use = g / SM::kStages;
+                    if (use > 0 && !mbar_wait_for(&empty[s], (use - 1) & 1, kStepWaitNs)) {
+                        ok = false;
+                        break;
+                    }
+                    uint8_t* st = smem + s * SM::kStage;
+                    mbar_arrive_expect_tx(&full[s], SM::kStage);
+                    tma_load_3d(st, &mA128, &full[s], kc * kSlab, ti * 128, blkA);
+                    tma_load_3d(st + SM::kABytes, &mL128, &full[s], kc * kSlab, ti * 128, gA);
+                    tma_load_3d(st + 2 * SM::kABytes, &mAB, &full[s], kc * kSlab, 0, blkB);
+                    tma_load_3d(st + 2 * SM::kABytes + SM::kBBytes, &mLB, &full[s], kc * kSlab, 0, gB);
+                }
+            }
+            if (!ok) atomicExch(a.err, 1);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issuer
+            constexpr uint32_t idesc = umma_idesc(kFmtTF32, kFmtTF32, 128, BSZ);
+            uint32_t g = 0;
+            int it = 0;
+            for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++it) {
+                const int b = it & 1, u = it >> 1;
+                if (u > 0 && !mbar_wait_for(&tempty[b], (u - 1) & 1, kStepWaitNs)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t dcol = taddr + (uint32_t)(b * BSZ);
+                for (int kc = 0; kc < kSlabs; ++kc, ++g) {
+                    const uint32_t s = g % SM::kStages, use = g / SM::kStages;
+                    if (!mbar_wait_for(&full[s], use & 1, kStepWaitNs)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t base = smem_u32(smem + s * SM::kStage);
+                    const uint32_t aHi = base, aLo = base + SM::kABytes;
+                    const uint32_t bHi = base + 2 * SM::kABytes, bLo = bHi + SM::kBBytes;
+#pragma unroll
+                    for (int ks = 0; ks < kSlab / 8; ++ks) {
+                        const uint32_t off = ks * 32;
+                        const uint64_t dAh = umma_desc_sw128(aHi + off), dAl = umma_desc_sw128(aLo + off);
+                        const uint64_t dBh = umma_desc_sw128(bHi + off), dBl = umma_desc_sw128(bLo + off);
+                        umma_tf32(dcol, dAh, dBh, idesc, (kc | ks) != 0);
+                        umma_tf32(dcol, dAh, dBl, idesc, 1);
+                        umma_tf32(dcol, dAl, dBh, idesc, 1);
+                    }
+                    umma_commit(&empty[s]);
+                }
+                if (!ok) break;
+                umma_commit(&tfull[b]);
+            }
+            if (!ok) atomicExch(a.err, 1);
+        }
+    } else {
+        // ---- epilogue warps 2..5: lane quarter q = warp % 4 holds tile rows 32q..32q+31
+        const int q = warp & 3;
+        const int row = q * 32 + lane;
+        int it = 0;
+        for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+            const int b = it & 1, u = it >> 1;
+            int wok = 0;
+            if (lane == 0) wok = mbar_wait_for(&tfull[b], u & 1, kStepWaitNs) ? 1 : 0;
+            wok = __shfl_sync(0xffffffffu, wok, 0);
+            if (!wok) {
+                if (lane == 0) atomicExch(a.err, 1);
+                break;
+            }
+            tc_fence_after();
+            int r, c, ti;
+            decode(t, &r, &c, &ti);
+            float* outp = a.A32 + (size_t)block_id(r, c, a.nb) * bb + (size_t)(ti * 128 + row) * BSZ;
+#pragma unroll 1
+            for (int j = 0; j < BSZ / 32; ++j) {
+                uint32_t v[32];
+                tmem_ld_32x32b_x32(taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BSZ + j * 32), v);
+                tmem_ld_wait();
+                float4* o4 = reinterpret_cast<float4*>(outp + j * 32);
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    float4 cv = o4[e];
+                    cv.x -= __uint_as_float(v[4 * e + 0]);
+                    cv.y -= __uint_as_float(v[4 * e + 1]);
+                    cv.z -= __uint_as_float(v[4 * e + 2]);
+                    cv.w -= __uint_as_float(v[4 * e + 3]);
+                    o4[e] = cv;
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[b]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(taddr, kAccCols);
+}
+
 // ------------------------------------------------------------------ helpers
 __global__ void f64_to_f32_kernel(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
     const int64_t n2 = n / 2;
@@ -229,12 +432,14 @@ __global__ void lo_part_kernel(const float* __restrict__ a, float* __restrict__ 
     }
 }
 
-// S (FP64, bsz x bsz) = A32 diagonal block; T (FP64) = identity
+// S (FP64, bsz x bsz) = A32 diagonal block with a unit diagonal on the padding
+// rows >= valid (the padded factor is diag(L, I)); I (FP64) = identity
 __global__ void diag_in_kernel(const float* __restrict__ blk, double* __restrict__ S, double* __restrict__ I,
-                               int bsz) {
+                               int bsz, int valid) {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < bsz * bsz; e += gridDim.x * blockDim.x) {
-        S[e] = (double)blk[e];
-        I[e] = (e / bsz == e % bsz) ? 1.0 : 0.0;
+        const bool d = (e / bsz == e % bsz);
+        S[e] = (d && e / bsz >= valid) ? 1.0 : (double)blk[e];
+        I[e] = d ? 1.0 : 0.0;
     }
 }
 
@@ -305,6 +510,19 @@ hs_status tc_launch(hs_ctx ctx, int mode, const MixedWork& w, TcArgs a, int64_t 
     return HS_OK;
 }
 
+template <int BSZ>
+hs_status tc_update_launch(hs_ctx ctx, const MixedWork& w, const TcArgs& a, cudaStream_t s) {
+    using SM = TcSmem<BSZ>;
+    const int m = a.nb - a.k - 1;
+    const int64_t ntiles = tri64(m) * SM::kTiles;
+    if (ntiles <= 0) return HS_OK;
+    const int grid = (int)(ntiles < ctx->num_sms ? ntiles : ctx->num_sms);
+    ctx->launches += 1;
+    tc_update_kernel<BSZ><<<grid, kUpdThreads, SM::kBytes, s>>>(w.mA128, w.mAB, w.mL128, w.mLB, a);
+    HS_CHECK_LAUNCH("tc_update_kernel");
+    return HS_OK;
+}
+
 bool g_tc_attr[64][2] = {};
 
 template <int BSZ>
@@ -316,6 +534,8 @@ hs_status tc_attrs() {
     HS_CUDA(cudaFuncSetAttribute(tc_tile_kernel<BSZ, MODE_TRSM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  TcSmem<BSZ>::kBytes));
     HS_CUDA(cudaFuncSetAttribute(tc_tile_kernel<BSZ, MODE_UPDATE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TcSmem<BSZ>::kBytes));
+    HS_CUDA(cudaFuncSetAttribute(tc_update_kernel<BSZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  TcSmem<BSZ>::kBytes));
     if (dev < 64) g_tc_attr[dev][slot] = true;
     return HS_OK;
@@ -337,7 +557,8 @@ size_t mixed_workspace_bytes(int64_t N, int bsz) {
     bytes += T * bb * 4;                 // A32 / L32
     bytes += (size_t)(nb + 2) * bb * 4;  // LO
     bytes += (size_t)nb * bb * 8;        // Ldiag64
-    bytes += 2 * bb * 8;                 // S, I/Y
+    bytes += (size_t)nb * bb * 8;        // Yinv
+    bytes += bb * 8;                     // S
     bytes += 1024;                       // flags
     return bytes;
 }
@@ -353,9 +574,9 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
     p += (size_t)(nb + 2) * bb * 4;
     w->Ld = reinterpret_cast<double*>(p);
     p += (size_t)nb * bb * 8;
+    w->Yinv = reinterpret_cast<double*>(p);
+    p += (size_t)nb * bb * 8;
     w->S = reinterpret_cast<double*>(p);
-    p += bb * 8;
-    w->Y = reinterpret_cast<double*>(p);
     p += bb * 8;
     w->err = reinterpret_cast<int*>(p);
     hs_status st = make_map(&w->mA128, w->A32, bsz, (int64_t)T, 128);
@@ -382,14 +603,16 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         const int64_t blockID = T - (int64_t)right * (right + 1) / 2;
         float* dblk = w.A32 + (size_t)blockID * bb;
         // diagonal block in FP64: POTRF, then Y = L^-T by TRSM on the identity
+        double* Yk = w.Yinv + (size_t)k * bb;
+        const int64_t valid = ctx->N - (int64_t)k * bsz;
         ctx->launches += 1;
-        diag_in_kernel<<<64, 256, 0, s>>>(dblk, w.S, w.Y, bsz);
+        diag_in_kernel<<<64, 256, 0, s>>>(dblk, w.S, Yk, bsz, valid < bsz ? (int)valid : bsz);
         st = launch_potrf(ctx, w.S, 0, k, s);  // block 0 of the scratch, guard rows of block row k
         if (st != HS_OK) return st;
-        st = launch_trsm_on(ctx, w.S, bsz, w.Y, 1, s);
+        st = launch_trsm_on(ctx, w.S, bsz, Yk, 1, s);
         if (st != HS_OK) return st;
         ctx->launches += 1;
-        diag_out_kernel<<<64, 256, 0, s>>>(w.S, w.Y, dblk, w.Ld + (size_t)k * bb, w.LO + (size_t)nb * bb,
+        diag_out_kernel<<<64, 256, 0, s>>>(w.S, Yk, dblk, w.Ld + (size_t)k * bb, w.LO + (size_t)nb * bb,
                                            w.LO + (size_t)(nb + 1) * bb, bsz);
         HS_CHECK_LAUNCH("mixed diag");
         const int m = nb - k - 1;
@@ -417,8 +640,7 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         a.syrkStart = k + 1;
         a.totalPairs = a.gemmPairs + m;
         prof_begin(ctx, s, HS_KERNEL_UPDATE);
-        st = bsz == 256 ? tc_launch<256>(ctx, MODE_UPDATE, w, a, a.totalPairs, s)
-                        : tc_launch<128>(ctx, MODE_UPDATE, w, a, a.totalPairs, s);
+        st = bsz == 256 ? tc_update_launch<256>(ctx, w, a, s) : tc_update_launch<128>(ctx, w, a, s);
         if (st != HS_OK) return st;
         const double n3 = (double)bsz * bb;
         prof_end(ctx, s, HS_KERNEL_UPDATE, (double)a.gemmPairs * 2.0 * n3 + (double)m * bsz * bsz * (bsz + 1.0),

@@ -355,6 +355,57 @@ __global__ void __launch_bounds__(kThreads) column_update_f32_kernel(const float
     for (int r = threadIdx.x; r < BSZ; r += blockDim.x) bi[r] -= out[r];
 }
 
+// One launch of a triangular sweep with the mixed-precision factor: FP32
+// off-diagonal blocks, FP64 inverse diagonal blocks Y_i = L_ii^-T.
+// forward, column j: CTA g updates b_i -= L_ij b_j for i = j+1+g; the CTA of
+// i = j+1 then owns the final b_i and applies L_ii^-1 = Y_i^T.  j = -1 applies
+// only the inverse of block 0.
+// backward, column j: CTA g updates b_g -= L_jg^T b_j for g < j; the CTA of
+// g = j-1 then applies L_gg^-T = Y_g.  j = nb applies only the inverse of block nb-1.
+template <int BSZ>
+__global__ void __launch_bounds__(kThreads) mixed_sweep_kernel(const float* __restrict__ A, const double* __restrict__ Y,
+                                                               double* __restrict__ b, int nb, int j, int forward) {
+    __shared__ double smem[8 * BSZ];
+    __shared__ double out[BSZ];
+    __shared__ double xs[BSZ];
+    const size_t bb = (size_t)BSZ * BSZ;
+    const int g = blockIdx.x;
+    int i;
+    bool diag;
+    if (forward) {
+        i = j + 1 + g;
+        diag = (g == 0);
+        if (j >= 0) {
+            BlockApply<BSZ, float>::run(A + (size_t)block_id(i, j, nb) * bb, b + (size_t)j * BSZ, nullptr, out,
+                                        nullptr, 1, smem);
+        }
+    } else {
+        i = (j == nb) ? nb - 1 : g;
+        diag = (j == nb) || (g == j - 1);
+        if (j < nb) {
+            BlockApply<BSZ, float>::run(A + (size_t)block_id(j, g, nb) * bb, nullptr, b + (size_t)j * BSZ, nullptr,
+                                        out, 2, smem);
+        }
+    }
+    double* bi = b + (size_t)i * BSZ;
+    const bool updated = forward ? (j >= 0) : (j < nb);
+    __syncthreads();
+    for (int r = threadIdx.x; r < BSZ; r += blockDim.x) {
+        const double v = updated ? bi[r] - out[r] : bi[r];
+        if (diag) xs[r] = v;
+        else bi[r] = v;
+    }
+    if (!diag) return;
+    __syncthreads();
+    const double* Yi = Y + (size_t)i * bb;
+    if (forward)  // L^-1 x = Y^T x: column part of Y
+        BlockApply<BSZ, double>::run(Yi, nullptr, xs, nullptr, out, 2, smem);
+    else          // L^-T x = Y x: row part of Y
+        BlockApply<BSZ, double>::run(Yi, xs, nullptr, out, nullptr, 1, smem);
+    __syncthreads();
+    for (int r = threadIdx.x; r < BSZ; r += blockDim.x) bi[r] = out[r];
+}
+
 // ------------------------------------------------------------------ TRSV
 // Blocked substitution on one diagonal block: 32-row chunks, warp 0 solves the
 // chunk's triangle (column oriented, as the reference), all warps then apply
@@ -558,6 +609,26 @@ hs_status launch_column_update(hs_ctx ctx, const double* A, double* b, int block
     HS_CHECK_LAUNCH("column_update");
     prof_end(ctx, s, HS_KERNEL_COLUPD, 2.0 * blockCount * (double)bsz * bsz,
              (double)blockCount * bsz * bsz * 8.0 + 24.0 * blockCount * bsz);
+    return HS_OK;
+}
+
+hs_status launch_mixed_sweep(hs_ctx ctx, const float* A32, const double* Y, double* b, int j, int forward,
+                             cudaStream_t s) {
+    const int bsz = ctx->bsz, nb = ctx->nb;
+    HS_REQUIRE(bsz == 128 || bsz == 256, "the mixed sweep supports matrixBlockSize 128 or 256");
+    int grid;
+    if (forward) grid = (j < 0) ? 1 : nb - j - 1;
+    else grid = (j >= nb) ? 1 : j;
+    if (grid <= 0) return HS_OK;
+    prof_begin(ctx, s, HS_KERNEL_COLUPD);
+    ctx->launches += 1;
+    if (bsz == 256)
+        mixed_sweep_kernel<256><<<grid, kThreads, 0, s>>>(A32, Y, b, nb, j, forward);
+    else
+        mixed_sweep_kernel<128><<<grid, kThreads, 0, s>>>(A32, Y, b, nb, j, forward);
+    HS_CHECK_LAUNCH("mixed_sweep");
+    prof_end(ctx, s, HS_KERNEL_COLUPD, 2.0 * (grid + 1) * (double)bsz * bsz,
+             (double)grid * bsz * bsz * 4.0 + (double)bsz * bsz * 8.0 + 24.0 * grid * bsz);
     return HS_OK;
 }
 

@@ -271,6 +271,24 @@ hs_status hs_mixed_solve(hs_ctx ctx, const double* K, const double* b, double* x
  * *logdet is a host pointer. */
 hs_status hs_cholesky_logdet(hs_ctx ctx, const double* L, double* logdet);
 
+/* ------------------------------------------------------------------ prediction
+ * MatrixGenerator::generateTestKernelMatrix (src/utility/MatrixGenerator.cpp:163-213):
+ * K_star[j*N + i] = sf2 exp(-0.5/l^2 sum_k (x_ik - x*_jk)^2) for training rows
+ * X (N x d, N of the context) and test rows X_test (N_test x d), row major,
+ * device; `ell` (host) holds 1 or d lengthscales (ARD: each difference scaled
+ * by 1/l_k).  The reference's sliding window is X[i][k] = series[i+k-7]. */
+hs_status hs_gp_test_kernel_matrix(hs_ctx ctx, const double* X, const double* X_test, int64_t N_test, int d,
+                                   const double* ell, int n_ell, double sf2, double* K_star);
+/* MatrixVectorOperations::matrixVectorGP (src/kernel/MatrixVectorOperations.hpp:113,
+ * .cpp:379-395): result[i] = sum_k A[i*n + k] b[k] for i < m (A dense m x n). */
+hs_status hs_matrix_vector_gp(hs_ctx ctx, const double* A, const double* b, double* result, int64_t n, int64_t m);
+/* The two calls above fused (GaussianProcess::start's prediction,
+ * src/gaussianProcess/GaussianProcess.cpp:42-54): mean[j] = sum_i K_star[j][i]
+ * alpha[i] with K_star recomputed on the fly and never stored.  alpha = K^-1 y
+ * (N values, device), mean (N_test, device). */
+hs_status hs_gp_predict(hs_ctx ctx, const double* X, const double* X_test, int64_t N_test, int d, const double* ell,
+                        int n_ell, double sf2, const double* alpha, double* mean);
+
 /* ------------------------------------------------------------------ differentiation
  * No reference counterpart (new form).  Reverse-mode blocked Cholesky: with L
  * the packed factor of A = L L^T (hs_cholesky_factor) and Abar holding, on

@@ -360,3 +360,35 @@ void or_window_inputs(const double* series, int64_t N, double* X) {
             X[i * 8 + k] = s < 0 ? 0.0 : series[s];
         }
 }
+
+void or_test_kernel_matrix(const double* X, int64_t N, const double* Xt, int64_t Nt, int d, const double* ell,
+                           int n_ell, double sf2, double* K_star) {
+    /* MatrixGenerator.cpp:196-211: for each (test j, train i): distance =
+     * sum_k (train_i,k - test_j,k)^2 with k ascending, then
+     * sf2 * exp(-0.5 / l^2 * distance) stored at K_star[j * N + i]; the ARD
+     * form scales each difference by 1/l_k and uses exp(-0.5 * distance). */
+    const int ard = (n_ell == d && d > 1);
+    const double iso_scale = -0.5 / (ell[0] * ell[0]);
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < Nt; ++j) {
+        for (int64_t i = 0; i < N; ++i) {
+            double dist = 0.0;
+            for (int k = 0; k < d; ++k) {
+                const double t = ard ? (X[i * d + k] - Xt[j * d + k]) * (1.0 / ell[k]) : X[i * d + k] - Xt[j * d + k];
+                dist += t * t;
+            }
+            K_star[j * N + i] = sf2 * exp((ard ? -0.5 : iso_scale) * dist);
+        }
+    }
+}
+
+void or_matrix_vector_gp(const double* A, const double* b, double* result, int64_t n, int64_t m) {
+    /* MatrixVectorOperations.cpp:384-390: result[i] = sum_k A[i*n + k] b[k],
+     * one running sum per row in k order */
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < m; ++i) {
+        double sum = 0.0;
+        for (int64_t k = 0; k < n; ++k) sum += A[i * n + k] * b[k];
+        result[i] = sum;
+    }
+}

@@ -73,6 +73,12 @@ void or_rbf_assemble(double* A, const double* X, int64_t N, int d, int bsz, cons
                      double sf2, double sn2);
 /* sliding-window inputs of the reference generator — MatrixGenerator.cpp:76-99:
  * X[i][k] = s[i+k-7] (7 leading zeros), d = 8 */
+/* MatrixGenerator::generateTestKernelMatrix (MatrixGenerator.cpp:163-213) on
+ * row-major inputs: K_star[j*N + i] */
+void or_test_kernel_matrix(const double* X, int64_t N, const double* Xt, int64_t Nt, int d, const double* ell,
+                           int n_ell, double sf2, double* K_star);
+/* MatrixVectorOperations::matrixVectorGP (MatrixVectorOperations.cpp:379-395) */
+void or_matrix_vector_gp(const double* A, const double* b, double* result, int64_t n, int64_t m);
 void or_window_inputs(const double* series, int64_t N, double* X);
 
 #ifdef __cplusplus

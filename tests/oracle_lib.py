@@ -37,6 +37,8 @@ _SIGS = {
     "or_cg": ([_P, _P, _P, _I64, _I, _D, _I64, _I, ctypes.POINTER(_D), ctypes.POINTER(_D)], _I64),
     "or_rbf_assemble": ([_P, _P, _I64, _I, _I, _P, _I, _D, _D], None),
     "or_window_inputs": ([_P, _I64, _P], None),
+    "or_test_kernel_matrix": ([_P, _I64, _P, _I64, _I, _P, _I, _D, _P], None),
+    "or_matrix_vector_gp": ([_P, _P, _P, _I64, _I64], None),
 }
 
 _lib = None
@@ -109,3 +111,28 @@ def packed_to_dense(data, N, bsz, lower_only=False):
             if i != j and not lower_only:
                 full[j * bsz:(j + 1) * bsz, i * bsz:(i + 1) * bsz] = blk.T
     return full[:N, :N]
+
+
+def test_kernel_matrix(X, Xt, ell, sf2):
+    """K_star (N_test x N, row major) of MatrixGenerator::generateTestKernelMatrix."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Xt = np.ascontiguousarray(Xt, dtype=np.float64)
+    ell = np.atleast_1d(np.asarray(ell, dtype=np.float64))
+    K = np.zeros((Xt.shape[0], X.shape[0]))
+    lib().or_test_kernel_matrix(ptr(X), X.shape[0], ptr(Xt), Xt.shape[0], X.shape[1], ptr(ell), ell.size, sf2, ptr(K))
+    return K
+
+
+def matrix_vector_gp(A, b, n, m):
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    out = np.zeros(m)
+    lib().or_matrix_vector_gp(ptr(A), ptr(b), ptr(out), n, m)
+    return out
+
+
+def window_inputs(series, N):
+    s = np.ascontiguousarray(series, dtype=np.float64)
+    X = np.zeros((N, 8))
+    lib().or_window_inputs(ptr(s), N, ptr(X))
+    return X

@@ -136,3 +136,16 @@ def test_nlml_rejects_bad_arguments(hs, ctx):
     ctx.set_problem(256, 64)
     with pytest.raises(hs.HSError):
         hs.gp_nlml_grad(ctx, X, y, np.zeros(3), n_ell=1)  # block size 64 unsupported
+
+
+def test_fit_hyperparameters_decreases_nlml(hs, ctx):
+    """A few L-BFGS steps on the analytic gradient lower the NLML; the result
+    agrees with the dense NLML at the returned theta."""
+    N, bsz, d = 1024, 128, 3
+    X, y, theta_true = _c4_problem(N, d, seed=17)
+    theta0 = np.concatenate([np.zeros(d), [0.5, np.log(1e-2)]])
+    ctx.set_problem(N, bsz)
+    out = hs.fit_hyperparameters(ctx, X, y, theta0, maxiter=8)
+    nlml0 = g.nlml_value(X, y, theta0, d)
+    assert out["nlml"] < nlml0 - 1.0
+    assert abs(out["nlml"] - g.nlml_value(X, y, out["theta"], d)) <= 1e-9 * abs(out["nlml"])

@@ -1,0 +1,83 @@
+"""GPU suite: GP prediction (MatrixGenerator::generateTestKernelMatrix,
+MatrixVectorOperations::matrixVectorGP, GaussianProcess::start) against the
+oracle's restatement of the reference's CPU code, and the fused predictive
+mean against the two-step form."""
+import numpy as np
+import pytest
+import torch
+
+import oracle_lib as ol
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("N,Nt,d,ell", [(1000, 300, 8, 1.0), (777, 129, 3, 0.6), (512, 1, 8, [0.3, 0.5, 0.8, 1.0,
+                                                                                             1.2, 1.5, 2.0, 0.9])])
+def test_test_kernel_matrix_matches_oracle(hs, ctx, N, Nt, d, ell):
+    rng = np.random.default_rng(N)
+    X, Xt = rng.random((N, d)), rng.random((Nt, d))
+    ctx.set_problem(N, 128)
+    K = hs.MatrixGenerator.generateTestKernelMatrix(ctx, X, Xt, ell, 1.3).cpu().numpy()
+    ref = ol.test_kernel_matrix(X, Xt, ell, 1.3)
+    assert K.shape == (Nt, N)
+    assert np.max(np.abs(K - ref)) <= 1e-14
+
+
+@pytest.mark.parametrize("n,m", [(1000, 300), (33, 7), (4096, 64), (1, 5)])
+def test_matrix_vector_gp_matches_oracle(hs, ctx, n, m):
+    rng = np.random.default_rng(n + m)
+    A, b = rng.standard_normal((m, n)), rng.standard_normal(n)
+    ctx.set_problem(max(n, 1), 128)
+    out = torch.empty(m, dtype=torch.float64, device="cuda:0")
+    hs.MatrixVectorOperations.matrixVectorGP(ctx, torch.from_numpy(A).cuda(), torch.from_numpy(b).cuda(), out, n, m)
+    ref = ol.matrix_vector_gp(A, b, n, m)
+    assert np.max(np.abs(out.cpu().numpy() - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref)))
+
+
+def test_fused_predict_matches_two_step(hs, ctx):
+    rng = np.random.default_rng(3)
+    N, Nt, d = 3000, 517, 8
+    X, Xt, alpha = rng.random((N, d)), rng.random((Nt, d)), rng.standard_normal(N)
+    ctx.set_problem(N, 256)
+    mean = hs.gp_predict(ctx, X, Xt, alpha, 0.7, 1.0).cpu().numpy()
+    ref = ol.matrix_vector_gp(ol.test_kernel_matrix(X, Xt, 0.7, 1.0), alpha, N, Nt)
+    assert np.max(np.abs(mean - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("algorithm", ["cholesky", "cg"])
+def test_gaussian_process_pipeline_matches_oracle(hs, ctx, tmp_path, algorithm):
+    """GaussianProcess::start from the reference's text inputs: training series,
+    targets, test series (one value per line), 8-sample windows, l = 1, sf2 = 1,
+    sn2 = 0.01 (MatrixGenerator.cpp:126-130)."""
+    rng = np.random.default_rng(11)
+    N, Nt, bsz = 600, 90, 128
+    train = np.sin(np.linspace(0, 12, N)) + 0.05 * rng.standard_normal(N)
+    target = np.roll(train, -1)
+    test = np.sin(np.linspace(12, 14, Nt))
+    for name, v in (("train.txt", train), ("y.txt", target), ("test.txt", test)):
+        (tmp_path / name).write_text("\n".join(f"{x:.17g}" for x in v) + "\n")
+    A = hs.MatrixGenerator.generateSPDMatrix(ctx, tmp_path / "train.txt", N, bsz)
+    b = hs.RightHandSide(N, bsz)
+    b.rightHandSideData[:N] = torch.from_numpy(np.loadtxt(tmp_path / "y.txt"))
+    gp = hs.GaussianProcess(A, b, tmp_path / "train.txt", tmp_path / "test.txt", ctx, algorithm=algorithm)
+    if algorithm == "cg":
+        ctx.set_reference_order(8)  # the oracle's CG iterates exactly (8 CPU chunks)
+    try:
+        mean = gp.start()
+    finally:
+        ctx.set_reference_order(0)
+    # oracle: the reference's CPU path end to end
+    X = ol.window_inputs(train, N)
+    Xt = ol.window_inputs(test, Nt)
+    K = ol.rbf_assemble(X, bsz, 1.0, 1.0, 1e-2)
+    yb = np.zeros(hs.padded_size(N, bsz))
+    yb[:N] = target
+    if algorithm == "cholesky":
+        alpha = ol.triangular_solve(ol.cholesky(K, N, bsz), yb, N, bsz)
+    else:
+        alpha, _, _, _ = ol.cg(K, yb, N, bsz, 1e-6, 100000, chunks=8)
+    ref = ol.matrix_vector_gp(ol.test_kernel_matrix(X, Xt, 1.0, 1.0), alpha[:N], N, Nt)
+    assert np.max(np.abs(mean - ref)) <= 1e-10 * np.max(np.abs(ref))
+    out = hs.UtilityFunctions.writeResult(tmp_path, mean)
+    vals = [float(v) for v in out.read_text().split()]
+    np.testing.assert_allclose(vals, mean, rtol=1e-15)

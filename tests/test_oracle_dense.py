@@ -67,3 +67,16 @@ def test_cg_matches_lapack():
     x, it, dn, d0 = ol.cg(A, b, N, bsz, 1e-10, 10000)
     assert dn <= 1e-20 * d0 and it > 0
     assert np.allclose(x[:N], np.linalg.solve(K, y), rtol=1e-7, atol=1e-8)
+
+
+def test_oracle_test_kernel_matrix_is_the_rbf_formula():
+    """The restatement of generateTestKernelMatrix against the closed form."""
+    rng = np.random.default_rng(0)
+    X, Xt = rng.random((40, 8)), rng.random((13, 8))
+    for ell in (1.0, np.linspace(0.3, 2.0, 8)):
+        K = ol.test_kernel_matrix(X, Xt, ell, 1.7)
+        e = np.broadcast_to(np.atleast_1d(ell), (8,))
+        D = ((Xt[:, None, :] - X[None, :, :]) / e) ** 2
+        np.testing.assert_allclose(K, 1.7 * np.exp(-0.5 * D.sum(-1)), rtol=1e-14)
+    A, b = rng.standard_normal((5, 40)), rng.standard_normal(40)
+    np.testing.assert_allclose(ol.matrix_vector_gp(A, b, 40, 5), A @ b, rtol=1e-13)
