@@ -41,12 +41,14 @@ __global__ void __launch_bounds__(512) potrf_smem_kernel(double* __restrict__ Ab
         for (int i = k + 1 + (int)threadIdx.x; i < valid; i += blockDim.x) S[i * sld + k] = S[i * sld + k] / s;
         __syncthreads();
         if (threadIdx.x == 0) S[k * sld + k] = s;
-        // lower trailing part: j in (k, n), i in [j, valid)
-        const int m = n - k - 1;
-        for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-            const int j = k + 1 + e / m;
-            const int i = k + 1 + e % m;
-            if (i >= j && i < valid) S[i * sld + j] = S[i * sld + j] - S[i * sld + k] * S[j * sld + k];
+        // lower trailing part: j in (k, n), i in [j, valid); one warp per column,
+        // lanes over rows (no index divisions, no idle lanes above the diagonal)
+        {
+            const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+            for (int j = k + 1 + warp; j < valid; j += nw) {
+                const double sjk = S[j * sld + k];
+                for (int i = j + lane; i < valid; i += 32) S[i * sld + j] = S[i * sld + j] - S[i * sld + k] * sjk;
+            }
         }
         __syncthreads();
     }
