@@ -66,6 +66,8 @@ def parse_args():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
     ap.add_argument("--tol", type=float, default=1e-14, help="backward-error target of the mixed solve")
     ap.add_argument("--lml-n", type=int, default=16384, help="N of the NLML+gradient leg (0: skip)")
+    ap.add_argument("--sweep", action="store_true",
+                    help="conditioning sweep: mixed vs FP64 solve for sn2 in {1e-1, 1e-3, 1e-6} (one JSON line)")
     ap.add_argument("--lml-steps", type=int, default=3)
     return ap.parse_args()
 
@@ -239,6 +241,74 @@ def bench_lml(hs, torch, device, N, steps):
             "useful_tflops_whole": (N ** 3 / 3 + 2 * N ** 3 / 3) / (t_ms * 1e-3) / 1e12}
 
 
+def run_sweep(args, hs, torch, ctx, Xd, bd, A, N, cfg, device):
+    """Mixed (3xTF32 factor + FP64 refinement / PCG) against FP64 factor + solve on the
+    same RBF system for sn2 in {1e-1, 1e-3, 1e-6}: times, backward errors, refinement
+    steps and PCG iterations, and the mixed results' error against the FP64 ones."""
+    import ctypes
+    lib = hs._lib.load()
+    nb, bsz = ctx.blockCountXY, cfg["bsz"]
+
+    def P(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def k_fro():
+        blocks = A.view(-1, bsz * bsz)
+        diag_ids = torch.tensor([hs.block_id(k, k, nb) for k in range(nb)], device=A.device)
+        sq = (blocks * blocks).sum(dim=1)
+        return float(torch.sqrt(2.0 * sq.sum() - sq[diag_ids].sum()).item())
+
+    out = []
+    for sn2 in (1e-1, 1e-3, 1e-6):
+        def assemble():
+            hs.MatrixGenerator.assemble(ctx, A, Xd, cfg["lengthscale"], cfg["sf2"], sn2)
+
+        def bwd(x):
+            assemble()
+            r = torch.empty_like(bd)
+            hs.MatrixVectorOperations.matrixVectorBlock(ctx, A, x, r, 0, 0, nb, nb, nb)
+            return torch.linalg.norm(r - bd).item() / (k_fro() * torch.linalg.norm(x).item())
+
+        row = {"sn2": sn2}
+        xm = torch.empty_like(bd)
+        rep = hs._lib.MixedReport()
+        assemble()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = lib.hs_mixed_solve(ctx.handle, P(A), P(bd), P(xm), hs.PRECISIONS["tf32x3"], args.tol, 30,
+                                ctypes.byref(rep))
+        e1.record()
+        torch.cuda.synchronize()
+        row["mixed"] = {f: getattr(rep, f) for f, _ in hs._lib.MixedReport._fields_}
+        row["mixed"]["status"] = hs._lib.STATUS_NAMES.get(int(st), int(st))
+        row["mixed"]["ms"] = e0.elapsed_time(e1)
+        row["mixed"]["backward_error_host_check"] = bwd(xm) if st == 0 else None
+        x64 = torch.empty_like(bd)
+        info = ctypes.c_int64()
+        assemble()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        st64 = lib.hs_cholesky_factor(ctx.handle, P(A), ctypes.byref(info))
+        x64.copy_(bd)
+        if st64 == 0:
+            lib.hs_cholesky_solve(ctx.handle, P(A), P(x64))
+        f1.record()
+        torch.cuda.synchronize()
+        row["fp64"] = {"status": hs._lib.STATUS_NAMES.get(int(st64), int(st64)), "ms": f0.elapsed_time(f1)}
+        if st64 == 0:
+            ld64 = hs.cholesky_logdet(ctx, A)
+            row["fp64"]["logdet"] = ld64
+            row["fp64"]["backward_error"] = bwd(x64)
+            if st == 0:
+                row["mixed_x_rel_err_vs_fp64"] = float((torch.linalg.norm(xm - x64) / torch.linalg.norm(x64)).item())
+                row["mixed_logdet_rel_err_vs_fp64"] = abs(rep.logdet - ld64) / abs(ld64)
+                row["speedup_mixed_vs_fp64"] = row["fp64"]["ms"] / row["mixed"]["ms"]
+        out.append(row)
+    return out
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -315,6 +385,13 @@ def main():
     for _ in range(args.warmup):
         step_mixed()
     torch.cuda.synchronize()
+    if args.sweep:
+        rows = run_sweep(args, hs, torch, ctx, Xd, bd, A, N, cfg, device)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "mode": "conditioning sweep", "n_gpus": world,
+                              "config": dict(bench_config(N, world), sn2="sweep"), "sweep": rows}), flush=True)
+        ctx.close()
+        return
     tf32_peak = measure_gemm_peak(torch, device, torch.float32, tf32=True)
 
     # ---------------- timed region: mixed-precision solve (device-resident inputs)
@@ -346,7 +423,7 @@ def main():
         dist.barrier()
     ms_per_step = t_max_ms / args.steps
     value = world * args.steps / (t_max_ms * 1e-3)
-    mixed_report = {f: getattr(mrep, f) for f, _ in hs._lib.MixedReport._fields_ if f != "reserved"}
+    mixed_report = {f: getattr(mrep, f) for f, _ in hs._lib.MixedReport._fields_}
     x_mixed = xd.clone()
     bwd_mixed = backward_error(x_mixed)
 

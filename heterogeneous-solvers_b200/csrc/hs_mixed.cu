@@ -111,6 +111,24 @@ __global__ void logdiag_kernel(const double* __restrict__ L, int bsz, int nb, in
     if (threadIdx.x == 0) *out = 2.0 * s;
 }
 
+// largest diagonal entry over the valid rows of the packed matrix
+__global__ void maxdiag_kernel(const double* __restrict__ A, int bsz, int nb, int64_t N, double* __restrict__ out) {
+    __shared__ double sh[32];
+    double m = 0.0;
+    const int64_t bb = (int64_t)bsz * bsz;
+    for (int64_t i = threadIdx.x; i < N; i += blockDim.x) {
+        const int k = (int)(i / bsz), r = (int)(i % bsz);
+        m = fmax(m, A[block_id(k, k, nb) * bb + (int64_t)r * bsz + r]);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, sh[w]);
+        *out = m;
+    }
+}
+
 // x += d
 __global__ void add_kernel(double* __restrict__ x, const double* __restrict__ d, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -196,24 +214,39 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
         HS_CUDA(cudaStreamSynchronize(s));
         R.norm_k_fro = std::sqrt(h[8]);
     }
-    // factor (a non-positive FP64 pivot of the FP32 matrix is recorded in ctx->d_info)
+    // factor (a non-positive FP64 pivot of the FP32 matrix is recorded in ctx->d_info);
+    // on breakdown, factor K + shift*I with a growing shift and use it as a CG preconditioner
+    double shift = 0.0;
     HS_CUDA(cudaEventRecord(ev.e[0], s));
-    ctx->launches += 1;
-    set_i64_dev(ctx->d_info, INT64_MAX, s);
-    st = mixed_factor(ctx, K, w, s);
-    if (st != HS_OK) return st;
-    HS_CUDA(cudaEventRecord(ev.e[1], s));
-    HS_CUDA(cudaStreamSynchronize(s));
-    st = mixed_check_error(ctx, w);
-    if (st != HS_OK) return st;
-    int64_t info = -1;
-    st = hs_ctx_take_info(ctx, &info);
-    if (st != HS_OK) return st;
-    if (info >= 0) {
-        set_error("hs_mixed_solve: the FP32 factor met a non-positive pivot at row " + std::to_string(info) +
-                  " (matrix too ill-conditioned for the low-precision factor)");
-        return HS_ERR_NOT_SPD;
+    for (int attempt = 1;; ++attempt) {
+        ctx->launches += 1;
+        set_i64_dev(ctx->d_info, INT64_MAX, s);
+        st = mixed_factor(ctx, K, w, s, shift);
+        if (st != HS_OK) return st;
+        HS_CUDA(cudaStreamSynchronize(s));
+        st = mixed_check_error(ctx, w);
+        if (st != HS_OK) return st;
+        int64_t info = -1;
+        st = hs_ctx_take_info(ctx, &info);
+        if (st != HS_OK) return st;
+        R.factor_attempts = attempt;
+        R.shift = shift;
+        if (info < 0) break;
+        if (attempt == 5) {
+            set_error("hs_mixed_solve: the FP32 factor met a non-positive pivot at row " + std::to_string(info) +
+                      " even with a diagonal shift of " + std::to_string(shift));
+            return HS_ERR_NOT_SPD;
+        }
+        if (attempt == 1) {
+            ctx->launches += 1;
+            maxdiag_kernel<<<1, 1024, 0, s>>>(K, bsz, nb, ctx->N, scal + 3);
+            HS_CHECK_LAUNCH("maxdiag");
+            HS_CUDA(cudaMemcpyAsync((void*)(h + 9), scal + 3, sizeof(double), cudaMemcpyDeviceToHost, s));
+            HS_CUDA(cudaStreamSynchronize(s));
+        }
+        shift = h[9] * std::pow(10.0, -7 + attempt);  // 1e-6, 1e-5, 1e-4, 1e-3 x max diag
     }
+    HS_CUDA(cudaEventRecord(ev.e[1], s));
     // log|K| from the FP64 diagonal blocks
     ctx->launches += 1;
     logdiag_kernel<<<1, 1024, 0, s>>>(w.Ld, bsz, nb, ctx->N, 1, scal + 2);
@@ -241,7 +274,9 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     int stalls = 0;
     bool converged = false;
     int steps = 0;
-    for (; steps < max_steps; ++steps) {
+    // a shifted factor is only a preconditioner: no refinement, straight to CG
+    const int ref_steps = shift > 0.0 ? 0 : max_steps;
+    for (; steps < ref_steps; ++steps) {
         st = residual(&rn, &xn);
         if (st != HS_OK) return st;
         R.backward_error = rn / (R.norm_k_fro * xn);
@@ -270,6 +305,7 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
         R.fallback_pcg = 1;
         st = residual(&rn, &xn);  // r = b - K x
         if (st != HS_OK) return st;
+        if (steps == 0) R.initial_backward_error = rn / (R.norm_k_fro * xn);
         HS_CUDA(cudaMemcpyAsync(z, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         st = mixed_apply(ctx, w, z, s);
         if (st != HS_OK) return st;

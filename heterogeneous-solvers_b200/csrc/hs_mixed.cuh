@@ -16,12 +16,14 @@ struct MixedWork {
     double* Yinv = nullptr; // FP64 inverse diagonal blocks, Y_k = L_kk^-T (nb blocks)
     double* S = nullptr;    // FP64 scratch block (POTRF)
     int* err = nullptr;     // tensor-core tile timeout flag
-    CUtensorMap mA128, mAB, mL128, mLB;
+    CUtensorMap mA128, mAB, mL128, mLB;  // 128-byte swizzle, 32-wide K boxes (TRSM)
+    CUtensorMap mU128, mUB, mV128, mVB;  // 64-byte swizzle, 16-wide K boxes over A32 / LO (update)
 };
 
 size_t mixed_workspace_bytes(int64_t N, int bsz);
 hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w);
-hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s);
+// shift != 0: factor K + shift*I
+hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift = 0.0);
 hs_status mixed_check_error(hs_ctx ctx, const MixedWork& w);
 // the mixed-precision solve behind hs_mixed_solve (workspace kept by the context)
 hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,

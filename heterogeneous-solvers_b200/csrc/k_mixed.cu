@@ -215,16 +215,40 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // SM walks the 128 x BSZ output tiles in a grouped order (vertical strips of
 // kGroup block rows, column by column), so that the CTAs running at the same
 // time share panel blocks through L2.  Warp roles:
-//   warp 0 (one thread)  TMA producer: A_hi/A_lo/B_hi/B_lo slabs into a 2-stage
-//                        ring, plus an L2 prefetch of the tile's C rows
-//   warp 1 (one thread)  MMA issuer: 3 x 4 tcgen05.mma per slab into one of two
-//                        TMEM accumulators (2 x BSZ columns), so that the
-//                        epilogue of tile i overlaps the MMAs of tile i+1
+//   warp 0 (one thread)  TMA producer: A_hi/A_lo/B_hi/B_lo slabs of kUpdK
+//                        K-columns into a ring of stages, plus an L2 prefetch of
+//                        the tile's C rows
+//   warp 1 (one thread)  MMA issuer: kUpdK/8 x 3 tcgen05.mma per slab (hi*hi, hi*lo,
+//                        lo*hi) into one of two TMEM accumulators (2 x BSZ
+//                        columns), so that the epilogue of tile i overlaps the
+//                        MMAs of tile i+1
 //   warps 2-5            epilogue: TMEM -> registers, C -= D, then free the
 //                        accumulator (one arrival per warp)
+// (Forming the low parts in shared memory instead of loading them halves the
+// L2 traffic but adds shared-memory traffic on the port the tensor core reads
+// its operands through; measured slower.)
 constexpr int kGroup = 8;
 constexpr int kUpdThreads = 192;
+// K floats per stage: 32 (128-byte rows, 128-byte swizzle, 2 stages of 96 KB)
+// measured faster than 16 (64-byte swizzle, 4 stages of 48 KB); the kernel is
+// limited by the shared-memory traffic of TMA writes plus the tensor core's
+// operand reads, not by the depth of the ring
+constexpr int kUpdK = 32;
 constexpr uint64_t kStepWaitNs = 2000000000ull;
+
+template <int BSZ>
+struct UpdSmem {
+    static constexpr int kA = 128 * kUpdK * 4;       // 8 KB
+    static constexpr int kB = BSZ * kUpdK * 4;       // 16 / 8 KB
+    static constexpr int kRaw = kA + kB;             // one of hi / lo
+    static constexpr int kStage = 2 * kRaw;          // A_hi, B_hi, A_lo, B_lo (TMA bytes per stage)
+    static constexpr int kStages = kUpdK == 32 ? 2 : 4;
+    static constexpr int kBytes = kStages * kStage + 1024 /* barriers, slot */ + 1024 /* alignment */;
+};
+
+__device__ __forceinline__ uint64_t upd_desc(uint32_t addr) {
+    return kUpdK == 32 ? umma_desc_sw128(addr) : umma_desc_sw64(addr);
+}
 
 __host__ __device__ __forceinline__ int64_t tri64(int64_t n) { return n * (n + 1) / 2; }
 
@@ -255,11 +279,11 @@ __device__ __forceinline__ void grouped_pair(int64_t p, int m, int* rr, int* cc)
 
 template <int BSZ>
 __global__ void __launch_bounds__(kUpdThreads, 1)
-    tc_update_kernel(const __grid_constant__ CUtensorMap mA128, const __grid_constant__ CUtensorMap mAB,
-                     const __grid_constant__ CUtensorMap mL128, const __grid_constant__ CUtensorMap mLB, TcArgs a) {
-    using SM = TcSmem<BSZ>;
-    constexpr int kTiles = SM::kTiles;
-    constexpr int kSlabs = BSZ / kSlab;
+    tc_update_kernel(const __grid_constant__ CUtensorMap mU128, const __grid_constant__ CUtensorMap mUB,
+                     const __grid_constant__ CUtensorMap mV128, const __grid_constant__ CUtensorMap mVB, TcArgs a) {
+    using SM = UpdSmem<BSZ>;
+    constexpr int kTiles = BSZ / 128;
+    constexpr int kSlabs = BSZ / kUpdK;
     constexpr uint32_t kAccCols = 2 * BSZ;  // two accumulators
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -321,10 +345,10 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                     }
                     uint8_t* st = smem + s * SM::kStage;
                     mbar_arrive_expect_tx(&full[s], SM::kStage);
-                    tma_load_3d(st, &mA128, &full[s], kc * kSlab, ti * 128, blkA);
-                    tma_load_3d(st + SM::kABytes, &mL128, &full[s], kc * kSlab, ti * 128, gA);
-                    tma_load_3d(st + 2 * SM::kABytes, &mAB, &full[s], kc * kSlab, 0, blkB);
-                    tma_load_3d(st + 2 * SM::kABytes + SM::kBBytes, &mLB, &full[s], kc * kSlab, 0, gB);
+                    tma_load_3d(st, &mU128, &full[s], kc * kUpdK, ti * 128, blkA);
+                    tma_load_3d(st + SM::kA, &mUB, &full[s], kc * kUpdK, 0, blkB);
+                    tma_load_3d(st + SM::kRaw, &mV128, &full[s], kc * kUpdK, ti * 128, gA);
+                    tma_load_3d(st + SM::kRaw + SM::kA, &mVB, &full[s], kc * kUpdK, 0, gB);
                 }
             }
             if (!ok) atomicExch(a.err, 1);
@@ -351,13 +375,13 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                     }
                     tc_fence_after();
                     const uint32_t base = smem_u32(smem + s * SM::kStage);
-                    const uint32_t aHi = base, aLo = base + SM::kABytes;
-                    const uint32_t bHi = base + 2 * SM::kABytes, bLo = bHi + SM::kBBytes;
+                    const uint32_t aHi = base, bHi = base + SM::kA;
+                    const uint32_t aLo = base + SM::kRaw, bLo = aLo + SM::kA;
 #pragma unroll
-                    for (int ks = 0; ks < kSlab / 8; ++ks) {
-                        const uint32_t off = ks * 32;
-                        const uint64_t dAh = umma_desc_sw128(aHi + off), dAl = umma_desc_sw128(aLo + off);
-                        const uint64_t dBh = umma_desc_sw128(bHi + off), dBl = umma_desc_sw128(bLo + off);
+                    for (int ks = 0; ks < kUpdK / 8; ++ks) {
+                        const uint32_t off = ks * 32;  // 8 TF32 = 32 bytes along K
+                        const uint64_t dAh = upd_desc(aHi + off), dAl = upd_desc(aLo + off);
+                        const uint64_t dBh = upd_desc(bHi + off), dBl = upd_desc(bLo + off);
                         umma_tf32(dcol, dAh, dBh, idesc, (kc | ks) != 0);
                         umma_tf32(dcol, dAh, dBl, idesc, 1);
                         umma_tf32(dcol, dAl, dBh, idesc, 1);
@@ -423,6 +447,15 @@ __global__ void f64_to_f32_kernel(const double* __restrict__ in, float* __restri
     if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) out[n - 1] = (float)in[n - 1];
 }
 
+// diagonal shift of the FP32 copy (valid rows only)
+__global__ void shift_diag_kernel(float* __restrict__ A, int bsz, int nb, int64_t N, float shift) {
+    const int64_t bb = (int64_t)bsz * bsz;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(i / bsz), r = (int)(i % bsz);
+        A[block_id(k, k, nb) * bb + (int64_t)r * bsz + r] += shift;
+    }
+}
+
 // lo[i] = a[i] - tf32(a[i]) over n floats
 __global__ void lo_part_kernel(const float* __restrict__ a, float* __restrict__ lo, int64_t n4) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
@@ -476,15 +509,16 @@ hs_status get_encoder() {
 }
 
 // 3-D FP32 map over `blocks` blocks of bsz x bsz, box = 32 columns x box_rows rows x 1 block
-hs_status make_map(CUtensorMap* m, float* base, int bsz, int64_t blocks, int box_rows) {
+hs_status make_map(CUtensorMap* m, float* base, int bsz, int64_t blocks, int box_rows, int box_k = kSlab) {
     hs_status st = get_encoder();
     if (st != HS_OK) return st;
     cuuint64_t dims[3] = {(cuuint64_t)bsz, (cuuint64_t)bsz, (cuuint64_t)blocks};
     cuuint64_t strides[2] = {(cuuint64_t)bsz * 4, (cuuint64_t)bsz * bsz * 4};
-    cuuint32_t box[3] = {(cuuint32_t)kSlab, (cuuint32_t)box_rows, 1};
+    cuuint32_t box[3] = {(cuuint32_t)box_k, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          box_k * 4 == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
@@ -512,13 +546,13 @@ hs_status tc_launch(hs_ctx ctx, int mode, const MixedWork& w, TcArgs a, int64_t 
 
 template <int BSZ>
 hs_status tc_update_launch(hs_ctx ctx, const MixedWork& w, const TcArgs& a, cudaStream_t s) {
-    using SM = TcSmem<BSZ>;
+    using SM = UpdSmem<BSZ>;
     const int m = a.nb - a.k - 1;
-    const int64_t ntiles = tri64(m) * SM::kTiles;
+    const int64_t ntiles = tri64(m) * (BSZ / 128);
     if (ntiles <= 0) return HS_OK;
     const int grid = (int)(ntiles < ctx->num_sms ? ntiles : ctx->num_sms);
     ctx->launches += 1;
-    tc_update_kernel<BSZ><<<grid, kUpdThreads, SM::kBytes, s>>>(w.mA128, w.mAB, w.mL128, w.mLB, a);
+    tc_update_kernel<BSZ><<<grid, kUpdThreads, SM::kBytes, s>>>(w.mU128, w.mUB, w.mV128, w.mVB, a);
     HS_CHECK_LAUNCH("tc_update_kernel");
     return HS_OK;
 }
@@ -536,7 +570,7 @@ hs_status tc_attrs() {
     HS_CUDA(cudaFuncSetAttribute(tc_tile_kernel<BSZ, MODE_UPDATE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  TcSmem<BSZ>::kBytes));
     HS_CUDA(cudaFuncSetAttribute(tc_update_kernel<BSZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 TcSmem<BSZ>::kBytes));
+                                 UpdSmem<BSZ>::kBytes));
     if (dev < 64) g_tc_attr[dev][slot] = true;
     return HS_OK;
 }
@@ -583,10 +617,14 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
     if (st == HS_OK) st = make_map(&w->mAB, w->A32, bsz, (int64_t)T, bsz);
     if (st == HS_OK) st = make_map(&w->mL128, w->LO, bsz, nb + 2, 128);
     if (st == HS_OK) st = make_map(&w->mLB, w->LO, bsz, nb + 2, bsz);
+    if (st == HS_OK) st = make_map(&w->mU128, w->A32, bsz, (int64_t)T, 128, kUpdK);
+    if (st == HS_OK) st = make_map(&w->mUB, w->A32, bsz, (int64_t)T, bsz, kUpdK);
+    if (st == HS_OK) st = make_map(&w->mV128, w->LO, bsz, nb + 2, 128, kUpdK);
+    if (st == HS_OK) st = make_map(&w->mVB, w->LO, bsz, nb + 2, bsz, kUpdK);
     return st;
 }
 
-hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s) {
+hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift) {
     const int bsz = ctx->bsz, nb = ctx->nb;
     HS_REQUIRE(bsz == 128 || bsz == 256, "the mixed-precision factor supports matrixBlockSize 128 or 256");
     hs_status st = bsz == 256 ? tc_attrs<256>() : tc_attrs<128>();
@@ -597,6 +635,11 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
     set_int_kernel<<<1, 1, 0, s>>>(w.err, 0);
     f64_to_f32_kernel<<<grid_for_elems(T * (int64_t)bb / 2, ctx->num_sms), 256, 0, s>>>(K64, w.A32, T * (int64_t)bb);
     HS_CHECK_LAUNCH("f64_to_f32");
+    if (shift != 0.0) {
+        ctx->launches += 1;
+        shift_diag_kernel<<<64, 256, 0, s>>>(w.A32, bsz, nb, ctx->N, (float)shift);
+        HS_CHECK_LAUNCH("shift_diag");
+    }
     // the factor works on a temporary context view whose "matrix" is the FP64 scratch block S
     for (int k = 0; k < nb; ++k) {
         const int right = nb - k;

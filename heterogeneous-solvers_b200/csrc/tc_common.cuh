@@ -104,6 +104,18 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr) {
     return d;
 }
 
+// the same for a K-major tile written by TMA with 64-byte swizzle: rows of 64
+// bytes, 8-row groups 512 bytes apart, layout type 4 (64B swizzle)
+__device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t smem_addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_addr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(512 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)4 << 61;
+    return d;
+}
+
 // instruction descriptor, kind::tf32 / kind::f16: D f32 ([4,6)=1), A/B format
 // ([7,10), [10,13)), both K-major, N >> 3 in [17,23), M >> 4 in [24,29)
 __host__ __device__ constexpr uint32_t umma_idesc(int a_fmt, int b_fmt, int M, int N) {

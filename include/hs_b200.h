@@ -244,10 +244,14 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
  * x <- x + (L L^T)^-1 (b - K x) with FP64 residuals until the backward error
  * ||b - K x|| / (||K||_F ||x||) <= tol.  When refinement stops contracting it
  * continues with conjugate gradients preconditioned by the FP32 factor.  b and x
- * are device vectors of hs_padded_vector_size doubles.  Allocates its own
- * workspace (FP32 factor: half the packed matrix).  Returns
- * HS_ERR_REFINEMENT_STALLED when neither reaches tol, HS_ERR_NOT_SPD when the
- * FP32 factor meets a non-positive pivot. */
+ * are device vectors of hs_padded_vector_size doubles.  The workspace (FP32
+ * factor: half the packed matrix) is kept by the context between calls.  When
+ * the FP32 factor of K meets a non-positive pivot (K too ill-conditioned for
+ * FP32), K + shift*I is factored instead, shift = 1e-6, 1e-5, 1e-4 or 1e-3
+ * times the largest diagonal entry, and the solve goes straight to CG
+ * preconditioned by that factor (report->shift; report->logdet is then the
+ * log-determinant of the shifted matrix).  Returns HS_ERR_REFINEMENT_STALLED
+ * when the target is not reached, HS_ERR_NOT_SPD when every shift fails. */
 typedef enum hs_precision {
     HS_PRECISION_FP64 = 0,
     HS_PRECISION_TF32X3 = 1,
@@ -257,7 +261,8 @@ typedef struct hs_mixed_report {
     int64_t refinement_steps;
     int64_t pcg_iterations;
     int fallback_pcg;
-    int reserved;
+    int factor_attempts;     /* 1 unless the FP32 factor of K broke down and K + shift*I was factored */
+    double shift;            /* diagonal shift of the low-precision factor (0: factor of K itself) */
     double backward_error;   /* ||b - K x|| / (||K||_F ||x||) at exit */
     double initial_backward_error; /* the same for x0 = (L L^T)^-1 b, before any refinement */
     double norm_k_fro;

@@ -121,3 +121,31 @@ def test_gp_solve_host_mixed(hs):
     assert bwd <= 2e-14
     assert rep.iterations >= 1
     np.testing.assert_array_equal(x, x2)
+
+
+def test_mixed_factor_breakdown_falls_back_to_shifted_preconditioner(hs, ctx):
+    """Duplicated inputs with sn2 = 1e-7 give pivots below the FP32 rounding noise,
+    so the FP32 factor of K breaks down; the solve then factors K + shift*I and
+    reaches the backward-error target with CG preconditioned by that factor."""
+    N, bsz, d = 1024, 128, 4
+    rng = np.random.default_rng(12)
+    base = rng.random((N // 2, d))
+    X = np.concatenate([base, base])[rng.permutation(N)]
+    y = np.sin(X.sum(axis=1)) + 0.1 * rng.standard_normal(N)
+    ctx.set_problem(N, bsz)
+    A = hs.SymmetricMatrix(N, bsz, device="cuda:0")
+    hs.MatrixGenerator.assemble(ctx, A.matrixData, X, 0.5, 1.0, 1e-7)
+    b = torch.zeros(hs.padded_size(N, bsz), dtype=torch.float64, device="cuda:0")
+    b[:N] = torch.from_numpy(y)
+    solver = hs.MixedPrecisionSolver(A, ctx)
+    x = solver.solve(b, tol=1e-14, max_steps=30)
+    rep = solver.report
+    print("breakdown case:", rep)
+    Kd = A.to_dense()
+    xg = x.cpu().numpy()[:N]
+    bwd = np.linalg.norm(y - Kd @ xg) / (np.linalg.norm(Kd, "fro") * np.linalg.norm(xg))
+    assert bwd <= 2e-14
+    if rep["factor_attempts"] > 1:
+        assert rep["shift"] > 0 and rep["fallback_pcg"] == 1
+    else:
+        assert rep["shift"] == 0.0
