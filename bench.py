@@ -65,6 +65,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
     ap.add_argument("--tol", type=float, default=1e-14, help="backward-error target of the mixed solve")
+    ap.add_argument("--precision", choices=["tf32x3", "bf16x3"], default="tf32x3",
+                    help="split products of the mixed factor's tensor-core updates")
     ap.add_argument("--lml-n", type=int, default=16384, help="N of the NLML+gradient leg (0: skip)")
     ap.add_argument("--sweep", action="store_true",
                     help="conditioning sweep: mixed vs FP64 solve for sn2 in {1e-1, 1e-3, 1e-6} (one JSON line)")
@@ -276,7 +278,7 @@ def run_sweep(args, hs, torch, ctx, Xd, bd, A, N, cfg, device):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        st = lib.hs_mixed_solve(ctx.handle, P(A), P(bd), P(xm), hs.PRECISIONS["tf32x3"], args.tol, 30,
+        st = lib.hs_mixed_solve(ctx.handle, P(A), P(bd), P(xm), hs.PRECISIONS[args.precision], args.tol, 30,
                                 ctypes.byref(rep))
         e1.record()
         torch.cuda.synchronize()
@@ -359,7 +361,7 @@ def main():
 
     def step_mixed():
         assemble()
-        hs._lib.check(lib.hs_mixed_solve(ctx.handle, P(A), P(bd), P(xd), hs.PRECISIONS["tf32x3"], args.tol,
+        hs._lib.check(lib.hs_mixed_solve(ctx.handle, P(A), P(bd), P(xd), hs.PRECISIONS[args.precision], args.tol,
                                          30, ctypes.byref(mrep)))
 
     def step_fp64(x_out):
@@ -528,6 +530,22 @@ def main():
     if cg_info and peaks.get("hbm_gbs") and cg_info["matvec_gbs"]:
         cg_info["matvec_frac_of_hbm"] = cg_info["matvec_gbs"] / peaks["hbm_gbs"]
 
+    if args.precision == "tf32x3":
+        peak3, peak_src, issued_key = tf32_peak / 3.0, (
+            "cuBLAS TF32 GEMM 8192^3 measured in this run, divided by the 3 TF32 products of one split FP32 "
+            "product (TF32 is absent from MEASURED_PEAKS.json)"), "issued_tf32_tflops"
+    else:
+        bf = peaks.get("bf16_tflops_sustained") or 1400.0
+        peak3, peak_src, issued_key = bf / 3.0, (
+            ("MEASURED_PEAKS.json bf16_tflops_sustained" if peaks.get("bf16_tflops_sustained") else
+             "fallback 1.4 PFLOP/s sustained bf16") + ", divided by the 3 BF16 products of one split product"), \
+            "issued_bf16_tflops"
+    roof = {"bound": "tensor", "achieved": useful, "peak": peak3 if useful else None, "unit": "TFLOP/s",
+            "frac": useful / peak3 if useful else None, "traffic": traffic,
+            "kernel": f"tc_update_kernel<256, {args.precision}> (split-product SYRK+GEMM trailing update, tcgen05, "
+                      "persistent)",
+            "peak_source": peak_src, "tf32_gemm_peak": tf32_peak, issued_key: 3 * useful if useful else None}
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -544,20 +562,14 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 (3xTF32 tensor-core factor) + f64 refinement",
+            "vs_baseline": None,
+            "dtype": ("f32 (3xTF32 tensor-core factor) + f64 refinement" if args.precision == "tf32x3" else
+                      "f32 (BF16-split tensor-core updates, 3xTF32 TRSM) + f64 refinement"),
             "data": f"synthetic: X~U[0,1]^({N}x{d}) seed {cfg['seed']}+rank, y=sin(sum_k x_k)+N(0,0.1^2)",
             "config": dict(bench_config(N, world), implementation=(
                 "RBF assembly + mixed-precision Cholesky (3xTF32 tensor-core TRSM/SYRK/GEMM, FP64 POTRF) + "
                 f"FP64 iterative refinement to backward error <= {args.tol:g}")),
-            "roofline": {"bound": "tensor", "achieved": useful,
-                         "peak": tf32_peak / 3.0 if useful else None, "unit": "TFLOP/s",
-                         "frac": useful / (tf32_peak / 3.0) if useful else None, "traffic": traffic,
-                         "kernel": "tc_update_kernel<256> (3xTF32 SYRK+GEMM trailing update, tcgen05, persistent)",
-                         "peak_source": "cuBLAS TF32 GEMM 8192^3 measured in this run, divided by the 3 TF32 "
-                                        "products of one split FP32 product (TF32 is absent from "
-                                        "MEASURED_PEAKS.json)",
-                         "tf32_gemm_peak": tf32_peak,
-                         "issued_tf32_tflops": 3 * useful if useful else None},
+            "roofline": roof,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "phases": phases, "mixed": mixed_report, "backward_error": bwd_mixed, "fp64": fp64,
             "lml_grad": lml, "cg": cg_info,

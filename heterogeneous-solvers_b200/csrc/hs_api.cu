@@ -68,6 +68,17 @@ hs_status ensure_mixed(hs_ctx ctx, size_t bytes) {
     return HS_OK;
 }
 
+hs_status ensure_gp(hs_ctx ctx, size_t bytes) {
+    if (ctx->gpws_bytes >= bytes) return HS_OK;
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->gpws) HS_CUDA(cudaFree(ctx->gpws));
+    ctx->gpws = nullptr;
+    ctx->gpws_bytes = 0;
+    HS_CUDA(cudaMalloc(&ctx->gpws, bytes));
+    ctx->gpws_bytes = bytes;
+    return HS_OK;
+}
+
 __global__ void set_i64_kernel(long long* p, long long v) { *p = v; }
 
 void set_i64_dev(long long* p, long long v, cudaStream_t s) { set_i64_kernel<<<1, 1, 0, s>>>(p, v); }
@@ -220,6 +231,7 @@ hs_status hs_ctx_destroy(hs_ctx ctx) {
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->work) cudaFree(ctx->work);
     if (ctx->mixed) cudaFree(ctx->mixed);
+    if (ctx->gpws) cudaFree(ctx->gpws);
     if (ctx->d_info) cudaFree(ctx->d_info);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     delete ctx;
@@ -237,8 +249,9 @@ hs_status hs_ctx_release_buffers(hs_ctx ctx) {
     if (ctx->scratch) HS_CUDA(cudaFree(ctx->scratch));
     if (ctx->work) HS_CUDA(cudaFree(ctx->work));
     if (ctx->mixed) HS_CUDA(cudaFree(ctx->mixed));
-    ctx->scratch = ctx->work = ctx->mixed = nullptr;
-    ctx->scratch_bytes = ctx->work_bytes = ctx->mixed_bytes = 0;
+    if (ctx->gpws) HS_CUDA(cudaFree(ctx->gpws));
+    ctx->scratch = ctx->work = ctx->mixed = ctx->gpws = nullptr;
+    ctx->scratch_bytes = ctx->work_bytes = ctx->mixed_bytes = ctx->gpws_bytes = 0;
     return HS_OK;
 }
 

@@ -248,9 +248,8 @@ hs_status hs_gp_nlml_grad(hs_ctx ctx, const double* X, const double* y, int d, c
     const size_t bytes = 2 * packed * sizeof(double) + adj + (size_t)n * sizeof(double) +
                          (size_t)N * d * sizeof(double) + 64 * sizeof(double) +
                          (size_t)parts * (dmax + 2) * sizeof(double) + 256 * sizeof(double);
-    DevBuf ws;
-    HS_CUDA(cudaMalloc(&ws.p, bytes));
-    double* L = static_cast<double*>(ws.p);
+    if ((st = ensure_gp(ctx, bytes)) != HS_OK) return st;  // kept by the context between calls
+    double* L = static_cast<double*>(ctx->gpws);
     double* Abar = L + packed;
     AdjointWork w;
     adjoint_bind(Abar + packed, nb, bsz, &w);

@@ -167,8 +167,8 @@ struct Events {
 
 hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,
                            int max_steps, hs_mixed_report* out) {
-    if (precision != HS_PRECISION_TF32X3) {
-        set_error("hs_mixed_solve: only HS_PRECISION_TF32X3 is implemented");
+    if (precision != HS_PRECISION_TF32X3 && precision != HS_PRECISION_BF16X3) {
+        set_error("hs_mixed_solve: precision must be HS_PRECISION_TF32X3 or HS_PRECISION_BF16X3");
         return HS_ERR_UNSUPPORTED;
     }
     if (!(tol > 0.0) || max_steps < 1) {
@@ -221,7 +221,7 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     for (int attempt = 1;; ++attempt) {
         ctx->launches += 1;
         set_i64_dev(ctx->d_info, INT64_MAX, s);
-        st = mixed_factor(ctx, K, w, s, shift);
+        st = mixed_factor(ctx, K, w, s, shift, precision);
         if (st != HS_OK) return st;
         HS_CUDA(cudaStreamSynchronize(s));
         st = mixed_check_error(ctx, w);
@@ -271,7 +271,6 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     st = mixed_apply(ctx, w, x, s);
     if (st != HS_OK) return st;
     double rn = 0, xn = 0, prev = INFINITY;
-    int stalls = 0;
     bool converged = false;
     int steps = 0;
     // a shifted factor is only a preconditioner: no refinement, straight to CG
@@ -285,11 +284,9 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
             converged = true;
             break;
         }
-        if (rn > 0.5 * prev) {
-            if (++stalls >= 2) break;
-        } else {
-            stalls = 0;
-        }
+        // a step that shrinks the residual by less than 8x means a poor contraction:
+        // conjugate gradients with the same preconditioner converges faster from here
+        if (rn > 0.125 * prev) break;
         prev = rn;
         // d = M^-1 r; x += d
         HS_CUDA(cudaMemcpyAsync(d, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_bf16.h>
 
 #include "hs_internal.cuh"
 
@@ -15,15 +16,19 @@ struct MixedWork {
     double* Ld = nullptr;   // FP64 diagonal blocks of L (nb blocks)
     double* Yinv = nullptr; // FP64 inverse diagonal blocks, Y_k = L_kk^-T (nb blocks)
     double* S = nullptr;    // FP64 scratch block (POTRF)
+    __nv_bfloat16* P16 = nullptr;  // BF16 split of the current panel: hi blocks 0..nb-1, lo blocks nb..2nb-1
     int* err = nullptr;     // tensor-core tile timeout flag
     CUtensorMap mA128, mAB, mL128, mLB;  // 128-byte swizzle, 32-wide K boxes (TRSM)
-    CUtensorMap mU128, mUB, mV128, mVB;  // 64-byte swizzle, 16-wide K boxes over A32 / LO (update)
+    CUtensorMap mU128, mUB, mV128, mVB;  // K boxes of 128 bytes over A32 / LO (TF32 update)
+    CUtensorMap mP128, mPB;              // K boxes of 128 bytes over P16 (BF16 update)
+    CUtensorMap mC32;                    // 32x32 FP32 boxes over A32 (TMA reduce of the update's C tiles)
 };
 
 size_t mixed_workspace_bytes(int64_t N, int bsz);
 hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w);
 // shift != 0: factor K + shift*I
-hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift = 0.0);
+hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift = 0.0,
+                       int precision = HS_PRECISION_TF32X3);
 hs_status mixed_check_error(hs_ctx ctx, const MixedWork& w);
 // the mixed-precision solve behind hs_mixed_solve (workspace kept by the context)
 hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,

@@ -21,6 +21,7 @@
 //              tile rows), C -= D (update) or L = D, L_lo = D - tf32(D) (TRSM)
 // Every mbarrier wait is bounded (2 s); on expiry the CTA records an error in
 // the context's flag word, frees its TMEM and returns.
+#include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
 #include "hs_internal.cuh"
@@ -222,13 +223,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 //                        lo*hi) into one of two TMEM accumulators (2 x BSZ
 //                        columns), so that the epilogue of tile i overlaps the
 //                        MMAs of tile i+1
-//   warps 2-5            epilogue: TMEM -> registers, C -= D, then free the
+//   warps 2-9            epilogue: TMEM -> registers -> -D in a swizzled shared
+//                        tile -> TMA reduce-add into C (two warps per TMEM lane
+//                        quarter, half the columns each), then free the
 //                        accumulator (one arrival per warp)
 // (Forming the low parts in shared memory instead of loading them halves the
 // L2 traffic but adds shared-memory traffic on the port the tensor core reads
 // its operands through; measured slower.)
 constexpr int kGroup = 8;
-constexpr int kUpdThreads = 192;
+constexpr int kUpdThreads = 320;
 // K floats per stage: 32 (128-byte rows, 128-byte swizzle, 2 stages of 96 KB)
 // measured faster than 16 (64-byte swizzle, 4 stages of 48 KB); the kernel is
 // limited by the shared-memory traffic of TMA writes plus the tensor core's
@@ -236,14 +239,29 @@ constexpr int kUpdThreads = 192;
 constexpr int kUpdK = 32;
 constexpr uint64_t kStepWaitNs = 2000000000ull;
 
+// operand formats of the update: TF32 (FP32 storage, hi = the FP32 value as
+// read by the tensor core, lo = x - tf32(x)) or BF16 (hi = bf16(x), lo =
+// bf16(x - hi)); both give 128-byte operand rows per slab and 32-byte K steps
+template <int PREC>
+struct UpdFmt;
+template <>
+struct UpdFmt<HS_PRECISION_TF32X3> {
+    static constexpr int kK = kUpdK, kKStep = 8, kFmt = kFmtTF32;
+};
+template <>
+struct UpdFmt<HS_PRECISION_BF16X3> {
+    static constexpr int kK = 2 * kUpdK, kKStep = 16, kFmt = kFmtBF16;
+};
+
 template <int BSZ>
 struct UpdSmem {
-    static constexpr int kA = 128 * kUpdK * 4;       // 8 KB
+    static constexpr int kA = 128 * kUpdK * 4;       // 8 KB per 16 K-columns of FP32
     static constexpr int kB = BSZ * kUpdK * 4;       // 16 / 8 KB
     static constexpr int kRaw = kA + kB;             // one of hi / lo
     static constexpr int kStage = 2 * kRaw;          // A_hi, B_hi, A_lo, B_lo (TMA bytes per stage)
     static constexpr int kStages = kUpdK == 32 ? 2 : 4;
-    static constexpr int kBytes = kStages * kStage + 1024 /* barriers, slot */ + 1024 /* alignment */;
+    static constexpr int kStaging = 8 * 32 * 32 * 4;  // one 32x32 FP32 tile per epilogue warp
+    static constexpr int kBytes = kStages * kStage + kStaging + 256 /* barriers, slot */ + 1024 /* alignment */;
 };
 
 __device__ __forceinline__ uint64_t upd_desc(uint32_t addr) {
@@ -277,17 +295,21 @@ __device__ __forceinline__ void grouped_pair(int64_t p, int m, int* rr, int* cc)
     *cc = r0 + j;
 }
 
-template <int BSZ>
+// mU*: maps of the hi parts, mV*: of the lo parts (*128: 128-row boxes, *B: BSZ-row boxes)
+template <int BSZ, int PREC>
 __global__ void __launch_bounds__(kUpdThreads, 1)
     tc_update_kernel(const __grid_constant__ CUtensorMap mU128, const __grid_constant__ CUtensorMap mUB,
-                     const __grid_constant__ CUtensorMap mV128, const __grid_constant__ CUtensorMap mVB, TcArgs a) {
+                     const __grid_constant__ CUtensorMap mV128, const __grid_constant__ CUtensorMap mVB,
+                     const __grid_constant__ CUtensorMap mC32, TcArgs a) {
     using SM = UpdSmem<BSZ>;
+    using F = UpdFmt<PREC>;
     constexpr int kTiles = BSZ / 128;
-    constexpr int kSlabs = BSZ / kUpdK;
+    constexpr int kSlabs = BSZ / F::kK;
     constexpr uint32_t kAccCols = 2 * BSZ;  // two accumulators
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + SM::kStages * SM::kStage);
+    uint8_t* staging = smem + SM::kStages * SM::kStage;  // 1024-aligned: the stage size is
+    uint64_t* full = reinterpret_cast<uint64_t*>(staging + SM::kStaging);
     uint64_t* empty = full + SM::kStages;
     uint64_t* tfull = empty + SM::kStages;
     uint64_t* tempty = tfull + 2;
@@ -296,7 +318,6 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m = a.nb - a.k - 1;
     const int64_t ntiles = tri64(m) * kTiles;
-    const size_t bb = (size_t)BSZ * BSZ;
 
     if (tid == 0) {
         for (int s = 0; s < SM::kStages; ++s) {
@@ -305,7 +326,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 4);
+            mbar_init(&tempty[b], 8);
         }
         fence_barrier_init();
     }
@@ -334,9 +355,12 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
                 int r, c, ti;
                 decode(t, &r, &c, &ti);
-                const int blkA = (int)(a.blockID + (r - a.k)), gA = r - a.k - 1;
-                const int blkB = (int)(a.blockID + (c - a.k)), gB = c - a.k - 1;
-                prefetch_l2(a.A32 + (size_t)block_id(r, c, a.nb) * bb + (size_t)ti * 128 * BSZ, 128 * BSZ * 4);
+                // TF32: hi = the FP32 panel block in A32, lo = its slot in LO;
+                // BF16: hi and lo are slots g and nb + g of the BF16 panel
+                const int gA = r - a.k - 1, gB = c - a.k - 1;
+                const bool bf = PREC == HS_PRECISION_BF16X3;
+                const int hiA = bf ? gA : (int)(a.blockID + (r - a.k)), loA = bf ? a.nb + gA : gA;
+                const int hiB = bf ? gB : (int)(a.blockID + (c - a.k)), loB = bf ? a.nb + gB : gB;
                 for (int kc = 0; kc < kSlabs; ++kc, ++g) {
                     const uint32_t s = g % SM::kStages, use = g / SM::kStages;
                     if (use > 0 && !mbar_wait_for(&empty[s], (use - 1) & 1, kStepWaitNs)) {
@@ -345,10 +369,10 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                     }
                     uint8_t* st = smem + s * SM::kStage;
                     mbar_arrive_expect_tx(&full[s], SM::kStage);
-                    tma_load_3d(st, &mU128, &full[s], kc * kUpdK, ti * 128, blkA);
-                    tma_load_3d(st + SM::kA, &mUB, &full[s], kc * kUpdK, 0, blkB);
-                    tma_load_3d(st + SM::kRaw, &mV128, &full[s], kc * kUpdK, ti * 128, gA);
-                    tma_load_3d(st + SM::kRaw + SM::kA, &mVB, &full[s], kc * kUpdK, 0, gB);
+                    tma_load_3d(st, &mU128, &full[s], kc * F::kK, ti * 128, hiA);
+                    tma_load_3d(st + SM::kA, &mUB, &full[s], kc * F::kK, 0, hiB);
+                    tma_load_3d(st + SM::kRaw, &mV128, &full[s], kc * F::kK, ti * 128, loA);
+                    tma_load_3d(st + SM::kRaw + SM::kA, &mVB, &full[s], kc * F::kK, 0, loB);
                 }
             }
             if (!ok) atomicExch(a.err, 1);
@@ -356,7 +380,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     } else if (warp == 1) {
         if (lane == 0) {
             // ---- MMA issuer
-            constexpr uint32_t idesc = umma_idesc(kFmtTF32, kFmtTF32, 128, BSZ);
+            constexpr uint32_t idesc = umma_idesc(F::kFmt, F::kFmt, 128, BSZ);
             uint32_t g = 0;
             int it = 0;
             for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++it) {
@@ -378,13 +402,19 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                     const uint32_t aHi = base, bHi = base + SM::kA;
                     const uint32_t aLo = base + SM::kRaw, bLo = aLo + SM::kA;
 #pragma unroll
-                    for (int ks = 0; ks < kUpdK / 8; ++ks) {
-                        const uint32_t off = ks * 32;  // 8 TF32 = 32 bytes along K
+                    for (int ks = 0; ks < F::kK / F::kKStep; ++ks) {
+                        const uint32_t off = ks * 32;  // one K step = 32 bytes along K
                         const uint64_t dAh = upd_desc(aHi + off), dAl = upd_desc(aLo + off);
                         const uint64_t dBh = upd_desc(bHi + off), dBl = upd_desc(bLo + off);
-                        umma_tf32(dcol, dAh, dBh, idesc, (kc | ks) != 0);
-                        umma_tf32(dcol, dAh, dBl, idesc, 1);
-                        umma_tf32(dcol, dAl, dBh, idesc, 1);
+                        if (PREC == HS_PRECISION_BF16X3) {
+                            umma_f16(dcol, dAh, dBh, idesc, (kc | ks) != 0);
+                            umma_f16(dcol, dAh, dBl, idesc, 1);
+                            umma_f16(dcol, dAl, dBh, idesc, 1);
+                        } else {
+                            umma_tf32(dcol, dAh, dBh, idesc, (kc | ks) != 0);
+                            umma_tf32(dcol, dAh, dBl, idesc, 1);
+                            umma_tf32(dcol, dAl, dBh, idesc, 1);
+                        }
                     }
                     umma_commit(&empty[s]);
                 }
@@ -394,9 +424,15 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             if (!ok) atomicExch(a.err, 1);
         }
     } else {
-        // ---- epilogue warps 2..5: lane quarter q = warp % 4 holds tile rows 32q..32q+31
+        // ---- epilogue warps 2..9: lane quarter q = warp % 4 holds tile rows 32q..32q+31;
+        // the two warps of a quarter split the BSZ columns.  Each 32x32 chunk of -D
+        // goes to the warp's shared tile (128-byte swizzle: 16-byte unit u of row i
+        // at unit u ^ (i % 8)) and is added into C by a TMA reduce, so C is read and
+        // written in whole lines by L2 instead of row by row by the SM.
         const int q = warp & 3;
-        const int row = q * 32 + lane;
+        const int half = (warp - 2) >> 2;  // 0: warps 2-5, 1: warps 6-9
+        constexpr int kChunks = BSZ / 64;   // 32-column chunks per warp
+        float4* stile = reinterpret_cast<float4*>(staging + (warp - 2) * 4096);
         int it = 0;
         for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
             const int b = it & 1, u = it >> 1;
@@ -410,21 +446,26 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             tc_fence_after();
             int r, c, ti;
             decode(t, &r, &c, &ti);
-            float* outp = a.A32 + (size_t)block_id(r, c, a.nb) * bb + (size_t)(ti * 128 + row) * BSZ;
+            const int cblk = (int)block_id(r, c, a.nb);
+            const int row0 = ti * 128 + q * 32;
+            const uint32_t tcol = taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BSZ + half * (BSZ / 2));
 #pragma unroll 1
-            for (int j = 0; j < BSZ / 32; ++j) {
+            for (int j = 0; j < kChunks; ++j) {
                 uint32_t v[32];
-                tmem_ld_32x32b_x32(taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BSZ + j * 32), v);
+                tmem_ld_32x32b_x32(tcol + (uint32_t)(j * 32), v);
                 tmem_ld_wait();
-                float4* o4 = reinterpret_cast<float4*>(outp + j * 32);
+                if (lane == 0) bulk_wait_read0();  // the previous chunk's reduce has read the tile
+                __syncwarp();
 #pragma unroll
-                for (int e = 0; e < 8; ++e) {
-                    float4 cv = o4[e];
-                    cv.x -= __uint_as_float(v[4 * e + 0]);
-                    cv.y -= __uint_as_float(v[4 * e + 1]);
-                    cv.z -= __uint_as_float(v[4 * e + 2]);
-                    cv.w -= __uint_as_float(v[4 * e + 3]);
-                    o4[e] = cv;
+                for (int e = 0; e < 8; ++e)
+                    stile[lane * 8 + (e ^ (lane & 7))] =
+                        make_float4(-__uint_as_float(v[4 * e + 0]), -__uint_as_float(v[4 * e + 1]),
+                                    -__uint_as_float(v[4 * e + 2]), -__uint_as_float(v[4 * e + 3]));
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) {
+                    tma_reduce_add_3d(&mC32, stile, half * (BSZ / 2) + j * 32, row0, cblk);
+                    bulk_commit();
                 }
             }
             tc_fence_before();
@@ -432,6 +473,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             if (lane == 0) mbar_arrive(&tempty[b]);
         }
     }
+    if (warp >= 2 && lane == 0) bulk_wait0();  // every reduce into C has completed
     tc_fence_before();
     __syncthreads();
     if (warp == 0) tmem_dealloc(taddr, kAccCols);
@@ -445,6 +487,18 @@ __global__ void f64_to_f32_kernel(const double* __restrict__ in, float* __restri
         reinterpret_cast<float2*>(out)[i] = make_float2((float)v.x, (float)v.y);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) out[n - 1] = (float)in[n - 1];
+}
+
+// BF16 split of the panel: P[i] = bf16(x), P[lo_off + i] = bf16(x - P[i]) (round to nearest)
+__global__ void panel_split_bf16_kernel(const float* __restrict__ x, __nv_bfloat16* __restrict__ P, int64_t n,
+                                        int64_t lo_off) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n / 2; i += (int64_t)gridDim.x * blockDim.x) {
+        const float2 v = reinterpret_cast<const float2*>(x)[i];
+        const __nv_bfloat162 hi = __floats2bfloat162_rn(v.x, v.y);
+        const float2 hf = __bfloat1622float2(hi);
+        reinterpret_cast<__nv_bfloat162*>(P)[i] = hi;
+        reinterpret_cast<__nv_bfloat162*>(P + lo_off)[i] = __floats2bfloat162_rn(v.x - hf.x, v.y - hf.y);
+    }
 }
 
 // diagonal shift of the FP32 copy (valid rows only)
@@ -509,16 +563,17 @@ hs_status get_encoder() {
 }
 
 // 3-D FP32 map over `blocks` blocks of bsz x bsz, box = 32 columns x box_rows rows x 1 block
-hs_status make_map(CUtensorMap* m, float* base, int bsz, int64_t blocks, int box_rows, int box_k = kSlab) {
+hs_status make_map(CUtensorMap* m, void* base, int bsz, int64_t blocks, int box_rows, int box_k = kSlab,
+                   int elem = 4) {
     hs_status st = get_encoder();
     if (st != HS_OK) return st;
     cuuint64_t dims[3] = {(cuuint64_t)bsz, (cuuint64_t)bsz, (cuuint64_t)blocks};
-    cuuint64_t strides[2] = {(cuuint64_t)bsz * 4, (cuuint64_t)bsz * bsz * 4};
+    cuuint64_t strides[2] = {(cuuint64_t)bsz * elem, (cuuint64_t)bsz * bsz * elem};
     cuuint32_t box[3] = {(cuuint32_t)box_k, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE,
-                          box_k * 4 == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+    CUresult r = g_encode(m, elem == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base,
+                          dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          box_k * elem == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
@@ -545,14 +600,19 @@ hs_status tc_launch(hs_ctx ctx, int mode, const MixedWork& w, TcArgs a, int64_t 
 }
 
 template <int BSZ>
-hs_status tc_update_launch(hs_ctx ctx, const MixedWork& w, const TcArgs& a, cudaStream_t s) {
+hs_status tc_update_launch(hs_ctx ctx, const MixedWork& w, const TcArgs& a, int precision, cudaStream_t s) {
     using SM = UpdSmem<BSZ>;
     const int m = a.nb - a.k - 1;
     const int64_t ntiles = tri64(m) * (BSZ / 128);
     if (ntiles <= 0) return HS_OK;
     const int grid = (int)(ntiles < ctx->num_sms ? ntiles : ctx->num_sms);
     ctx->launches += 1;
-    tc_update_kernel<BSZ><<<grid, kUpdThreads, SM::kBytes, s>>>(w.mU128, w.mUB, w.mV128, w.mVB, a);
+    if (precision == HS_PRECISION_BF16X3)
+        tc_update_kernel<BSZ, HS_PRECISION_BF16X3>
+            <<<grid, kUpdThreads, SM::kBytes, s>>>(w.mP128, w.mPB, w.mP128, w.mPB, w.mC32, a);
+    else
+        tc_update_kernel<BSZ, HS_PRECISION_TF32X3>
+            <<<grid, kUpdThreads, SM::kBytes, s>>>(w.mU128, w.mUB, w.mV128, w.mVB, w.mC32, a);
     HS_CHECK_LAUNCH("tc_update_kernel");
     return HS_OK;
 }
@@ -569,8 +629,10 @@ hs_status tc_attrs() {
                                  TcSmem<BSZ>::kBytes));
     HS_CUDA(cudaFuncSetAttribute(tc_tile_kernel<BSZ, MODE_UPDATE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  TcSmem<BSZ>::kBytes));
-    HS_CUDA(cudaFuncSetAttribute(tc_update_kernel<BSZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 UpdSmem<BSZ>::kBytes));
+    HS_CUDA(cudaFuncSetAttribute(tc_update_kernel<BSZ, HS_PRECISION_TF32X3>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, UpdSmem<BSZ>::kBytes));
+    HS_CUDA(cudaFuncSetAttribute(tc_update_kernel<BSZ, HS_PRECISION_BF16X3>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, UpdSmem<BSZ>::kBytes));
     if (dev < 64) g_tc_attr[dev][slot] = true;
     return HS_OK;
 }
@@ -592,6 +654,7 @@ size_t mixed_workspace_bytes(int64_t N, int bsz) {
     bytes += (size_t)(nb + 2) * bb * 4;  // LO
     bytes += (size_t)nb * bb * 8;        // Ldiag64
     bytes += (size_t)nb * bb * 8;        // Yinv
+    bytes += (size_t)2 * nb * bb * 2;    // BF16 panel hi / lo
     bytes += bb * 8;                     // S
     bytes += 1024;                       // flags
     return bytes;
@@ -610,6 +673,8 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
     p += (size_t)nb * bb * 8;
     w->Yinv = reinterpret_cast<double*>(p);
     p += (size_t)nb * bb * 8;
+    w->P16 = reinterpret_cast<__nv_bfloat16*>(p);
+    p += (size_t)2 * nb * bb * 2;
     w->S = reinterpret_cast<double*>(p);
     p += bb * 8;
     w->err = reinterpret_cast<int*>(p);
@@ -621,10 +686,13 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
     if (st == HS_OK) st = make_map(&w->mUB, w->A32, bsz, (int64_t)T, bsz, kUpdK);
     if (st == HS_OK) st = make_map(&w->mV128, w->LO, bsz, nb + 2, 128, kUpdK);
     if (st == HS_OK) st = make_map(&w->mVB, w->LO, bsz, nb + 2, bsz, kUpdK);
+    if (st == HS_OK) st = make_map(&w->mC32, w->A32, bsz, (int64_t)T, 32, 32);
+    if (st == HS_OK) st = make_map(&w->mP128, w->P16, bsz, 2 * (int64_t)nb, 128, 2 * kUpdK, 2);
+    if (st == HS_OK) st = make_map(&w->mPB, w->P16, bsz, 2 * (int64_t)nb, bsz, 2 * kUpdK, 2);
     return st;
 }
 
-hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift) {
+hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift, int precision) {
     const int bsz = ctx->bsz, nb = ctx->nb;
     HS_REQUIRE(bsz == 128 || bsz == 256, "the mixed-precision factor supports matrixBlockSize 128 or 256");
     hs_status st = bsz == 256 ? tc_attrs<256>() : tc_attrs<128>();
@@ -683,7 +751,15 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         a.syrkStart = k + 1;
         a.totalPairs = a.gemmPairs + m;
         prof_begin(ctx, s, HS_KERNEL_UPDATE);
-        st = bsz == 256 ? tc_update_launch<256>(ctx, w, a, s) : tc_update_launch<128>(ctx, w, a, s);
+        if (precision == HS_PRECISION_BF16X3) {
+            // BF16 hi / lo copies of the factored panel (blocks k+1..nb-1 of column k)
+            ctx->launches += 1;
+            panel_split_bf16_kernel<<<grid_for_elems((int64_t)m * bb / 2, ctx->num_sms), 256, 0, s>>>(
+                dblk + bb, w.P16, (int64_t)m * bb, (int64_t)nb * bb);
+            HS_CHECK_LAUNCH("panel_split_bf16");
+        }
+        st = bsz == 256 ? tc_update_launch<256>(ctx, w, a, precision, s)
+                        : tc_update_launch<128>(ctx, w, a, precision, s);
         if (st != HS_OK) return st;
         const double n3 = (double)bsz * bb;
         prof_end(ctx, s, HS_KERNEL_UPDATE, (double)a.gemmPairs * 2.0 * n3 + (double)m * bsz * bsz * (bsz + 1.0),

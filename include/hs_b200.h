@@ -61,7 +61,7 @@ hs_status hs_ctx_create(int device, void* stream, hs_ctx* out);
 hs_status hs_ctx_destroy(hs_ctx ctx);
 hs_status hs_ctx_set_stream(hs_ctx ctx, void* stream);
 /* The context keeps grow-only device buffers between calls (reduction partials,
- * matvec partial sums, solver work vectors, the mixed-precision workspace);
+ * matvec partial sums, solver work vectors, the mixed-precision and NLML workspaces);
  * this frees them all (after synchronising the stream).  They are allocated
  * again by the next call that needs them.  No reference counterpart (the
  * reference's solvers free their device copies in their destructors,
@@ -240,7 +240,10 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
  * No reference counterpart (new form).  hs_mixed_solve factors K (packed FP64,
  * device, left unchanged) in FP32 with the panel TRSM and the SYRK/GEMM trailing
  * updates on the tensor cores (tcgen05 kind::tf32, 3xTF32 split products, FP32
- * accumulation) and every diagonal-block POTRF in FP64, then refines
+ * accumulation) and every diagonal-block POTRF in FP64.  HS_PRECISION_BF16X3
+ * runs the trailing updates instead as BF16 split products (hi = bf16(x),
+ * lo = bf16(x - hi), hi*hi + hi*lo + lo*hi on tcgen05 kind::f16, FP32
+ * accumulation; ~2^-16 relative per product), the TRSM staying 3xTF32.  It then refines
  * x <- x + (L L^T)^-1 (b - K x) with FP64 residuals until the backward error
  * ||b - K x|| / (||K||_F ||x||) <= tol.  When refinement stops contracting it
  * continues with conjugate gradients preconditioned by the FP32 factor.  b and x
@@ -314,7 +317,8 @@ hs_status hs_cholesky_adjoint(hs_ctx ctx, const double* L, double* Abar);
  * (host, n_ell + 2 values; may be NULL).  FP64 factor on the tensor cores,
  * the gradient through hs_cholesky_adjoint of sum log L_ii and an on-the-fly
  * contraction that recomputes dK/dtheta from X (nothing of size N^2 besides L
- * and its adjoint is stored).  d <= 32; matrixBlockSize 128 or 256.  Returns
+ * and its adjoint is stored; that workspace is kept by the context between
+ * calls, see hs_ctx_release_buffers).  d <= 32; matrixBlockSize 128 or 256.  Returns
  * HS_ERR_NOT_SPD when K(theta) has no Cholesky factor. */
 typedef struct hs_gp_report {
     double factor_ms, adjoint_ms, grad_ms, total_ms;

@@ -149,3 +149,22 @@ def test_mixed_factor_breakdown_falls_back_to_shifted_preconditioner(hs, ctx):
         assert rep["shift"] > 0 and rep["fallback_pcg"] == 1
     else:
         assert rep["shift"] == 0.0
+
+
+@pytest.mark.parametrize("N,bsz,sn2", [(1000, 128, 1e-2), (2048, 256, 1e-2), (700, 256, 1e-1)])
+def test_mixed_bf16_split_reaches_fp64_backward_error(hs, ctx, N, bsz, sn2):
+    """The BF16 split variant of the trailing update: a less accurate factor
+    (~2^-16 per product instead of ~2^-21), still refined (or PCG-preconditioned)
+    to the FP64 backward-error target."""
+    A, b, X, y = _system(hs, ctx, N, bsz, 8, 0.5, sn2, seed=31)
+    solver = hs.MixedPrecisionSolver(A, ctx, "bf16x3")
+    x = solver.solve(b, tol=1e-14, max_steps=30)
+    rep = solver.report
+    Kd = A.to_dense()
+    xg = x.cpu().numpy()[:N]
+    bwd = np.linalg.norm(y - Kd @ xg) / (np.linalg.norm(Kd, "fro") * np.linalg.norm(xg))
+    print(f"bf16x3 N={N} bsz={bsz} sn2={sn2}: steps {rep['refinement_steps']} pcg {rep['pcg_iterations']} "
+          f"bwd0 {rep['initial_backward_error']:.2e} bwd {bwd:.2e}")
+    assert bwd <= 2e-14
+    # a BF16-split factor: unrefined backward error well below plain BF16's ~1e-3
+    assert rep["initial_backward_error"] <= 1e-4
