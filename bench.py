@@ -65,8 +65,9 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
     ap.add_argument("--tol", type=float, default=1e-14, help="backward-error target of the mixed solve")
-    ap.add_argument("--precision", choices=["tf32x3", "bf16x3"], default="tf32x3",
-                    help="split products of the mixed factor's tensor-core updates")
+    ap.add_argument("--precision", choices=["tf32x3", "bf16x3"], default="bf16x3",
+                    help="split products of the headline mixed factor's tensor-core updates (the other variant "
+                         "is timed as a leg of the same run)")
     ap.add_argument("--lml-n", type=int, default=16384, help="N of the NLML+gradient leg (0: skip)")
     ap.add_argument("--sweep", action="store_true",
                     help="conditioning sweep: mixed vs FP64 solve for sn2 in {1e-1, 1e-3, 1e-6} (one JSON line)")
@@ -429,6 +430,30 @@ def main():
     x_mixed = xd.clone()
     bwd_mixed = backward_error(x_mixed)
 
+    # ---------------- the other split variant of the mixed form on the same system
+    other = "tf32x3" if args.precision == "bf16x3" else "bf16x3"
+    alt = None
+    if not args.no_fp64:
+        orep = hs._lib.MixedReport()
+        xo = torch.empty_like(bd)
+
+        def step_other():
+            assemble()
+            hs._lib.check(lib.hs_mixed_solve(ctx.handle, P(A), P(bd), P(xo), hs.PRECISIONS[other], args.tol, 30,
+                                             ctypes.byref(orep)))
+
+        step_other()  # warm-up (kernel loading)
+        torch.cuda.synchronize()
+        o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        o0.record()
+        step_other()
+        o1.record()
+        torch.cuda.synchronize()
+        alt = {"precision": other, "ms_per_step": o0.elapsed_time(o1),
+               "report": {f: getattr(orep, f) for f, _ in hs._lib.MixedReport._fields_},
+               "backward_error": backward_error(xo)}
+        del xo
+
     # ---------------- FP64 factor + solve on the same system (the comparison at equal error)
     fp64 = None
     if not args.no_fp64:
@@ -458,6 +483,8 @@ def main():
                 "update_dmma_tflops": upd64["flops"] / (upd64["ms"] * 1e-3) / 1e12 if upd64["ms"] else None,
                 "speedup_mixed_vs_fp64": fp64_ms / ms_per_step}
         fp64["mixed_x_rel_diff"] = float((torch.linalg.norm(x_mixed - x64) / torch.linalg.norm(x64)).item())
+        if alt is not None:
+            alt["speedup_vs_fp64"] = fp64_ms / alt["ms_per_step"]
         fp64["mixed_logdet_rel_diff"] = abs(mixed_report["logdet"] - logdet64) / abs(logdet64)
         fp64["logdet"] = logdet64
         del x64
@@ -567,12 +594,14 @@ def main():
                       "f32 (BF16-split tensor-core updates, 3xTF32 TRSM) + f64 refinement"),
             "data": f"synthetic: X~U[0,1]^({N}x{d}) seed {cfg['seed']}+rank, y=sin(sum_k x_k)+N(0,0.1^2)",
             "config": dict(bench_config(N, world), implementation=(
-                "RBF assembly + mixed-precision Cholesky (3xTF32 tensor-core TRSM/SYRK/GEMM, FP64 POTRF) + "
-                f"FP64 iterative refinement to backward error <= {args.tol:g}")),
+                "RBF assembly + mixed-precision Cholesky (" +
+                ("3xTF32 tensor-core TRSM/SYRK/GEMM" if args.precision == "tf32x3" else
+                 "BF16-split tensor-core SYRK/GEMM, 3xTF32 tensor-core TRSM") +
+                f", FP64 POTRF) + FP64 iterative refinement / preconditioned CG to backward error <= {args.tol:g}")),
             "roofline": roof,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "phases": phases, "mixed": mixed_report, "backward_error": bwd_mixed, "fp64": fp64,
-            "lml_grad": lml, "cg": cg_info,
+            "precision": args.precision, "other_split_variant": alt, "lml_grad": lml, "cg": cg_info,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -48,6 +48,7 @@ struct TcArgs {
     int syrkStart;
     int64_t totalPairs;
     int* err;          // error flag (timeouts)
+    int part;          // persistent update: 0 all of columns k+1.., 1 column k+1 only, 2 columns k+2..
 };
 
 template <int BSZ>
@@ -317,7 +318,10 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m = a.nb - a.k - 1;
-    const int64_t ntiles = tri64(m) * kTiles;
+    // part 1: the m blocks of column k+1; part 2: the lower triangle of columns k+2..;
+    // part 0: both (the m x m lower triangle of columns k+1..)
+    const int mt = a.part == 2 ? m - 1 : m;
+    const int64_t ntiles = (a.part == 1 ? (int64_t)m : tri64(mt)) * kTiles;
 
     if (tid == 0) {
         for (int s = 0; s < SM::kStages; ++s) {
@@ -341,11 +345,18 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     bool ok = true;
 
     auto decode = [&](int64_t t, int* r, int* c, int* ti) {
-        int rr, cc;
-        grouped_pair(t / kTiles, m, &rr, &cc);
         *ti = (int)(t % kTiles);
-        *r = a.k + 1 + rr;
-        *c = a.k + 1 + cc;
+        const int64_t p = t / kTiles;
+        if (a.part == 1) {
+            *r = a.k + 1 + (int)p;
+            *c = a.k + 1;
+            return;
+        }
+        int rr, cc;
+        grouped_pair(p, mt, &rr, &cc);
+        const int base = a.k + (a.part == 2 ? 2 : 1);
+        *r = base + rr;
+        *c = base + cc;
     };
 
     if (warp == 0) {
@@ -600,12 +611,13 @@ hs_status tc_launch(hs_ctx ctx, int mode, const MixedWork& w, TcArgs a, int64_t 
 }
 
 template <int BSZ>
-hs_status tc_update_launch(hs_ctx ctx, const MixedWork& w, const TcArgs& a, int precision, cudaStream_t s) {
+hs_status tc_update_launch(hs_ctx ctx, const MixedWork& w, const TcArgs& a, int precision, cudaStream_t s,
+                           int max_ctas) {
     using SM = UpdSmem<BSZ>;
     const int m = a.nb - a.k - 1;
-    const int64_t ntiles = tri64(m) * (BSZ / 128);
+    const int64_t ntiles = (a.part == 1 ? (int64_t)m : tri64(a.part == 2 ? m - 1 : m)) * (BSZ / 128);
     if (ntiles <= 0) return HS_OK;
-    const int grid = (int)(ntiles < ctx->num_sms ? ntiles : ctx->num_sms);
+    const int grid = (int)(ntiles < max_ctas ? ntiles : max_ctas);
     ctx->launches += 1;
     if (precision == HS_PRECISION_BF16X3)
         tc_update_kernel<BSZ, HS_PRECISION_BF16X3>
@@ -708,26 +720,37 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         shift_diag_kernel<<<64, 256, 0, s>>>(w.A32, bsz, nb, ctx->N, (float)shift);
         HS_CHECK_LAUNCH("shift_diag");
     }
-    // the factor works on a temporary context view whose "matrix" is the FP64 scratch block S
-    for (int k = 0; k < nb; ++k) {
-        const int right = nb - k;
-        const int64_t blockID = T - (int64_t)right * (right + 1) / 2;
-        float* dblk = w.A32 + (size_t)blockID * bb;
-        // diagonal block in FP64: POTRF, then Y = L^-T by TRSM on the identity
+    // diagonal block k in FP64: POTRF of its FP32 values, Y_k = L_kk^-T by TRSM on the
+    // identity, then the FP32 copy, the FP64 L_kk, and the split L_kk^-1 for the TRSM
+    auto diag_chain = [&](int k, cudaStream_t st_) -> hs_status {
+        const int64_t id = T - (int64_t)(nb - k) * (nb - k + 1) / 2;
+        float* dblk = w.A32 + (size_t)id * bb;
         double* Yk = w.Yinv + (size_t)k * bb;
         const int64_t valid = ctx->N - (int64_t)k * bsz;
         ctx->launches += 1;
-        diag_in_kernel<<<64, 256, 0, s>>>(dblk, w.S, Yk, bsz, valid < bsz ? (int)valid : bsz);
-        st = launch_potrf(ctx, w.S, 0, k, s);  // block 0 of the scratch, guard rows of block row k
-        if (st != HS_OK) return st;
-        st = launch_trsm_on(ctx, w.S, bsz, Yk, 1, s);
-        if (st != HS_OK) return st;
+        diag_in_kernel<<<64, 256, 0, st_>>>(dblk, w.S, Yk, bsz, valid < bsz ? (int)valid : bsz);
+        hs_status r = launch_potrf(ctx, w.S, 0, k, st_);  // block 0 of the scratch, guard rows of block row k
+        if (r != HS_OK) return r;
+        r = launch_trsm_on(ctx, w.S, bsz, Yk, 1, st_);
+        if (r != HS_OK) return r;
         ctx->launches += 1;
-        diag_out_kernel<<<64, 256, 0, s>>>(w.S, Yk, dblk, w.Ld + (size_t)k * bb, w.LO + (size_t)nb * bb,
-                                           w.LO + (size_t)(nb + 1) * bb, bsz);
+        diag_out_kernel<<<64, 256, 0, st_>>>(w.S, Yk, dblk, w.Ld + (size_t)k * bb, w.LO + (size_t)nb * bb,
+                                             w.LO + (size_t)(nb + 1) * bb, bsz);
         HS_CHECK_LAUNCH("mixed diag");
+        return HS_OK;
+    };
+    // Lookahead: the update of column k runs in two launches, column k+1 first; the
+    // diagonal chain of block k+1 then runs on the side stream, on SMs the second
+    // (larger) launch leaves free, while that launch updates columns k+2..
+    const bool lookahead = ctx->side != nullptr && ctx->num_sms > 8;
+    const int kFree = 2;
+    if ((st = diag_chain(0, s)) != HS_OK) return st;
+    const double n3 = (double)bsz * bb;
+    for (int k = 0; k < nb - 1; ++k) {
+        const int right = nb - k;
+        const int64_t blockID = T - (int64_t)right * (right + 1) / 2;
+        float* dblk = w.A32 + (size_t)blockID * bb;
         const int m = nb - k - 1;
-        if (m == 0) break;
         // low parts of the raw panel, TRSM-as-GEMM with L^-T (writes L and its low part)
         ctx->launches += 1;
         lo_part_kernel<<<grid_for_elems((int64_t)m * bb / 4, ctx->num_sms), 256, 0, s>>>(dblk + bb, w.LO,
@@ -744,13 +767,6 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         st = bsz == 256 ? tc_launch<256>(ctx, MODE_TRSM, w, a, m, s) : tc_launch<128>(ctx, MODE_TRSM, w, a, m, s);
         if (st != HS_OK) return st;
         prof_end(ctx, s, HS_KERNEL_TRSM, (double)m * 2.0 * bsz * bb, 4.0 * m * bb * 4.0);
-        // trailing update: GEMM pairs for rows k+2.., SYRK blocks k+1.. (as full blocks)
-        const int64_t g0 = 1, g1 = m;  // rows r' = r - k - 1 in [1, m)
-        a.pairBase = g0 * (g0 - 1) / 2;
-        a.gemmPairs = g1 * (g1 - 1) / 2 - a.pairBase;
-        a.syrkStart = k + 1;
-        a.totalPairs = a.gemmPairs + m;
-        prof_begin(ctx, s, HS_KERNEL_UPDATE);
         if (precision == HS_PRECISION_BF16X3) {
             // BF16 hi / lo copies of the factored panel (blocks k+1..nb-1 of column k)
             ctx->launches += 1;
@@ -758,12 +774,38 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
                 dblk + bb, w.P16, (int64_t)m * bb, (int64_t)nb * bb);
             HS_CHECK_LAUNCH("panel_split_bf16");
         }
-        st = bsz == 256 ? tc_update_launch<256>(ctx, w, a, precision, s)
-                        : tc_update_launch<128>(ctx, w, a, precision, s);
+        // trailing update, part 1: column k+1 (m - 1 GEMM blocks + the SYRK block k+1)
+        a.part = 1;
+        prof_begin(ctx, s, HS_KERNEL_UPDATE);
+        st = bsz == 256 ? tc_update_launch<256>(ctx, w, a, precision, s, ctx->num_sms)
+                        : tc_update_launch<128>(ctx, w, a, precision, s, ctx->num_sms);
         if (st != HS_OK) return st;
-        const double n3 = (double)bsz * bb;
-        prof_end(ctx, s, HS_KERNEL_UPDATE, (double)a.gemmPairs * 2.0 * n3 + (double)m * bsz * bsz * (bsz + 1.0),
-                 ((double)a.totalPairs * 2.0 + 2.0 * m) * bb * 4.0);
+        prof_end(ctx, s, HS_KERNEL_UPDATE, (m - 1.0) * 2.0 * n3 + (double)bsz * bsz * (bsz + 1.0),
+                 ((m - 1.0) * 2.0 + 2.0 + 2.0 * m) * bb * 4.0);
+        const bool side = lookahead && m >= 2;
+        if (side) {
+            HS_CUDA(cudaEventRecord(ctx->ev_a, s));
+            HS_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_a, 0));
+            if ((st = diag_chain(k + 1, ctx->side)) != HS_OK) return st;
+            HS_CUDA(cudaEventRecord(ctx->ev_b, ctx->side));
+        }
+        // part 2: columns k+2.. (the (m-1) x (m-1) lower triangle)
+        if (m >= 2) {
+            a.part = 2;
+            const double gp = (m - 1.0) * (m - 2.0) / 2.0;
+            prof_begin(ctx, s, HS_KERNEL_UPDATE);
+            const int cap = side ? ctx->num_sms - kFree : ctx->num_sms;
+            st = bsz == 256 ? tc_update_launch<256>(ctx, w, a, precision, s, cap)
+                            : tc_update_launch<128>(ctx, w, a, precision, s, cap);
+            if (st != HS_OK) return st;
+            prof_end(ctx, s, HS_KERNEL_UPDATE, gp * 2.0 * n3 + (m - 1.0) * bsz * bsz * (bsz + 1.0),
+                     ((gp + m - 1.0) * 2.0 + 2.0 * m) * bb * 4.0);
+        }
+        if (side) {
+            HS_CUDA(cudaStreamWaitEvent(s, ctx->ev_b, 0));
+        } else if ((st = diag_chain(k + 1, s)) != HS_OK) {
+            return st;
+        }
     }
     return HS_OK;
 }
