@@ -283,7 +283,7 @@ def run_sweep(args, hs, torch, ctx, Xd, bd, A, N, cfg, device):
                                 ctypes.byref(rep))
         e1.record()
         torch.cuda.synchronize()
-        row["mixed"] = {f: getattr(rep, f) for f, _ in hs._lib.MixedReport._fields_}
+        row["mixed"] = {f: getattr(rep, f) for f, _ in hs._lib.MixedReport._fields_ if f != "reserved"}
         row["mixed"]["status"] = hs._lib.STATUS_NAMES.get(int(st), int(st))
         row["mixed"]["ms"] = e0.elapsed_time(e1)
         row["mixed"]["backward_error_host_check"] = bwd(xm) if st == 0 else None
@@ -426,7 +426,7 @@ def main():
         dist.barrier()
     ms_per_step = t_max_ms / args.steps
     value = world * args.steps / (t_max_ms * 1e-3)
-    mixed_report = {f: getattr(mrep, f) for f, _ in hs._lib.MixedReport._fields_}
+    mixed_report = {f: getattr(mrep, f) for f, _ in hs._lib.MixedReport._fields_ if f != "reserved"}
     x_mixed = xd.clone()
     bwd_mixed = backward_error(x_mixed)
 
@@ -450,7 +450,7 @@ def main():
         o1.record()
         torch.cuda.synchronize()
         alt = {"precision": other, "ms_per_step": o0.elapsed_time(o1),
-               "report": {f: getattr(orep, f) for f, _ in hs._lib.MixedReport._fields_},
+               "report": {f: getattr(orep, f) for f, _ in hs._lib.MixedReport._fields_ if f != "reserved"},
                "backward_error": backward_error(xo)}
         del xo
 

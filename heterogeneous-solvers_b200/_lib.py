@@ -42,7 +42,8 @@ class SolveReport(ctypes.Structure):
 
 class MixedReport(ctypes.Structure):
     _fields_ = [("refinement_steps", ctypes.c_int64), ("pcg_iterations", ctypes.c_int64),
-                ("fallback_pcg", ctypes.c_int), ("factor_attempts", ctypes.c_int), ("shift", ctypes.c_double),
+                ("fallback_pcg", ctypes.c_int), ("factor_attempts", ctypes.c_int),
+                ("precision_used", ctypes.c_int), ("reserved", ctypes.c_int), ("shift", ctypes.c_double),
                 ("backward_error", ctypes.c_double),
                 ("initial_backward_error", ctypes.c_double), ("norm_k_fro", ctypes.c_double),
                 ("logdet", ctypes.c_double), ("factor_ms", ctypes.c_double), ("refine_ms", ctypes.c_double),

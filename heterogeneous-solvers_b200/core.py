@@ -444,7 +444,7 @@ class MixedPrecisionSolver:
         status = _lib.load().hs_mixed_solve(ctx.handle, _dptr(K, ctx), _dptr(bd, ctx), _dptr(x, ctx),
                                             PRECISIONS[self.precision], float(tol), int(max_steps),
                                             ctypes.byref(rep))
-        self.report = {f: getattr(rep, f) for f, _ in MixedReport._fields_}
+        self.report = {f: getattr(rep, f) for f, _ in MixedReport._fields_ if f != "reserved"}
         _lib.check(status)
         return x
 

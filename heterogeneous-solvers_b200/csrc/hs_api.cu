@@ -79,6 +79,17 @@ hs_status ensure_gp(hs_ctx ctx, size_t bytes) {
     return HS_OK;
 }
 
+hs_status ensure_hostws(hs_ctx ctx, size_t bytes) {
+    if (ctx->hostws_bytes >= bytes) return HS_OK;
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->hostws) HS_CUDA(cudaFree(ctx->hostws));
+    ctx->hostws = nullptr;
+    ctx->hostws_bytes = 0;
+    HS_CUDA(cudaMalloc(&ctx->hostws, bytes));
+    ctx->hostws_bytes = bytes;
+    return HS_OK;
+}
+
 __global__ void set_i64_kernel(long long* p, long long v) { *p = v; }
 
 void set_i64_dev(long long* p, long long v, cudaStream_t s) { set_i64_kernel<<<1, 1, 0, s>>>(p, v); }
@@ -232,6 +243,7 @@ hs_status hs_ctx_destroy(hs_ctx ctx) {
     if (ctx->work) cudaFree(ctx->work);
     if (ctx->mixed) cudaFree(ctx->mixed);
     if (ctx->gpws) cudaFree(ctx->gpws);
+    if (ctx->hostws) cudaFree(ctx->hostws);
     if (ctx->d_info) cudaFree(ctx->d_info);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     delete ctx;
@@ -250,8 +262,9 @@ hs_status hs_ctx_release_buffers(hs_ctx ctx) {
     if (ctx->work) HS_CUDA(cudaFree(ctx->work));
     if (ctx->mixed) HS_CUDA(cudaFree(ctx->mixed));
     if (ctx->gpws) HS_CUDA(cudaFree(ctx->gpws));
-    ctx->scratch = ctx->work = ctx->mixed = ctx->gpws = nullptr;
-    ctx->scratch_bytes = ctx->work_bytes = ctx->mixed_bytes = ctx->gpws_bytes = 0;
+    if (ctx->hostws) HS_CUDA(cudaFree(ctx->hostws));
+    ctx->scratch = ctx->work = ctx->mixed = ctx->gpws = ctx->hostws = nullptr;
+    ctx->scratch_bytes = ctx->work_bytes = ctx->mixed_bytes = ctx->gpws_bytes = ctx->hostws_bytes = 0;
     return HS_OK;
 }
 

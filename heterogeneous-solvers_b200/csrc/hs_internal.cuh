@@ -32,6 +32,9 @@ struct hs_ctx_s {
     // grow-only workspace of the NLML + gradient (factor, adjoint, temporaries)
     void* gpws = nullptr;
     size_t gpws_bytes = 0;
+    // grow-only device copies of the host-buffer GP solve (X, K, y, x)
+    void* hostws = nullptr;
+    size_t hostws_bytes = 0;
 
     // device word holding the smallest failing pivot row (INT64_MAX = none)
     long long* d_info = nullptr;
@@ -98,6 +101,7 @@ hs_status ensure_scratch(hs_ctx ctx, size_t bytes);
 hs_status ensure_work(hs_ctx ctx, size_t bytes);
 hs_status ensure_mixed(hs_ctx ctx, size_t bytes);
 hs_status ensure_gp(hs_ctx ctx, size_t bytes);
+hs_status ensure_hostws(hs_ctx ctx, size_t bytes);
 
 // scratch layout: [0, 32 KB) reduction partials, [32 KB, 48 KB) solver scalars,
 // [56 KB, 64 KB) small constants; matvec partial blocks start at 64 KB

@@ -217,34 +217,43 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     // factor (a non-positive FP64 pivot of the FP32 matrix is recorded in ctx->d_info);
     // on breakdown, factor K + shift*I with a growing shift and use it as a CG preconditioner
     double shift = 0.0;
+    int prec = precision;
     HS_CUDA(cudaEventRecord(ev.e[0], s));
     for (int attempt = 1;; ++attempt) {
         ctx->launches += 1;
         set_i64_dev(ctx->d_info, INT64_MAX, s);
-        st = mixed_factor(ctx, K, w, s, shift, precision);
+        st = mixed_factor(ctx, K, w, s, shift, prec);
         if (st != HS_OK) return st;
         HS_CUDA(cudaStreamSynchronize(s));
+        if (ctx->side) HS_CUDA(cudaStreamSynchronize(ctx->side));
         st = mixed_check_error(ctx, w);
         if (st != HS_OK) return st;
         int64_t info = -1;
         st = hs_ctx_take_info(ctx, &info);
         if (st != HS_OK) return st;
         R.factor_attempts = attempt;
+        R.precision_used = prec;
         R.shift = shift;
         if (info < 0) break;
-        if (attempt == 5) {
-            set_error("hs_mixed_solve: the FP32 factor met a non-positive pivot at row " + std::to_string(info) +
-                      " even with a diagonal shift of " + std::to_string(shift));
+        if (prec == HS_PRECISION_BF16X3) {  // the more accurate split products first
+            prec = HS_PRECISION_TF32X3;
+            continue;
+        }
+        if (shift > 0.0 && shift >= 0.05 * h[9]) {
+            set_error("hs_mixed_solve: the low-precision factor met a non-positive pivot at row " +
+                      std::to_string(info) + " even with a diagonal shift of " + std::to_string(shift));
             return HS_ERR_NOT_SPD;
         }
-        if (attempt == 1) {
+        if (shift == 0.0) {
             ctx->launches += 1;
             maxdiag_kernel<<<1, 1024, 0, s>>>(K, bsz, nb, ctx->N, scal + 3);
             HS_CHECK_LAUNCH("maxdiag");
             HS_CUDA(cudaMemcpyAsync((void*)(h + 9), scal + 3, sizeof(double), cudaMemcpyDeviceToHost, s));
             HS_CUDA(cudaStreamSynchronize(s));
+            shift = 1e-6 * h[9];
+        } else {
+            shift *= 10.0;  // 1e-6 .. 1e-1 x the largest diagonal entry
         }
-        shift = h[9] * std::pow(10.0, -7 + attempt);  // 1e-6, 1e-5, 1e-4, 1e-3 x max diag
     }
     HS_CUDA(cudaEventRecord(ev.e[1], s));
     // log|K| from the FP64 diagonal blocks

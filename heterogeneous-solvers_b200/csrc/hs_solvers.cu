@@ -322,10 +322,6 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
     cudaEvent_t ev[5] = {};
     auto cleanup = [&]() {
         cudaStreamSynchronize(s);
-        if (Xd) cudaFree(Xd);
-        if (Ad) cudaFree(Ad);
-        if (bd) cudaFree(bd);
-        if (xd) cudaFree(xd);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
     };
@@ -340,10 +336,16 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
     } while (0)
     for (auto& e : ev) HS_E2E(cudaEventCreate(&e));
     HS_E2E(cudaEventRecord(ev[0], s));
-    HS_E2E(cudaMalloc(&Xd, (size_t)N * d * sizeof(double)));
-    HS_E2E(cudaMalloc(&Ad, packed * sizeof(double)));
-    HS_E2E(cudaMalloc(&bd, n * sizeof(double)));
-    HS_E2E(cudaMalloc(&xd, n * sizeof(double)));
+    {
+        // device copies kept by the context between calls (hs_ctx_release_buffers frees them)
+        const size_t xbytes = ((size_t)N * d * sizeof(double) + 255) & ~size_t(255);
+        st = ensure_hostws(ctx, xbytes + (packed + 2 * (size_t)n) * sizeof(double));
+        if (st != HS_OK) { cleanup(); return st; }
+        Xd = static_cast<double*>(ctx->hostws);
+        Ad = reinterpret_cast<double*>(static_cast<char*>(ctx->hostws) + xbytes);
+        bd = Ad + packed;
+        xd = bd + n;
+    }
     HS_E2E(cudaMemcpyAsync(Xd, X_host, (size_t)N * d * sizeof(double), cudaMemcpyHostToDevice, s));
     HS_E2E(cudaMemsetAsync(bd, 0, n * sizeof(double), s));
     HS_E2E(cudaMemcpyAsync(bd, y_host, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s));

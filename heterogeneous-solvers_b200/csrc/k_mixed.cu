@@ -49,7 +49,19 @@ struct TcArgs {
     int64_t totalPairs;
     int* err;          // error flag (timeouts)
     int part;          // persistent update: 0 all of columns k+1.., 1 column k+1 only, 2 columns k+2..
+    const long long* abort_flag;  // smallest failing pivot row so far (INT64_MAX: none)
 };
+
+// CTA-uniform early exit once a diagonal POTRF has recorded a non-positive pivot:
+// the factor will be discarded, so the remaining tensor-core work is skipped.  The
+// decision is taken by thread 0 and shared before any barrier or TMEM use, because
+// the look-ahead POTRF may record a pivot while this kernel runs.
+__device__ __forceinline__ bool factor_aborted(const long long* flag) {
+    __shared__ int s_abort;
+    if (threadIdx.x == 0) s_abort = (*reinterpret_cast<const volatile long long*>(flag) != INT64_MAX) ? 1 : 0;
+    __syncthreads();
+    return s_abort != 0;
+}
 
 template <int BSZ>
 struct TcSmem {
@@ -66,6 +78,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_tile_kernel(const __grid_constant__ CUtensorMap mA128, const __grid_constant__ CUtensorMap mAB,
                    const __grid_constant__ CUtensorMap mL128, const __grid_constant__ CUtensorMap mLB, TcArgs a) {
     using SM = TcSmem<BSZ>;
+    if (factor_aborted(a.abort_flag)) return;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + SM::kStages * SM::kStage);
@@ -304,6 +317,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                      const __grid_constant__ CUtensorMap mC32, TcArgs a) {
     using SM = UpdSmem<BSZ>;
     using F = UpdFmt<PREC>;
+    if (factor_aborted(a.abort_flag)) return;
     constexpr int kTiles = BSZ / 128;
     constexpr int kSlabs = BSZ / F::kK;
     constexpr uint32_t kAccCols = 2 * BSZ;  // two accumulators
@@ -763,6 +777,7 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         a.k = k;
         a.nb = nb;
         a.err = w.err;
+        a.abort_flag = ctx->d_info;
         prof_begin(ctx, s, HS_KERNEL_TRSM);
         st = bsz == 256 ? tc_launch<256>(ctx, MODE_TRSM, w, a, m, s) : tc_launch<128>(ctx, MODE_TRSM, w, a, m, s);
         if (st != HS_OK) return st;

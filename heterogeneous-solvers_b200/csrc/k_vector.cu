@@ -234,11 +234,16 @@ __device__ __forceinline__ void block_apply(const double* M, int bsz, const doub
 template <int BSZ>
 __global__ void __launch_bounds__(kThreads) symv_partials(const double* __restrict__ A, const double* __restrict__ b,
                                                           double* __restrict__ P, int bsz, int nb, int bi0,
-                                                          int bj0, int nbi, int nbj) {
+                                                          int bj0, int nbi, int nbj, int full) {
     __shared__ double smem[(BSZ > 0 ? 8 * BSZ : 1)];
     const int64_t pos = blockIdx.x;
-    const int I = bi0 + (int)(pos / nbj);
-    const int J = bj0 + (int)(pos % nbj);
+    int I, J;
+    if (full) {
+        block_coords(pos, nb, &I, &J);  // CTA = stored block (I, J), J <= I
+    } else {
+        I = bi0 + (int)(pos / nbj);
+        J = bj0 + (int)(pos % nbj);
+    }
     const auto inRect = [&](int i, int j) { return i >= bi0 && i < bi0 + nbi && j >= bj0 && j < bj0 + nbj; };
     const size_t bb = (size_t)bsz * bsz;
     if (J <= I) {
@@ -528,26 +533,26 @@ hs_status launch_symv(hs_ctx ctx, const double* A, const double* b, double* resu
     if (st != HS_OK) return st;
     double* small = static_cast<double*>(ctx->scratch);
     double* P = reinterpret_cast<double*>(static_cast<char*>(ctx->scratch) + kSmallScratch);
-    // algorithmic bytes: every stored block the rectangle touches, read once, plus the vectors
-    int64_t stored = 0;
-    for (int I = bi0; I < bi0 + nbi; ++I) {
-        const int lo = bj0, hi = bj0 + nbj;  // J range
-        for (int J = lo; J < hi; ++J) {
-            const bool mirrored = J > I && J >= bi0 && J < bi0 + nbi && I >= bj0 && I < bj0 + nbj;
-            if (!mirrored) ++stored;
-        }
-    }
+    // algorithmic bytes: every stored block the rectangle touches, read once, plus the
+    // vectors; positions (I, J), J > I, whose mirror (J, I) is also in the rectangle
+    // reuse that block: c(c-1)/2 of them, c = the overlap of the row and column ranges
+    const int64_t ov_lo = bi0 > bj0 ? bi0 : bj0, ov_hi = (bi0 + nbi < bj0 + nbj) ? bi0 + nbi : bj0 + nbj;
+    const int64_t c_ov = ov_hi > ov_lo ? ov_hi - ov_lo : 0;
+    const int64_t stored = (int64_t)nbi * nbj - c_ov * (c_ov - 1) / 2;
+    // the whole matrix: one CTA per stored block instead of one per rectangle position
+    const bool full = bi0 == 0 && bj0 == 0 && nbi == ctx->nb && nbj == ctx->nb;
     const double bb = (double)bsz * bsz;
     prof_begin(ctx, s, HS_KERNEL_SYMV);
     if (nbj > 0) {
         ctx->launches += 1;
-        const int64_t grid = (int64_t)nbi * nbj;
+        const int64_t grid = full ? total_blocks(ctx->nb) : (int64_t)nbi * nbj;
+        const int fl = full ? 1 : 0;
         if (bsz == 256)
-            symv_partials<256><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
+            symv_partials<256><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj, fl);
         else if (bsz == 128)
-            symv_partials<128><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
+            symv_partials<128><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj, fl);
         else
-            symv_partials<0><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
+            symv_partials<0><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj, fl);
         HS_CHECK_LAUNCH("symv_partials");
     }
     const int64_t rows = (int64_t)nbi * bsz;
@@ -574,11 +579,11 @@ hs_status launch_symv_partials_at(hs_ctx ctx, const double* A, const double* b, 
         const int64_t grid = (int64_t)nbi * nbj;
         ctx->launches += 1;
         if (bsz == 256)
-            symv_partials<256><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
+            symv_partials<256><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj, 0);
         else if (bsz == 128)
-            symv_partials<128><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
+            symv_partials<128><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj, 0);
         else
-            symv_partials<0><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
+            symv_partials<0><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj, 0);
         HS_CHECK_LAUNCH("symv_partials");
     }
     const int64_t rows = (int64_t)nbi * bsz;

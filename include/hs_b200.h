@@ -61,7 +61,8 @@ hs_status hs_ctx_create(int device, void* stream, hs_ctx* out);
 hs_status hs_ctx_destroy(hs_ctx ctx);
 hs_status hs_ctx_set_stream(hs_ctx ctx, void* stream);
 /* The context keeps grow-only device buffers between calls (reduction partials,
- * matvec partial sums, solver work vectors, the mixed-precision and NLML workspaces);
+ * matvec partial sums, solver work vectors, the mixed-precision and NLML workspaces,
+ * the device copies of hs_gp_solve_host);
  * this frees them all (after synchronising the stream).  They are allocated
  * again by the next call that needs them.  No reference counterpart (the
  * reference's solvers free their device copies in their destructors,
@@ -226,7 +227,8 @@ hs_status hs_cg_solve(hs_ctx ctx, const double* A, const double* b, double* x, d
  * CG (algorithm 1: epsilon, iMax as in hs_cg_solve) or the mixed-precision solve
  * (algorithm 2, no reference counterpart: epsilon = backward-error target, iMax =
  * refinement step limit; report->factor_ms then covers factor and refinement) ->
- * x_host (N).  Device buffers are allocated inside. */
+ * x_host (N).  The device copies (X, the packed K, y, x) are kept by the context
+ * between calls; hs_ctx_release_buffers frees them. */
 typedef struct hs_solve_report {
     int64_t info;            /* factor: -1 or failing row */
     int64_t iterations;      /* CG iterations (algorithm 1) */
@@ -249,11 +251,12 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
  * continues with conjugate gradients preconditioned by the FP32 factor.  b and x
  * are device vectors of hs_padded_vector_size doubles.  The workspace (FP32
  * factor: half the packed matrix) is kept by the context between calls.  When
- * the FP32 factor of K meets a non-positive pivot (K too ill-conditioned for
- * FP32), K + shift*I is factored instead, shift = 1e-6, 1e-5, 1e-4 or 1e-3
- * times the largest diagonal entry, and the solve goes straight to CG
- * preconditioned by that factor (report->shift; report->logdet is then the
- * log-determinant of the shifted matrix).  Returns HS_ERR_REFINEMENT_STALLED
+ * the low-precision factor of K meets a non-positive pivot (K too ill-conditioned
+ * for it; the factorization stops at that block), a BF16-split factor is redone
+ * with 3xTF32 products, and then K + shift*I is factored with shift = 1e-6, 1e-5,
+ * ... 1e-1 times the largest diagonal entry, the solve going straight to CG
+ * preconditioned by that factor (report->shift, report->precision_used;
+ * report->logdet is then the log-determinant of the shifted matrix).  Returns HS_ERR_REFINEMENT_STALLED
  * when the target is not reached, HS_ERR_NOT_SPD when every shift fails. */
 typedef enum hs_precision {
     HS_PRECISION_FP64 = 0,
@@ -264,7 +267,9 @@ typedef struct hs_mixed_report {
     int64_t refinement_steps;
     int64_t pcg_iterations;
     int fallback_pcg;
-    int factor_attempts;     /* 1 unless the FP32 factor of K broke down and K + shift*I was factored */
+    int factor_attempts;     /* 1 unless the low-precision factor of K broke down and was redone */
+    int precision_used;      /* split products of the factor that was used (HS_PRECISION_*) */
+    int reserved;
     double shift;            /* diagonal shift of the low-precision factor (0: factor of K itself) */
     double backward_error;   /* ||b - K x|| / (||K||_F ||x||) at exit */
     double initial_backward_error; /* the same for x0 = (L L^T)^-1 b, before any refinement */

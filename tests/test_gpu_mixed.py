@@ -145,10 +145,35 @@ def test_mixed_factor_breakdown_falls_back_to_shifted_preconditioner(hs, ctx):
     xg = x.cpu().numpy()[:N]
     bwd = np.linalg.norm(y - Kd @ xg) / (np.linalg.norm(Kd, "fro") * np.linalg.norm(xg))
     assert bwd <= 2e-14
-    if rep["factor_attempts"] > 1:
-        assert rep["shift"] > 0 and rep["fallback_pcg"] == 1
+    if rep["shift"] > 0:
+        assert rep["factor_attempts"] > 1 and rep["fallback_pcg"] == 1
     else:
-        assert rep["shift"] == 0.0
+        assert rep["factor_attempts"] == 1
+
+
+def test_mixed_bf16_breakdown_falls_back_to_tf32(hs, ctx):
+    """A BF16-split factor that breaks down is redone with 3xTF32 products before
+    any diagonal shift is tried; the solve still reaches the target."""
+    N, bsz, d = 1024, 128, 4
+    rng = np.random.default_rng(12)
+    base = rng.random((N // 2, d))
+    X = np.concatenate([base, base])[rng.permutation(N)]
+    y = np.sin(X.sum(axis=1)) + 0.1 * rng.standard_normal(N)
+    ctx.set_problem(N, bsz)
+    A = hs.SymmetricMatrix(N, bsz, device="cuda:0")
+    hs.MatrixGenerator.assemble(ctx, A.matrixData, X, 0.5, 1.0, 1e-7)
+    b = torch.zeros(hs.padded_size(N, bsz), dtype=torch.float64, device="cuda:0")
+    b[:N] = torch.from_numpy(y)
+    solver = hs.MixedPrecisionSolver(A, ctx, "bf16x3")
+    x = solver.solve(b, tol=1e-14, max_steps=30)
+    rep = solver.report
+    print("bf16 breakdown case:", rep)
+    if rep["factor_attempts"] > 1:
+        assert rep["precision_used"] == hs.PRECISIONS["tf32x3"]
+    Kd = A.to_dense()
+    xg = x.cpu().numpy()[:N]
+    bwd = np.linalg.norm(y - Kd @ xg) / (np.linalg.norm(Kd, "fro") * np.linalg.norm(xg))
+    assert bwd <= 2e-14
 
 
 @pytest.mark.parametrize("N,bsz,sn2", [(1000, 128, 1e-2), (2048, 256, 1e-2), (700, 256, 1e-1)])
