@@ -13,7 +13,8 @@ comparison at equal error), with both backward errors.
 
 Prints one JSON line on rank 0.  `value` is whole-job throughput in solves/s
 (N independent replicas under torchrun: the path does not shard).  `e2e` is
-the same metric through hs_gp_solve_host (algorithm 2) with pinned host buffers.  The
+the same metric through hs_gp_solve_host (the mixed algorithm of the headline's
+split variant) with pinned host buffers.  The
 reference arm (--impl reference) times the CPU restatement of the reference's
 CPU path (or its sources compiled through oracle/ref_build.py when present) on
 a bounded sample and extrapolates by N^3.
@@ -525,7 +526,7 @@ def main():
         Xh = torch.from_numpy(X).pin_memory()
         yh = torch.from_numpy(y).pin_memory()
         xh = torch.empty(N, dtype=torch.float64).pin_memory()
-        kw = dict(algorithm="mixed", epsilon=args.tol, iMax=30, out=xh)
+        kw = dict(algorithm=f"mixed_{args.precision}", epsilon=args.tol, iMax=30, out=xh)
         hs.gp_solve_host(ctx, Xh, yh, cfg["lengthscale"], cfg["sf2"], cfg["sn2"], **kw)  # warm-up
         if world > 1:
             dist.barrier()

@@ -704,6 +704,28 @@ class MatrixParser:
         return A
 
     @staticmethod
+    def writeFullMatrix(path, matrix):
+        """MatrixParser.cpp:214-274: every row of the padded matrix, the stored
+        blocks left of and on the diagonal read row-wise and the blocks right of
+        it read transposed, each value with 20 fixed decimals followed by ';'
+        (non-negative values preceded by a space), one line per row."""
+        b, nb = matrix.blockSize, matrix.blockCountXY
+        data = matrix.matrixData.detach().cpu().numpy()
+        with open(path, "w") as out:
+            for row in range(nb * b):
+                rb, ri = divmod(row, b)
+                parts = []
+                for cb in range(nb):
+                    if cb <= rb:
+                        s0 = block_id(rb, cb, nb) * b * b
+                        vals = data[s0 + ri * b:s0 + (ri + 1) * b]
+                    else:
+                        s0 = block_id(cb, rb, nb) * b * b
+                        vals = data[s0 + ri:s0 + b * b:b]
+                    parts.extend((" " if v >= 0 else "") + f"{v:.20f};" for v in vals)
+                out.write("".join(parts) + "\n")
+
+    @staticmethod
     def parseRightHandSide(path, matrixBlockSize):
         """`# N` then one line `v; v; ...` (MatrixParser.cpp:43-72)."""
         N, lines = MatrixParser._rows(Path(path).read_text())
@@ -714,15 +736,16 @@ class MatrixParser:
 
 
 # hs_gp_solve_host algorithms
-_ALGORITHMS = {"cholesky": 0, "cg": 1, "mixed": 2}
+_ALGORITHMS = {"cholesky": 0, "cg": 1, "mixed": 2, "mixed_tf32x3": 2, "mixed_bf16x3": 3}
 
 
 def gp_solve_host(ctx, X, y, lengthscale=1.0, signal_variance=1.0, noise_variance=0.01, algorithm="cholesky",
                   epsilon=1e-10, iMax=100000, out=None):
     """End-to-end GP solve through host buffers (hs_gp_solve_host): host X
     (N x d) and y (N) in, host x = K^-1 y out, plus the phase report.
-    ``algorithm`` is "cholesky", "cg" or "mixed" (for "mixed", ``epsilon`` is
-    the backward-error target and ``iMax`` the refinement step limit).  X, y
+    ``algorithm`` is "cholesky", "cg", "mixed" / "mixed_tf32x3" or "mixed_bf16x3"
+    (for the mixed forms, ``epsilon`` is the backward-error target and ``iMax``
+    the refinement step limit).  X, y
     and ``out`` may be CPU torch tensors (pinned memory gives asynchronous
     copies) or numpy arrays."""
 

@@ -234,16 +234,11 @@ __device__ __forceinline__ void block_apply(const double* M, int bsz, const doub
 template <int BSZ>
 __global__ void __launch_bounds__(kThreads) symv_partials(const double* __restrict__ A, const double* __restrict__ b,
                                                           double* __restrict__ P, int bsz, int nb, int bi0,
-                                                          int bj0, int nbi, int nbj, int full) {
+                                                          int bj0, int nbi, int nbj) {
     __shared__ double smem[(BSZ > 0 ? 8 * BSZ : 1)];
     const int64_t pos = blockIdx.x;
-    int I, J;
-    if (full) {
-        block_coords(pos, nb, &I, &J);  // CTA = stored block (I, J), J <= I
-    } else {
-        I = bi0 + (int)(pos / nbj);
-        J = bj0 + (int)(pos % nbj);
-    }
+    const int I = bi0 + (int)(pos / nbj);
+    const int J = bj0 + (int)(pos % nbj);
     const auto inRect = [&](int i, int j) { return i >= bi0 && i < bi0 + nbi && j >= bj0 && j < bj0 + nbj; };
     const size_t bb = (size_t)bsz * bsz;
     if (J <= I) {
@@ -539,20 +534,20 @@ hs_status launch_symv(hs_ctx ctx, const double* A, const double* b, double* resu
     const int64_t ov_lo = bi0 > bj0 ? bi0 : bj0, ov_hi = (bi0 + nbi < bj0 + nbj) ? bi0 + nbi : bj0 + nbj;
     const int64_t c_ov = ov_hi > ov_lo ? ov_hi - ov_lo : 0;
     const int64_t stored = (int64_t)nbi * nbj - c_ov * (c_ov - 1) / 2;
-    // the whole matrix: one CTA per stored block instead of one per rectangle position
-    const bool full = bi0 == 0 && bj0 == 0 && nbi == ctx->nb && nbj == ctx->nb;
     const double bb = (double)bsz * bsz;
     prof_begin(ctx, s, HS_KERNEL_SYMV);
     if (nbj > 0) {
         ctx->launches += 1;
-        const int64_t grid = full ? total_blocks(ctx->nb) : (int64_t)nbi * nbj;
-        const int fl = full ? 1 : 0;
+        // one CTA per rectangle position (I, J), row-major; positions whose block is
+        // handled through its mirror exit at once.  Measured faster than one CTA per
+        // stored block in storage order (5.2 vs 4.95 TB/s at N=131072).
+        const int64_t grid = (int64_t)nbi * nbj;
         if (bsz == 256)
-            symv_partials<256><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj, fl);
+            symv_partials<256><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
         else if (bsz == 128)
-            symv_partials<128><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj, fl);
+            symv_partials<128><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
         else
-            symv_partials<0><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj, fl);
+            symv_partials<0><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
         HS_CHECK_LAUNCH("symv_partials");
     }
     const int64_t rows = (int64_t)nbi * bsz;
@@ -579,11 +574,11 @@ hs_status launch_symv_partials_at(hs_ctx ctx, const double* A, const double* b, 
         const int64_t grid = (int64_t)nbi * nbj;
         ctx->launches += 1;
         if (bsz == 256)
-            symv_partials<256><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj, 0);
+            symv_partials<256><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
         else if (bsz == 128)
-            symv_partials<128><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj, 0);
+            symv_partials<128><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
         else
-            symv_partials<0><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj, 0);
+            symv_partials<0><<<(unsigned)grid, kThreads, 0, s>>>(A, b, P, bsz, ctx->nb, bi0, bj0, nbi, nbj);
         HS_CHECK_LAUNCH("symv_partials");
     }
     const int64_t rows = (int64_t)nbi * bsz;

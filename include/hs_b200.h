@@ -225,8 +225,9 @@ hs_status hs_cg_solve(hs_ctx ctx, const double* A, const double* b, double* x, d
  * solve (src/gaussianProcess/GaussianProcess.cpp:20-40) and main.cpp:201-249:
  * X_host (N x d), y_host (N) -> RBF assembly -> factor + solve (algorithm 0),
  * CG (algorithm 1: epsilon, iMax as in hs_cg_solve) or the mixed-precision solve
- * (algorithm 2, no reference counterpart: epsilon = backward-error target, iMax =
- * refinement step limit; report->factor_ms then covers factor and refinement) ->
+ * (no reference counterpart: algorithm 2 with 3xTF32, 3 with BF16-split updates;
+ * epsilon = backward-error target, iMax = refinement step limit;
+ * report->factor_ms then covers factor and refinement) ->
  * x_host (N).  The device copies (X, the packed K, y, x) are kept by the context
  * between calls; hs_ctx_release_buffers frees them. */
 typedef struct hs_solve_report {
