@@ -144,14 +144,16 @@ int grid_n(int64_t n, int sms) {
 }  // namespace
 
 // b <- (L L^T)^-1 b with the mixed factor: FP32 off-diagonal blocks, FP64
-// inverse diagonal blocks; one launch per block column and direction
-hs_status mixed_apply(hs_ctx ctx, const MixedWork& w, double* b, cudaStream_t s) {
+// inverse diagonal blocks; one launch per block column and direction.  The
+// forward sweep reduces b in place and writes L^-1 b into tmp; the backward
+// sweep reduces tmp in place and writes the result into b.
+hs_status mixed_apply(hs_ctx ctx, const MixedWork& w, double* b, double* tmp, cudaStream_t s) {
     const int nb = ctx->nb;
     hs_status st;
     for (int j = -1; j < nb - 1; ++j)
-        if ((st = launch_mixed_sweep(ctx, w.A32, w.Yinv, b, j, 1, s)) != HS_OK) return st;
+        if ((st = launch_mixed_sweep(ctx, w.A32, w.Yinv, b, tmp, j, 1, s)) != HS_OK) return st;
     for (int j = nb; j >= 1; --j)
-        if ((st = launch_mixed_sweep(ctx, w.A32, w.Yinv, b, j, 0, s)) != HS_OK) return st;
+        if ((st = launch_mixed_sweep(ctx, w.A32, w.Yinv, tmp, b, j, 0, s)) != HS_OK) return st;
     return HS_OK;
 }
 
@@ -181,15 +183,16 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     const auto t0 = std::chrono::steady_clock::now();
     hs_mixed_report& R = *out;
     R = hs_mixed_report{};
-    // workspace (kept by the context): factor + 5 vectors
+    // workspace (kept by the context): factor + 6 vectors
     const size_t fbytes = (mixed_workspace_bytes(ctx->N, bsz) + 255) & ~size_t(255);
-    hs_status st = ensure_mixed(ctx, fbytes + (size_t)5 * n * sizeof(double));
+    hs_status st = ensure_mixed(ctx, fbytes + (size_t)6 * n * sizeof(double));
     if (st != HS_OK) return st;
     double* r = reinterpret_cast<double*>(static_cast<char*>(ctx->mixed) + fbytes);
     double* d = r + n;
     double* p = d + n;
     double* q = p + n;
     double* z = q + n;
+    double* tmp = z + n;  // triangular-sweep intermediate
     MixedWork w;
     st = mixed_bind(ctx, ctx->mixed, &w);
     if (st != HS_OK) return st;
@@ -277,7 +280,7 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     };
     // x0 = M^-1 b
     HS_CUDA(cudaMemcpyAsync(x, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    st = mixed_apply(ctx, w, x, s);
+    st = mixed_apply(ctx, w, x, tmp, s);
     if (st != HS_OK) return st;
     double rn = 0, xn = 0, prev = INFINITY;
     bool converged = false;
@@ -299,7 +302,7 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
         prev = rn;
         // d = M^-1 r; x += d
         HS_CUDA(cudaMemcpyAsync(d, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-        st = mixed_apply(ctx, w, d, s);
+        st = mixed_apply(ctx, w, d, tmp, s);
         if (st != HS_OK) return st;
         ctx->launches += 1;
         add_kernel<<<g, kThreads, 0, s>>>(x, d, n);
@@ -313,7 +316,7 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
         if (st != HS_OK) return st;
         if (steps == 0) R.initial_backward_error = rn / (R.norm_k_fro * xn);
         HS_CUDA(cudaMemcpyAsync(z, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-        st = mixed_apply(ctx, w, z, s);
+        st = mixed_apply(ctx, w, z, tmp, s);
         if (st != HS_OK) return st;
         HS_CUDA(cudaMemcpyAsync(p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         st = launch_dot(ctx, r, z, scal + 6, 0, n, s);
@@ -355,7 +358,7 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
                 }
             }
             HS_CUDA(cudaMemcpyAsync(z, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-            if ((st = mixed_apply(ctx, w, z, s)) != HS_OK) return st;
+            if ((st = mixed_apply(ctx, w, z, tmp, s)) != HS_OK) return st;
             if ((st = launch_dot(ctx, r, z, scal + 6, 0, n, s)) != HS_OK) return st;
             HS_CUDA(cudaMemcpyAsync((void*)(h + 12), scal + 6, sizeof(double), cudaMemcpyDeviceToHost, s));
             HS_CUDA(cudaStreamSynchronize(s));

@@ -38,8 +38,8 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
 // lower triangle L (bsz x bsz): B <- B L^-T
 hs_status launch_trsm_on(hs_ctx ctx, const double* L, int n, double* B, int items, cudaStream_t s);
 // one launch of a forward / backward sweep with the mixed factor (k_vector.cu)
-hs_status launch_mixed_sweep(hs_ctx ctx, const float* A32, const double* Y, double* b, int j, int forward,
-                             cudaStream_t s);
+hs_status launch_mixed_sweep(hs_ctx ctx, const float* A32, const double* Y, double* work, double* out, int j,
+                             int forward, cudaStream_t s);
 // column update reading FP32 blocks (accumulation in FP64)
 hs_status launch_column_update_f32(hs_ctx ctx, const float* A32, double* b, int blockStart, int blockCount,
                                    int blockRow, int blockID, int transposed, cudaStream_t s);
