@@ -41,15 +41,26 @@ enum { MODE_UPDATE = 0, MODE_TRSM = 1 };
 
 struct TcArgs {
     float* A32;        // packed FP32 working matrix
-    float* LO;         // low parts: panel blocks 0..m-1, slot nb = L_kk^-T hi, nb+1 = lo
+    float* LO;         // FP32 low parts of panel blocks and of L_kk^-T (slots below)
     int64_t blockID;   // id of the diagonal block of column k
     int k, nb;
     int64_t gemmPairs, pairBase;  // MODE_UPDATE: GEMM pairs c < r, rows k+2..
     int syrkStart;
     int64_t totalPairs;
     int* err;          // error flag (timeouts)
-    int part;          // persistent update: 0 all of columns k+1.., 1 column k+1 only, 2 columns k+2..
+    int part;          // persistent update: 0 columns first_col.., 1 column first_col only, 2 columns first_col+1..
     const long long* abort_flag;  // smallest failing pivot row so far (INT64_MAX: none)
+    // slots (bsz x bsz blocks): FP32 low parts of panel k in LO from lo_base (row r at
+    // lo_base + r - k - 1), L_kk^-1 hi / lo at LO[inv], LO[inv + 1]
+    int lo_base, inv;
+    // persistent update over npanels consecutive panel columns k, k+1 (npanels 1 or 2),
+    // updating the trailing columns from first_col on; panel k+1's diagonal block id,
+    // its FP32 low-part base, and the BF16 split bases of both panels (hi of row r of
+    // panel p at base_p + r - (k + p) - 1, lo at that slot + nb)
+    int npanels;
+    int64_t blockID2;
+    int lo_base2, p16_base, p16_base2;
+    int first_col;
 };
 
 // CTA-uniform early exit once a diagonal POTRF has recorded a non-positive pivot:
@@ -106,9 +117,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     // operand coordinates: (column, row, block) in the TMA maps
     const int blkA = (int)(a.blockID + (r - a.k));  // panel block of row r
-    const int gA = r - a.k - 1;                     // its low-part slot
-    const int blkB = (MODE == MODE_TRSM) ? a.nb : (int)(a.blockID + (c - a.k));
-    const int gB = (MODE == MODE_TRSM) ? a.nb + 1 : c - a.k - 1;
+    const int gA = a.lo_base + r - a.k - 1;         // its low-part slot
+    const int blkB = (MODE == MODE_TRSM) ? a.inv : (int)(a.blockID + (c - a.k));
+    const int gB = (MODE == MODE_TRSM) ? a.inv + 1 : a.lo_base + c - a.k - 1;
 
     if (tid == 0) {
         for (int s = 0; s < SM::kStages; ++s) {
@@ -319,7 +330,8 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     using F = UpdFmt<PREC>;
     if (factor_aborted(a.abort_flag)) return;
     constexpr int kTiles = BSZ / 128;
-    constexpr int kSlabs = BSZ / F::kK;
+    constexpr int kSlabsP = BSZ / F::kK;  // slabs per panel
+    const int kSlabs = a.npanels * kSlabsP;
     constexpr uint32_t kAccCols = 2 * BSZ;  // two accumulators
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -331,9 +343,9 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     uint32_t* tslot = reinterpret_cast<uint32_t*>(tempty + 2);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m = a.nb - a.k - 1;
-    // part 1: the m blocks of column k+1; part 2: the lower triangle of columns k+2..;
-    // part 0: both (the m x m lower triangle of columns k+1..)
+    const int m = a.nb - a.first_col;
+    // part 1: the m blocks of column first_col; part 2: the lower triangle of the
+    // columns after it; part 0: both (the m x m lower triangle from first_col on)
     const int mt = a.part == 2 ? m - 1 : m;
     const int64_t ntiles = (a.part == 1 ? (int64_t)m : tri64(mt)) * kTiles;
 
@@ -362,13 +374,13 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         *ti = (int)(t % kTiles);
         const int64_t p = t / kTiles;
         if (a.part == 1) {
-            *r = a.k + 1 + (int)p;
-            *c = a.k + 1;
+            *r = a.first_col + (int)p;
+            *c = a.first_col;
             return;
         }
         int rr, cc;
         grouped_pair(p, mt, &rr, &cc);
-        const int base = a.k + (a.part == 2 ? 2 : 1);
+        const int base = a.first_col + (a.part == 2 ? 1 : 0);
         *r = base + rr;
         *c = base + cc;
     };
@@ -380,24 +392,30 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
                 int r, c, ti;
                 decode(t, &r, &c, &ti);
-                // TF32: hi = the FP32 panel block in A32, lo = its slot in LO;
-                // BF16: hi and lo are slots g and nb + g of the BF16 panel
-                const int gA = r - a.k - 1, gB = c - a.k - 1;
                 const bool bf = PREC == HS_PRECISION_BF16X3;
-                const int hiA = bf ? gA : (int)(a.blockID + (r - a.k)), loA = bf ? a.nb + gA : gA;
-                const int hiB = bf ? gB : (int)(a.blockID + (c - a.k)), loB = bf ? a.nb + gB : gB;
                 for (int kc = 0; kc < kSlabs; ++kc, ++g) {
                     const uint32_t s = g % SM::kStages, use = g / SM::kStages;
                     if (use > 0 && !mbar_wait_for(&empty[s], (use - 1) & 1, kStepWaitNs)) {
                         ok = false;
                         break;
                     }
+                    // panel pi = column k + pi: TF32 hi = its FP32 block in A32, lo = its
+                    // LO slot; BF16 hi / lo = its split slots in P16
+                    const int pi = kc / kSlabsP, kk = kc % kSlabsP;
+                    const int colp = a.k + pi;
+                    const int gA = r - colp - 1, gB = c - colp - 1;
+                    const int64_t dblk = pi ? a.blockID2 : a.blockID;
+                    const int lob = pi ? a.lo_base2 : a.lo_base, pb = pi ? a.p16_base2 : a.p16_base;
+                    const int hiA = bf ? pb + gA : (int)(dblk + (r - colp));
+                    const int loA = bf ? pb + a.nb + gA : lob + gA;
+                    const int hiB = bf ? pb + gB : (int)(dblk + (c - colp));
+                    const int loB = bf ? pb + a.nb + gB : lob + gB;
                     uint8_t* st = smem + s * SM::kStage;
                     mbar_arrive_expect_tx(&full[s], SM::kStage);
-                    tma_load_3d(st, &mU128, &full[s], kc * F::kK, ti * 128, hiA);
-                    tma_load_3d(st + SM::kA, &mUB, &full[s], kc * F::kK, 0, hiB);
-                    tma_load_3d(st + SM::kRaw, &mV128, &full[s], kc * F::kK, ti * 128, loA);
-                    tma_load_3d(st + SM::kRaw + SM::kA, &mVB, &full[s], kc * F::kK, 0, loB);
+                    tma_load_3d(st, &mU128, &full[s], kk * F::kK, ti * 128, hiA);
+                    tma_load_3d(st + SM::kA, &mUB, &full[s], kk * F::kK, 0, hiB);
+                    tma_load_3d(st + SM::kRaw, &mV128, &full[s], kk * F::kK, ti * 128, loA);
+                    tma_load_3d(st + SM::kRaw + SM::kA, &mVB, &full[s], kk * F::kK, 0, loB);
                 }
             }
             if (!ok) atomicExch(a.err, 1);
@@ -556,7 +574,7 @@ __global__ void diag_in_kernel(const float* __restrict__ blk, double* __restrict
 }
 
 // after POTRF(S) and Y = I L^-T (= (L^-1)^T): A32 diagonal block = float(L),
-// Ldiag64[k] = L, LO[nb] = hi of L^-1 (row-major, i.e. Y transposed), LO[nb+1] = lo
+// Ldiag64[k] = L, invHi = hi of L^-1 (row-major, i.e. Y transposed), invLo = lo
 __global__ void diag_out_kernel(const double* __restrict__ S, const double* __restrict__ Y, float* __restrict__ blk,
                                 double* __restrict__ Ld, float* __restrict__ invHi, float* __restrict__ invLo,
                                 int bsz) {
@@ -628,7 +646,7 @@ template <int BSZ>
 hs_status tc_update_launch(hs_ctx ctx, const MixedWork& w, const TcArgs& a, int precision, cudaStream_t s,
                            int max_ctas) {
     using SM = UpdSmem<BSZ>;
-    const int m = a.nb - a.k - 1;
+    const int m = a.nb - a.first_col;
     const int64_t ntiles = (a.part == 1 ? (int64_t)m : tri64(a.part == 2 ? m - 1 : m)) * (BSZ / 128);
     if (ntiles <= 0) return HS_OK;
     const int grid = (int)(ntiles < max_ctas ? ntiles : max_ctas);
@@ -677,10 +695,10 @@ size_t mixed_workspace_bytes(int64_t N, int bsz) {
     const size_t T = (size_t)(nb * (nb + 1) / 2);
     size_t bytes = 0;
     bytes += T * bb * 4;                 // A32 / L32
-    bytes += (size_t)(nb + 2) * bb * 4;  // LO
+    bytes += (size_t)(2 * nb + 2) * bb * 4;  // LO: two panels' low parts + L_kk^-1 hi / lo
     bytes += (size_t)nb * bb * 8;        // Ldiag64
     bytes += (size_t)nb * bb * 8;        // Yinv
-    bytes += (size_t)2 * nb * bb * 2;    // BF16 panel hi / lo
+    bytes += (size_t)4 * nb * bb * 2;    // BF16 split of two panels (hi / lo each)
     bytes += bb * 8;                     // S
     bytes += 1024;                       // flags
     return bytes;
@@ -694,27 +712,27 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
     w->A32 = reinterpret_cast<float*>(p);
     p += T * bb * 4;
     w->LO = reinterpret_cast<float*>(p);
-    p += (size_t)(nb + 2) * bb * 4;
+    p += (size_t)(2 * nb + 2) * bb * 4;
     w->Ld = reinterpret_cast<double*>(p);
     p += (size_t)nb * bb * 8;
     w->Yinv = reinterpret_cast<double*>(p);
     p += (size_t)nb * bb * 8;
     w->P16 = reinterpret_cast<__nv_bfloat16*>(p);
-    p += (size_t)2 * nb * bb * 2;
+    p += (size_t)4 * nb * bb * 2;
     w->S = reinterpret_cast<double*>(p);
     p += bb * 8;
     w->err = reinterpret_cast<int*>(p);
     hs_status st = make_map(&w->mA128, w->A32, bsz, (int64_t)T, 128);
     if (st == HS_OK) st = make_map(&w->mAB, w->A32, bsz, (int64_t)T, bsz);
-    if (st == HS_OK) st = make_map(&w->mL128, w->LO, bsz, nb + 2, 128);
-    if (st == HS_OK) st = make_map(&w->mLB, w->LO, bsz, nb + 2, bsz);
+    if (st == HS_OK) st = make_map(&w->mL128, w->LO, bsz, 2 * nb + 2, 128);
+    if (st == HS_OK) st = make_map(&w->mLB, w->LO, bsz, 2 * nb + 2, bsz);
     if (st == HS_OK) st = make_map(&w->mU128, w->A32, bsz, (int64_t)T, 128, kUpdK);
     if (st == HS_OK) st = make_map(&w->mUB, w->A32, bsz, (int64_t)T, bsz, kUpdK);
-    if (st == HS_OK) st = make_map(&w->mV128, w->LO, bsz, nb + 2, 128, kUpdK);
-    if (st == HS_OK) st = make_map(&w->mVB, w->LO, bsz, nb + 2, bsz, kUpdK);
+    if (st == HS_OK) st = make_map(&w->mV128, w->LO, bsz, 2 * nb + 2, 128, kUpdK);
+    if (st == HS_OK) st = make_map(&w->mVB, w->LO, bsz, 2 * nb + 2, bsz, kUpdK);
     if (st == HS_OK) st = make_map(&w->mC32, w->A32, bsz, (int64_t)T, 32, 32);
-    if (st == HS_OK) st = make_map(&w->mP128, w->P16, bsz, 2 * (int64_t)nb, 128, 2 * kUpdK, 2);
-    if (st == HS_OK) st = make_map(&w->mPB, w->P16, bsz, 2 * (int64_t)nb, bsz, 2 * kUpdK, 2);
+    if (st == HS_OK) st = make_map(&w->mP128, w->P16, bsz, 4 * (int64_t)nb, 128, 2 * kUpdK, 2);
+    if (st == HS_OK) st = make_map(&w->mPB, w->P16, bsz, 4 * (int64_t)nb, bsz, 2 * kUpdK, 2);
     return st;
 }
 
@@ -748,77 +766,104 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         r = launch_trsm_on(ctx, w.S, bsz, Yk, 1, st_);
         if (r != HS_OK) return r;
         ctx->launches += 1;
-        diag_out_kernel<<<64, 256, 0, st_>>>(w.S, Yk, dblk, w.Ld + (size_t)k * bb, w.LO + (size_t)nb * bb,
-                                             w.LO + (size_t)(nb + 1) * bb, bsz);
+        diag_out_kernel<<<64, 256, 0, st_>>>(w.S, Yk, dblk, w.Ld + (size_t)k * bb, w.LO + (size_t)2 * nb * bb,
+                                             w.LO + (size_t)(2 * nb + 1) * bb, bsz);
         HS_CHECK_LAUNCH("mixed diag");
         return HS_OK;
     };
-    // Lookahead: the update of column k runs in two launches, column k+1 first; the
-    // diagonal chain of block k+1 then runs on the side stream, on SMs the second
-    // (larger) launch leaves free, while that launch updates columns k+2..
+    // Panels are factored in pairs (k, k+1) and the columns after them are updated with
+    // both at once (K = 2 bsz per pass over C), which halves the read-modify-write
+    // traffic on the trailing matrix.  Panel k of a pair keeps its low parts in slot
+    // set 0, panel k+1 in set 1.  Lookahead: the update of columns k+2.. runs in two
+    // launches, column k+2 first; the diagonal chain of block k+2 then runs on the side
+    // stream, on SMs the second (larger) launch leaves free.
     const bool lookahead = ctx->side != nullptr && ctx->num_sms > 8;
     const int kFree = 2;
-    if ((st = diag_chain(0, s)) != HS_OK) return st;
     const double n3 = (double)bsz * bb;
-    for (int k = 0; k < nb - 1; ++k) {
-        const int right = nb - k;
-        const int64_t blockID = T - (int64_t)right * (right + 1) / 2;
+    auto diag_id = [&](int k) { return T - (int64_t)(nb - k) * (nb - k + 1) / 2; };
+    TcArgs base{};
+    base.A32 = w.A32;
+    base.LO = w.LO;
+    base.nb = nb;
+    base.err = w.err;
+    base.abort_flag = ctx->d_info;
+    base.inv = 2 * nb;
+    base.lo_base2 = nb;
+    base.p16_base2 = 2 * nb;
+    // blocks k+1..nb-1 of column k: FP32 low parts into set `set`, TRSM-as-GEMM with
+    // L_kk^-T (writes L and its low part), and for BF16 the split of L into P16
+    auto panel = [&](int k, int set) -> hs_status {
+        const int64_t blockID = diag_id(k);
         float* dblk = w.A32 + (size_t)blockID * bb;
         const int m = nb - k - 1;
-        // low parts of the raw panel, TRSM-as-GEMM with L^-T (writes L and its low part)
         ctx->launches += 1;
-        lo_part_kernel<<<grid_for_elems((int64_t)m * bb / 4, ctx->num_sms), 256, 0, s>>>(dblk + bb, w.LO,
-                                                                                          (int64_t)m * bb / 4);
+        lo_part_kernel<<<grid_for_elems((int64_t)m * bb / 4, ctx->num_sms), 256, 0, s>>>(
+            dblk + bb, w.LO + (size_t)set * nb * bb, (int64_t)m * bb / 4);
         HS_CHECK_LAUNCH("lo_part");
-        TcArgs a{};
-        a.A32 = w.A32;
-        a.LO = w.LO;
+        TcArgs a = base;
         a.blockID = blockID;
         a.k = k;
-        a.nb = nb;
-        a.err = w.err;
-        a.abort_flag = ctx->d_info;
+        a.lo_base = set * nb;
         prof_begin(ctx, s, HS_KERNEL_TRSM);
-        st = bsz == 256 ? tc_launch<256>(ctx, MODE_TRSM, w, a, m, s) : tc_launch<128>(ctx, MODE_TRSM, w, a, m, s);
-        if (st != HS_OK) return st;
+        hs_status r = bsz == 256 ? tc_launch<256>(ctx, MODE_TRSM, w, a, m, s) : tc_launch<128>(ctx, MODE_TRSM, w, a, m, s);
+        if (r != HS_OK) return r;
         prof_end(ctx, s, HS_KERNEL_TRSM, (double)m * 2.0 * bsz * bb, 4.0 * m * bb * 4.0);
         if (precision == HS_PRECISION_BF16X3) {
-            // BF16 hi / lo copies of the factored panel (blocks k+1..nb-1 of column k)
             ctx->launches += 1;
             panel_split_bf16_kernel<<<grid_for_elems((int64_t)m * bb / 2, ctx->num_sms), 256, 0, s>>>(
-                dblk + bb, w.P16, (int64_t)m * bb, (int64_t)nb * bb);
+                dblk + bb, w.P16 + (size_t)2 * set * nb * bb, (int64_t)m * bb, (int64_t)nb * bb);
             HS_CHECK_LAUNCH("panel_split_bf16");
         }
-        // trailing update, part 1: column k+1 (m - 1 GEMM blocks + the SYRK block k+1)
-        a.part = 1;
+        return HS_OK;
+    };
+    // trailing update with panels k (.. k + npanels - 1): part 1 = column c0, part 2 =
+    // the columns after it
+    auto update = [&](int k, int npanels, int c0, int part, int cap) -> hs_status {
+        TcArgs a = base;
+        a.k = k;
+        a.blockID = diag_id(k);
+        a.npanels = npanels;
+        a.blockID2 = npanels > 1 ? diag_id(k + 1) : 0;
+        a.first_col = c0;
+        a.part = part;
+        const double m = nb - c0, np = npanels;
+        double flops, bytes;
+        if (part == 1) {
+            flops = np * ((m - 1.0) * 2.0 * n3 + (double)bsz * bsz * (bsz + 1.0));
+            bytes = (m * 2.0 + 2.0 * np * (m + 1.0)) * bb * 4.0;
+        } else {
+            const double gp = (m - 1.0) * (m - 2.0) / 2.0;
+            flops = np * (gp * 2.0 * n3 + (m - 1.0) * bsz * bsz * (bsz + 1.0));
+            bytes = ((gp + m - 1.0) * 2.0 + 2.0 * np * m) * bb * 4.0;
+        }
         prof_begin(ctx, s, HS_KERNEL_UPDATE);
-        st = bsz == 256 ? tc_update_launch<256>(ctx, w, a, precision, s, ctx->num_sms)
-                        : tc_update_launch<128>(ctx, w, a, precision, s, ctx->num_sms);
-        if (st != HS_OK) return st;
-        prof_end(ctx, s, HS_KERNEL_UPDATE, (m - 1.0) * 2.0 * n3 + (double)bsz * bsz * (bsz + 1.0),
-                 ((m - 1.0) * 2.0 + 2.0 + 2.0 * m) * bb * 4.0);
-        const bool side = lookahead && m >= 2;
+        hs_status r = bsz == 256 ? tc_update_launch<256>(ctx, w, a, precision, s, cap)
+                                 : tc_update_launch<128>(ctx, w, a, precision, s, cap);
+        if (r != HS_OK) return r;
+        prof_end(ctx, s, HS_KERNEL_UPDATE, flops, bytes);
+        return HS_OK;
+    };
+    if ((st = diag_chain(0, s)) != HS_OK) return st;
+    for (int k = 0; k < nb - 1; k += 2) {
+        // precondition: column k is fully updated and its diagonal block factored
+        if ((st = panel(k, 0)) != HS_OK) return st;
+        if ((st = update(k, 1, k + 1, 1, ctx->num_sms)) != HS_OK) return st;  // column k+1
+        if ((st = diag_chain(k + 1, s)) != HS_OK) return st;
+        if (k + 1 == nb - 1) break;
+        if ((st = panel(k + 1, 1)) != HS_OK) return st;
+        if ((st = update(k, 2, k + 2, 1, ctx->num_sms)) != HS_OK) return st;  // column k+2
+        const bool more = k + 3 < nb;  // columns after k+2
+        const bool side = lookahead && more;
         if (side) {
             HS_CUDA(cudaEventRecord(ctx->ev_a, s));
             HS_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_a, 0));
-            if ((st = diag_chain(k + 1, ctx->side)) != HS_OK) return st;
+            if ((st = diag_chain(k + 2, ctx->side)) != HS_OK) return st;
             HS_CUDA(cudaEventRecord(ctx->ev_b, ctx->side));
         }
-        // part 2: columns k+2.. (the (m-1) x (m-1) lower triangle)
-        if (m >= 2) {
-            a.part = 2;
-            const double gp = (m - 1.0) * (m - 2.0) / 2.0;
-            prof_begin(ctx, s, HS_KERNEL_UPDATE);
-            const int cap = side ? ctx->num_sms - kFree : ctx->num_sms;
-            st = bsz == 256 ? tc_update_launch<256>(ctx, w, a, precision, s, cap)
-                            : tc_update_launch<128>(ctx, w, a, precision, s, cap);
-            if (st != HS_OK) return st;
-            prof_end(ctx, s, HS_KERNEL_UPDATE, gp * 2.0 * n3 + (m - 1.0) * bsz * bsz * (bsz + 1.0),
-                     ((gp + m - 1.0) * 2.0 + 2.0 * m) * bb * 4.0);
-        }
+        if (more && (st = update(k, 2, k + 2, 2, side ? ctx->num_sms - kFree : ctx->num_sms)) != HS_OK) return st;
         if (side) {
             HS_CUDA(cudaStreamWaitEvent(s, ctx->ev_b, 0));
-        } else if ((st = diag_chain(k + 1, s)) != HS_OK) {
+        } else if ((st = diag_chain(k + 2, s)) != HS_OK) {
             return st;
         }
     }
