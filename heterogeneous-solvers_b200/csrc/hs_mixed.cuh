@@ -12,11 +12,11 @@ namespace hs {
 // device workspace of one mixed-precision factorization
 struct MixedWork {
     float* A32 = nullptr;   // packed FP32 copy of K, overwritten by L (off-diagonal blocks used by the solves)
-    float* LO = nullptr;    // low parts of two panels (slots 0..nb-1, nb..2nb-1), 2nb / 2nb+1 = L_kk^-1 hi / lo
+    float* LO = nullptr;    // low parts of a panel group (panel p: slots p nb..), then L_kk^-1 hi / lo
     double* Ld = nullptr;   // FP64 diagonal blocks of L (nb blocks)
     double* Yinv = nullptr; // FP64 inverse diagonal blocks, Y_k = L_kk^-T (nb blocks)
     double* S = nullptr;    // FP64 scratch block (POTRF)
-    __nv_bfloat16* P16 = nullptr;  // BF16 split of two panels: panel p hi blocks 2p nb.., lo blocks (2p+1) nb..
+    __nv_bfloat16* P16 = nullptr;  // BF16 split of a panel group: panel p hi blocks 2p nb.., lo (2p+1) nb..
     int* err = nullptr;     // tensor-core tile timeout flag
     CUtensorMap mA128, mAB, mL128, mLB;  // 128-byte swizzle, 32-wide K boxes (TRSM)
     CUtensorMap mU128, mUB, mV128, mVB;  // K boxes of 128 bytes over A32 / LO (TF32 update)

@@ -53,13 +53,11 @@ struct TcArgs {
     // slots (bsz x bsz blocks): FP32 low parts of panel k in LO from lo_base (row r at
     // lo_base + r - k - 1), L_kk^-1 hi / lo at LO[inv], LO[inv + 1]
     int lo_base, inv;
-    // persistent update over npanels consecutive panel columns k, k+1 (npanels 1 or 2),
-    // updating the trailing columns from first_col on; panel k+1's diagonal block id,
-    // its FP32 low-part base, and the BF16 split bases of both panels (hi of row r of
-    // panel p at base_p + r - (k + p) - 1, lo at that slot + nb)
+    // persistent update with the npanels (1..kPanelGroup) consecutive panel columns
+    // k + p, updating the trailing columns from first_col on.  Panel p keeps its FP32
+    // low parts from LO slot p nb and its BF16 split from P16 slot 2 p nb (hi of row r
+    // at 2 p nb + r - (k + p) - 1, lo nb slots further)
     int npanels;
-    int64_t blockID2;
-    int lo_base2, p16_base, p16_base2;
     int first_col;
 };
 
@@ -262,6 +260,8 @@ constexpr int kUpdThreads = 320;
 // limited by the shared-memory traffic of TMA writes plus the tensor core's
 // operand reads, not by the depth of the ring
 constexpr int kUpdK = 32;
+// panels per pass of the trailing update over C
+constexpr int kPanelGroup = 4;
 constexpr uint64_t kStepWaitNs = 2000000000ull;
 
 // operand formats of the update: TF32 (FP32 storage, hi = the FP32 value as
@@ -392,6 +392,10 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
                 int r, c, ti;
                 decode(t, &r, &c, &ti);
+                // the tile's 128 rows of C are contiguous: bring them into L2 now, so
+                // the epilogue's reduce-add finds its lines there
+                prefetch_l2(a.A32 + (size_t)block_id(r, c, a.nb) * BSZ * BSZ + (size_t)ti * 128 * BSZ,
+                            128 * BSZ * 4);
                 const bool bf = PREC == HS_PRECISION_BF16X3;
                 for (int kc = 0; kc < kSlabs; ++kc, ++g) {
                     const uint32_t s = g % SM::kStages, use = g / SM::kStages;
@@ -404,8 +408,8 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                     const int pi = kc / kSlabsP, kk = kc % kSlabsP;
                     const int colp = a.k + pi;
                     const int gA = r - colp - 1, gB = c - colp - 1;
-                    const int64_t dblk = pi ? a.blockID2 : a.blockID;
-                    const int lob = pi ? a.lo_base2 : a.lo_base, pb = pi ? a.p16_base2 : a.p16_base;
+                    const int64_t dblk = block_id(colp, colp, a.nb);
+                    const int lob = pi * a.nb, pb = 2 * pi * a.nb;
                     const int hiA = bf ? pb + gA : (int)(dblk + (r - colp));
                     const int loA = bf ? pb + a.nb + gA : lob + gA;
                     const int hiB = bf ? pb + gB : (int)(dblk + (c - colp));
@@ -562,29 +566,271 @@ __global__ void lo_part_kernel(const float* __restrict__ a, float* __restrict__ 
     }
 }
 
-// S (FP64, bsz x bsz) = A32 diagonal block with a unit diagonal on the padding
-// rows >= valid (the padded factor is diag(L, I)); I (FP64) = identity
-__global__ void diag_in_kernel(const float* __restrict__ blk, double* __restrict__ S, double* __restrict__ I,
-                               int bsz, int valid) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < bsz * bsz; e += gridDim.x * blockDim.x) {
-        const bool d = (e / bsz == e % bsz);
-        S[e] = (d && e / bsz >= valid) ? 1.0 : (double)blk[e];
-        I[e] = d ? 1.0 : 0.0;
-    }
-}
+// ------------------------------------------------------------------ diagonal chain
+// The FP64 work on one diagonal block in a single CTA: Cholesky of the FP32 block
+// (lower triangle; rows / columns >= valid replaced by the identity) together with
+// X = L^-1, by one right-looking sweep over 32-column panels p:
+//   - warp 0 factors the 32 x 32 diagonal block in registers (lane = row) and
+//     inverts it (lane = column of X_pp);
+//   - block row p of X is X_pp B_p, B = the identity less the updates below;
+//     the panel rows below the diagonal become row X_pp^T;
+//   - rank-32 updates in 4 x 4 register tiles: the trailing lower triangle of S,
+//     S_rc -= L_rp L_cp^T, and the rows of B below, B_r -= L_rp X_p.
+// S (the working matrix) and B (held transposed in Y, which ends as X^T) stay in
+// global memory (L2-resident); the panel and block row p are staged in shared
+// memory, and column block p of L is written out from there.  Outputs: blk = float(L) (upper triangle zero), Ld = L, Y = X^T,
+// invHi = float(X), invLo = invHi - tf32(invHi).  A pivot that is not > 0 on a
+// valid row records its global row in *info.
+constexpr int kChainThreads = 512;
 
-// after POTRF(S) and Y = I L^-T (= (L^-1)^T): A32 diagonal block = float(L),
-// Ldiag64[k] = L, invHi = hi of L^-1 (row-major, i.e. Y transposed), invLo = lo
-__global__ void diag_out_kernel(const double* __restrict__ S, const double* __restrict__ Y, float* __restrict__ blk,
-                                double* __restrict__ Ld, float* __restrict__ invHi, float* __restrict__ invLo,
-                                int bsz) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < bsz * bsz; e += gridDim.x * blockDim.x) {
-        const int i = e / bsz, j = e % bsz;
-        blk[e] = (float)S[e];
-        Ld[e] = S[e];
-        const float y = (float)Y[(size_t)j * bsz + i];  // (L^-1)[i][j] = Y[j][i]
-        invHi[e] = y;
-        invLo[e] = y - tf32_trunc(y);
+template <int BSZ>
+struct ChainSmem {
+    static constexpr int kP = BSZ / 32;       // panels
+    static constexpr int kPs = 33;            // panel row stride (doubles)
+    static constexpr int kXr = BSZ + 1;       // block-row stride (doubles)
+    static constexpr int kPanel = BSZ * kPs;  // panel rows
+    static constexpr int kRow = 32 * kXr;     // block row p of B / X
+    static constexpr int kXpp = 32 * kPs;     // X_pp
+    static constexpr size_t kBytes = (size_t)(kPanel + kRow + kXpp + 2 * 32 + 32) * sizeof(double);
+};
+
+template <int BSZ>
+__global__ void __launch_bounds__(kChainThreads, 1)
+    diag_chain_kernel(float* __restrict__ blk, double* __restrict__ S, double* __restrict__ Y,
+                      double* __restrict__ Ld, float* __restrict__ invHi, float* __restrict__ invLo, int valid,
+                      long long* __restrict__ info, long long row_base) {
+    using CS = ChainSmem<BSZ>;
+    constexpr int n = BSZ;
+    extern __shared__ double csm[];
+    double* Ps = csm;                // panel rows (row rr = global row c0 + rr)
+    double* Xr = Ps + CS::kPanel;    // block row p: B_p, then X_p (a x c)
+    double* Xp = Xr + CS::kRow;      // X_pp
+    double* colb = Xp + CS::kXpp;    // 2 x 32 column broadcast
+    double* dinv = colb + 64;        // 1 / L_kk of the diagonal block
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    // phase 0: S = lower triangle of the block, B (in Y) = identity; the blocks of
+    // L (blk, Ld) and X (invHi, invLo) above the block diagonal are zero.  Four
+    // elements per step, eight steps in flight per thread.
+    constexpr int kQuads = n * n / 4;
+#pragma unroll 1
+    for (int e0 = tid; e0 < kQuads; e0 += 8 * kChainThreads) {
+        float4 v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * kChainThreads;
+            v[u] = e < kQuads ? reinterpret_cast<const float4*>(blk)[e] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * kChainThreads;
+            if (e >= kQuads) break;
+            const int r = (4 * e) / n, c = (4 * e) % n;  // 4 consecutive columns c..c+3 of row r
+            const float f[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+            double sv[4], yv[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int cc = c + q;
+                sv[q] = (r >= valid || cc >= valid) ? (r == cc ? 1.0 : 0.0) : (double)f[q];
+                yv[q] = r == cc ? 1.0 : 0.0;
+            }
+            double2* S2 = reinterpret_cast<double2*>(S + (size_t)4 * e);
+            double2* Y2 = reinterpret_cast<double2*>(Y + (size_t)4 * e);
+            if (c <= r) {  // the quad lies in the lower triangle up to the diagonal block
+                S2[0] = make_double2(sv[0], sv[1]);
+                S2[1] = make_double2(sv[2], sv[3]);
+            }
+            Y2[0] = make_double2(yv[0], yv[1]);
+            Y2[1] = make_double2(yv[2], yv[3]);
+            if ((r >> 5) < (c >> 5)) {
+                reinterpret_cast<float4*>(blk)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+                reinterpret_cast<double2*>(Ld + (size_t)4 * e)[0] = make_double2(0.0, 0.0);
+                reinterpret_cast<double2*>(Ld + (size_t)4 * e)[1] = make_double2(0.0, 0.0);
+                reinterpret_cast<float4*>(invHi)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+                reinterpret_cast<float4*>(invLo)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+    }
+    __syncthreads();
+
+    for (int p = 0; p < CS::kP; ++p) {
+        const int c0 = 32 * p, rows = n - c0, w = c0 + 32;
+        // panel rows (16 pairs a row) and B_p[a][c] = Y[c][c0 + a] (16 pairs a column):
+        // at most n * 16 / kChainThreads pairs of each per thread, all loads in flight
+        {
+            constexpr int kU = n * 16 / kChainThreads;
+            double2 v[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int e = tid + u * kChainThreads;
+                const int rr = e >> 4, k2 = e & 15;
+                v[u] = rr < rows ? *reinterpret_cast<const double2*>(S + (size_t)(c0 + rr) * n + c0 + 2 * k2)
+                                 : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int e = tid + u * kChainThreads;
+                const int rr = e >> 4, k = 2 * (e & 15);
+                if (rr < rows) {
+                    Ps[rr * CS::kPs + k] = k <= rr ? v[u].x : 0.0;
+                    Ps[rr * CS::kPs + k + 1] = k + 1 <= rr ? v[u].y : 0.0;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int e = tid + u * kChainThreads;
+                const int c = e >> 4, k2 = e & 15;
+                v[u] = c < w ? *reinterpret_cast<const double2*>(Y + (size_t)c * n + c0 + 2 * k2)
+                             : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int e = tid + u * kChainThreads;
+                const int c = e >> 4, a = 2 * (e & 15);
+                if (c < w) {
+                    Xr[a * CS::kXr + c] = v[u].x;
+                    Xr[(a + 1) * CS::kXr + c] = v[u].y;
+                }
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double x[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) x[j] = Ps[lane * CS::kPs + j];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+                const double piv = __shfl_sync(0xffffffffu, x[k], k);
+                if (lane == 0 && c0 + k < valid && !(piv > 0.0)) atomicMin(info, row_base + c0 + k);
+                const double sq = sqrt(piv);
+                const double ri = 1.0 / sq;
+                x[k] = lane == k ? sq : (lane > k ? x[k] * ri : 0.0);
+                if (lane == 0) dinv[k] = ri;
+                double* cb = colb + 32 * (k & 1);
+                cb[lane] = x[k];
+                __syncwarp();
+#pragma unroll
+                for (int j = k + 1; j < 32; ++j) x[j] = x[j] - x[k] * cb[j];
+            }
+#pragma unroll
+            for (int j = 0; j < 32; ++j) Ps[lane * CS::kPs + j] = x[j];
+            __syncwarp();
+            // column `lane` of X_pp
+            double z[32];
+#pragma unroll
+            for (int r = 0; r < 32; ++r) {
+                double v = r == lane ? 1.0 : 0.0;
+#pragma unroll
+                for (int k = 0; k < r; ++k) v = v - Ps[r * CS::kPs + k] * z[k];
+                z[r] = v * dinv[r];
+            }
+#pragma unroll
+            for (int r = 0; r < 32; ++r) Xp[r * CS::kPs + lane] = z[r];
+        }
+        __syncthreads();
+        if (tid < w) {
+            // column tid of block row p: X_p = X_pp B_p
+            double b[32];
+#pragma unroll
+            for (int a = 0; a < 32; ++a) b[a] = Xr[a * CS::kXr + tid];
+#pragma unroll
+            for (int a = 0; a < 32; ++a) {
+                double v = 0.0;
+#pragma unroll
+                for (int q = 0; q <= a; ++q) v = fma(Xp[a * CS::kPs + q], b[q], v);
+                Xr[a * CS::kXr + tid] = v;
+            }
+        } else if (tid < w + rows - 32) {
+            // panel row below the diagonal block: row X_pp^T
+            double* row = Ps + (32 + tid - w) * CS::kPs;
+            double x[32];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) x[k] = row[k];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                double v = 0.0;
+#pragma unroll
+                for (int k = 0; k <= j; ++k) v = fma(x[k], Xp[j * CS::kPs + k], v);
+                row[j] = v;
+            }
+        }
+        __syncthreads();
+        // column block p of L is final (nothing reads it from S again): the FP32
+        // working copy and Ld
+        for (int e = tid; e < rows * 32; e += kChainThreads) {
+            const int rr = e >> 5, k = e & 31;
+            const double l = Ps[rr * CS::kPs + k];
+            const size_t o = (size_t)(c0 + rr) * n + c0 + k;
+            blk[o] = (float)l;
+            Ld[o] = l;
+        }
+        for (int e = tid; e < 32 * w; e += kChainThreads) {
+            const int c = e >> 5, a = e & 31;
+            Y[(size_t)c * n + c0 + a] = Xr[a * CS::kXr + c];
+        }
+        for (int e = tid; e < 32 * w; e += kChainThreads) {
+            const int a = e / w, c = e % w;
+            const float f = (float)Xr[a * CS::kXr + c];
+            invHi[(size_t)(c0 + a) * n + c] = f;
+            invLo[(size_t)(c0 + a) * n + c] = f - tf32_trunc(f);
+        }
+        // rank-32 updates in 4 x 4 tiles: the trailing lower triangle of S (tiles
+        // t < ntri) and the rows of B below block row p (t >= ntri; B_rc in Y[c][r])
+        const int q4 = (rows - 32) >> 2, wq = w >> 2;
+        const int ntri = q4 * (q4 + 1) / 2;
+        const int ntiles = ntri + q4 * wq;
+        for (int t = tid; t < ntiles; t += kChainThreads) {
+            const double* pa;
+            const double* pb;
+            int sb, R, C;
+            if (t < ntri) {
+                R = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+                while (R * (R + 1) / 2 > t) --R;
+                while ((R + 1) * (R + 2) / 2 <= t) ++R;
+                C = t - R * (R + 1) / 2;
+                pb = Ps + (32 + 4 * C) * CS::kPs;
+                sb = CS::kPs;
+            } else {
+                R = (t - ntri) / wq;
+                C = (t - ntri) % wq;
+                pb = Xr + 4 * C;  // X_p[k][4C + j] at pb[k * kXr + j]
+                sb = 1;
+            }
+            pa = Ps + (32 + 4 * R) * CS::kPs;
+            double acc[4][4] = {};
+#pragma unroll 8
+            for (int k = 0; k < 32; ++k) {
+                double av[4], bv[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) av[i] = pa[i * CS::kPs + k];
+                if (t < ntri) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) bv[j] = pb[j * sb + k];
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) bv[j] = pb[k * CS::kXr + j];
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+            }
+            const int r0 = c0 + 32 + 4 * R;
+            if (t < ntri) {
+                double* out = S + (size_t)r0 * n + c0 + 32 + 4 * C;
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) out[(size_t)i * n + j] -= acc[i][j];
+            } else {
+                double* out = Y + (size_t)(4 * C) * n + r0;  // B[r0 + i][4C + j] = Y[4C + j][r0 + i]
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) out[(size_t)j * n + i] -= acc[i][j];
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -677,6 +923,8 @@ hs_status tc_attrs() {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, UpdSmem<BSZ>::kBytes));
     HS_CUDA(cudaFuncSetAttribute(tc_update_kernel<BSZ, HS_PRECISION_BF16X3>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, UpdSmem<BSZ>::kBytes));
+    HS_CUDA(cudaFuncSetAttribute(diag_chain_kernel<BSZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ChainSmem<BSZ>::kBytes));
     if (dev < 64) g_tc_attr[dev][slot] = true;
     return HS_OK;
 }
@@ -695,10 +943,10 @@ size_t mixed_workspace_bytes(int64_t N, int bsz) {
     const size_t T = (size_t)(nb * (nb + 1) / 2);
     size_t bytes = 0;
     bytes += T * bb * 4;                 // A32 / L32
-    bytes += (size_t)(2 * nb + 2) * bb * 4;  // LO: two panels' low parts + L_kk^-1 hi / lo
+    bytes += (size_t)(kPanelGroup * nb + 2) * bb * 4;  // LO: a group's low parts + L_kk^-1 hi / lo
     bytes += (size_t)nb * bb * 8;        // Ldiag64
     bytes += (size_t)nb * bb * 8;        // Yinv
-    bytes += (size_t)4 * nb * bb * 2;    // BF16 split of two panels (hi / lo each)
+    bytes += (size_t)2 * kPanelGroup * nb * bb * 2;  // BF16 split of a group's panels (hi / lo each)
     bytes += bb * 8;                     // S
     bytes += 1024;                       // flags
     return bytes;
@@ -712,27 +960,27 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
     w->A32 = reinterpret_cast<float*>(p);
     p += T * bb * 4;
     w->LO = reinterpret_cast<float*>(p);
-    p += (size_t)(2 * nb + 2) * bb * 4;
+    p += (size_t)(kPanelGroup * nb + 2) * bb * 4;
     w->Ld = reinterpret_cast<double*>(p);
     p += (size_t)nb * bb * 8;
     w->Yinv = reinterpret_cast<double*>(p);
     p += (size_t)nb * bb * 8;
     w->P16 = reinterpret_cast<__nv_bfloat16*>(p);
-    p += (size_t)4 * nb * bb * 2;
+    p += (size_t)2 * kPanelGroup * nb * bb * 2;
     w->S = reinterpret_cast<double*>(p);
     p += bb * 8;
     w->err = reinterpret_cast<int*>(p);
     hs_status st = make_map(&w->mA128, w->A32, bsz, (int64_t)T, 128);
     if (st == HS_OK) st = make_map(&w->mAB, w->A32, bsz, (int64_t)T, bsz);
-    if (st == HS_OK) st = make_map(&w->mL128, w->LO, bsz, 2 * nb + 2, 128);
-    if (st == HS_OK) st = make_map(&w->mLB, w->LO, bsz, 2 * nb + 2, bsz);
+    if (st == HS_OK) st = make_map(&w->mL128, w->LO, bsz, kPanelGroup * nb + 2, 128);
+    if (st == HS_OK) st = make_map(&w->mLB, w->LO, bsz, kPanelGroup * nb + 2, bsz);
     if (st == HS_OK) st = make_map(&w->mU128, w->A32, bsz, (int64_t)T, 128, kUpdK);
     if (st == HS_OK) st = make_map(&w->mUB, w->A32, bsz, (int64_t)T, bsz, kUpdK);
-    if (st == HS_OK) st = make_map(&w->mV128, w->LO, bsz, 2 * nb + 2, 128, kUpdK);
-    if (st == HS_OK) st = make_map(&w->mVB, w->LO, bsz, 2 * nb + 2, bsz, kUpdK);
+    if (st == HS_OK) st = make_map(&w->mV128, w->LO, bsz, kPanelGroup * nb + 2, 128, kUpdK);
+    if (st == HS_OK) st = make_map(&w->mVB, w->LO, bsz, kPanelGroup * nb + 2, bsz, kUpdK);
     if (st == HS_OK) st = make_map(&w->mC32, w->A32, bsz, (int64_t)T, 32, 32);
-    if (st == HS_OK) st = make_map(&w->mP128, w->P16, bsz, 4 * (int64_t)nb, 128, 2 * kUpdK, 2);
-    if (st == HS_OK) st = make_map(&w->mPB, w->P16, bsz, 4 * (int64_t)nb, bsz, 2 * kUpdK, 2);
+    if (st == HS_OK) st = make_map(&w->mP128, w->P16, bsz, 2 * kPanelGroup * (int64_t)nb, 128, 2 * kUpdK, 2);
+    if (st == HS_OK) st = make_map(&w->mPB, w->P16, bsz, 2 * kPanelGroup * (int64_t)nb, bsz, 2 * kUpdK, 2);
     return st;
 }
 
@@ -752,31 +1000,37 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         shift_diag_kernel<<<64, 256, 0, s>>>(w.A32, bsz, nb, ctx->N, (float)shift);
         HS_CHECK_LAUNCH("shift_diag");
     }
-    // diagonal block k in FP64: POTRF of its FP32 values, Y_k = L_kk^-T by TRSM on the
-    // identity, then the FP32 copy, the FP64 L_kk, and the split L_kk^-1 for the TRSM
+    // diagonal block k in FP64 (one CTA): L_kk, its FP32 copy in place, Y_k = L_kk^-T
+    // and the split L_kk^-1 for the panel TRSM
     auto diag_chain = [&](int k, cudaStream_t st_) -> hs_status {
         const int64_t id = T - (int64_t)(nb - k) * (nb - k + 1) / 2;
         float* dblk = w.A32 + (size_t)id * bb;
-        double* Yk = w.Yinv + (size_t)k * bb;
-        const int64_t valid = ctx->N - (int64_t)k * bsz;
+        const int64_t rem = ctx->N - (int64_t)k * bsz;
+        const int valid = rem < bsz ? (int)rem : bsz;
+        float* invHi = w.LO + (size_t)kPanelGroup * nb * bb;
+        prof_begin(ctx, st_, HS_KERNEL_POTRF);
         ctx->launches += 1;
-        diag_in_kernel<<<64, 256, 0, st_>>>(dblk, w.S, Yk, bsz, valid < bsz ? (int)valid : bsz);
-        hs_status r = launch_potrf(ctx, w.S, 0, k, st_);  // block 0 of the scratch, guard rows of block row k
-        if (r != HS_OK) return r;
-        r = launch_trsm_on(ctx, w.S, bsz, Yk, 1, st_);
-        if (r != HS_OK) return r;
-        ctx->launches += 1;
-        diag_out_kernel<<<64, 256, 0, st_>>>(w.S, Yk, dblk, w.Ld + (size_t)k * bb, w.LO + (size_t)2 * nb * bb,
-                                             w.LO + (size_t)(2 * nb + 1) * bb, bsz);
-        HS_CHECK_LAUNCH("mixed diag");
+        if (bsz == 256)
+            diag_chain_kernel<256><<<1, kChainThreads, ChainSmem<256>::kBytes, st_>>>(
+                dblk, w.S, w.Yinv + (size_t)k * bb, w.Ld + (size_t)k * bb, invHi, invHi + bb, valid, ctx->d_info,
+                (long long)k * bsz);
+        else
+            diag_chain_kernel<128><<<1, kChainThreads, ChainSmem<128>::kBytes, st_>>>(
+                dblk, w.S, w.Yinv + (size_t)k * bb, w.Ld + (size_t)k * bb, invHi, invHi + bb, valid, ctx->d_info,
+                (long long)k * bsz);
+        HS_CHECK_LAUNCH("diag_chain");
+        const double nn = bsz;
+        prof_end(ctx, st_, HS_KERNEL_POTRF, 2.0 * nn * nn * nn / 3.0, nn * nn * (4.0 + 8.0 * 4.0 + 4.0 + 4.0));
         return HS_OK;
     };
-    // Panels are factored in pairs (k, k+1) and the columns after them are updated with
-    // both at once (K = 2 bsz per pass over C), which halves the read-modify-write
-    // traffic on the trailing matrix.  Panel k of a pair keeps its low parts in slot
-    // set 0, panel k+1 in set 1.  Lookahead: the update of columns k+2.. runs in two
-    // launches, column k+2 first; the diagonal chain of block k+2 then runs on the side
-    // stream, on SMs the second (larger) launch leaves free.
+    // Panels are factored in groups of up to kPanelGroup (k .. k+g-1) and the columns
+    // after a group are updated with all of its panels at once (K = g bsz per pass
+    // over C), which divides the read-modify-write traffic on the trailing matrix by
+    // g.  Inside a group, column k+i+1 is brought up to date with panels k..k+i just
+    // before its diagonal chain and panel.  Panel k+i keeps its low parts in slot set
+    // i.  Lookahead: the update after a group runs in two launches, its first column
+    // first; the diagonal chain of that column then runs on the side stream, on SMs
+    // the second (larger) launch leaves free.
     const bool lookahead = ctx->side != nullptr && ctx->num_sms > 8;
     const int kFree = 2;
     const double n3 = (double)bsz * bb;
@@ -787,9 +1041,7 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
     base.nb = nb;
     base.err = w.err;
     base.abort_flag = ctx->d_info;
-    base.inv = 2 * nb;
-    base.lo_base2 = nb;
-    base.p16_base2 = 2 * nb;
+    base.inv = kPanelGroup * nb;
     // blocks k+1..nb-1 of column k: FP32 low parts into set `set`, TRSM-as-GEMM with
     // L_kk^-T (writes L and its low part), and for BF16 the split of L into P16
     auto panel = [&](int k, int set) -> hs_status {
@@ -816,14 +1068,13 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         }
         return HS_OK;
     };
-    // trailing update with panels k (.. k + npanels - 1): part 1 = column c0, part 2 =
+    // trailing update with panels k .. k + npanels - 1: part 1 = column c0, part 2 =
     // the columns after it
     auto update = [&](int k, int npanels, int c0, int part, int cap) -> hs_status {
         TcArgs a = base;
         a.k = k;
         a.blockID = diag_id(k);
         a.npanels = npanels;
-        a.blockID2 = npanels > 1 ? diag_id(k + 1) : 0;
         a.first_col = c0;
         a.part = part;
         const double m = nb - c0, np = npanels;
@@ -844,26 +1095,31 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         return HS_OK;
     };
     if ((st = diag_chain(0, s)) != HS_OK) return st;
-    for (int k = 0; k < nb - 1; k += 2) {
-        // precondition: column k is fully updated and its diagonal block factored
-        if ((st = panel(k, 0)) != HS_OK) return st;
-        if ((st = update(k, 1, k + 1, 1, ctx->num_sms)) != HS_OK) return st;  // column k+1
-        if ((st = diag_chain(k + 1, s)) != HS_OK) return st;
-        if (k + 1 == nb - 1) break;
-        if ((st = panel(k + 1, 1)) != HS_OK) return st;
-        if ((st = update(k, 2, k + 2, 1, ctx->num_sms)) != HS_OK) return st;  // column k+2
-        const bool more = k + 3 < nb;  // columns after k+2
+    for (int k = 0; k < nb - 1; k += kPanelGroup) {
+        // precondition: column k has seen every panel before it and its diagonal
+        // block is factored
+        const int g = kPanelGroup < nb - 1 - k ? kPanelGroup : nb - 1 - k;
+        for (int i = 0; i < g; ++i) {
+            if ((st = panel(k + i, i)) != HS_OK) return st;
+            if (i + 1 < g) {
+                if ((st = update(k, i + 1, k + i + 1, 1, ctx->num_sms)) != HS_OK) return st;
+                if ((st = diag_chain(k + i + 1, s)) != HS_OK) return st;
+            }
+        }
+        const int c0 = k + g;
+        if ((st = update(k, g, c0, 1, ctx->num_sms)) != HS_OK) return st;
+        const bool more = c0 + 1 < nb;  // columns after c0
         const bool side = lookahead && more;
         if (side) {
             HS_CUDA(cudaEventRecord(ctx->ev_a, s));
             HS_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_a, 0));
-            if ((st = diag_chain(k + 2, ctx->side)) != HS_OK) return st;
+            if ((st = diag_chain(c0, ctx->side)) != HS_OK) return st;
             HS_CUDA(cudaEventRecord(ctx->ev_b, ctx->side));
         }
-        if (more && (st = update(k, 2, k + 2, 2, side ? ctx->num_sms - kFree : ctx->num_sms)) != HS_OK) return st;
+        if (more && (st = update(k, g, c0, 2, side ? ctx->num_sms - kFree : ctx->num_sms)) != HS_OK) return st;
         if (side) {
             HS_CUDA(cudaStreamWaitEvent(s, ctx->ev_b, 0));
-        } else if ((st = diag_chain(k + 2, s)) != HS_OK) {
+        } else if ((st = diag_chain(c0, s)) != HS_OK) {
             return st;
         }
     }
