@@ -110,6 +110,14 @@ constexpr size_t kScalarOffset = 32 * 1024;
 constexpr size_t kConstOffset = 56 * 1024;
 constexpr int kMaxPartials = 4096;
 
+// FP64 tensor-core step: d (8 x 8, two entries a lane) += a (8 x 4, one entry) b (4 x 8,
+// one entry); lane l holds a[l/4][l%4], b[l%4][l/4], d[l/4][2(l%4) .. +1]
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+        : "+d"(d[0]), "+d"(d[1])
+        : "d"(a), "d"(b));
+}
+
 // --------------------------------------------------------- packed storage
 // block (i,j), i >= j: id = i + nb(nb-1)/2 - (nb-j-1)(nb-j)/2
 __host__ __device__ __forceinline__ int64_t block_id(int64_t i, int64_t j, int64_t nb) {

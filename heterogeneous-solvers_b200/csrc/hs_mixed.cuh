@@ -11,9 +11,9 @@ namespace hs {
 
 // device workspace of one mixed-precision factorization
 struct MixedWork {
-    float* A32 = nullptr;   // packed FP32 copy of K, overwritten by L (off-diagonal blocks used by the solves)
+    float* A32 = nullptr;   // packed FP32 copy of K; its off-diagonal blocks end as L (used by the solves)
     float* LO = nullptr;    // low parts of a panel group (panel p: slots p nb..), then L_kk^-1 hi / lo
-    double* Ld = nullptr;   // FP64 diagonal blocks of L (nb blocks)
+    double* Ld = nullptr;   // FP64 diagonal blocks of L (nb blocks; only the diagonal entries are written)
     double* Yinv = nullptr; // FP64 inverse diagonal blocks, Y_k = L_kk^-T (nb blocks)
     double* S = nullptr;    // FP64 scratch block (POTRF)
     __nv_bfloat16* P16 = nullptr;  // BF16 split of a panel group: panel p hi blocks 2p nb.., lo (2p+1) nb..

@@ -32,11 +32,6 @@ constexpr int kStage = 2 * kStageA;
 constexpr int kChainSmem = STAGES * kStage * (int)sizeof(double);  // 160 KB
 static_assert(BK * LDT <= kStageA, "stage layout");
 
-__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
-    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-        : "+d"(d[0]), "+d"(d[1])
-        : "d"(a), "d"(b));
-}
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));

@@ -177,11 +177,6 @@ size_t trsm_smem(int n) {
 constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4, SPAD = 20;
 constexpr int kTileSmem = 2 * STAGES * BM * SPAD * (int)sizeof(double);  // 160 KB
 
-__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
-    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(d[0]), "+d"(d[1])
-                 : "d"(a), "d"(b));
-}
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));

@@ -570,265 +570,347 @@ __global__ void lo_part_kernel(const float* __restrict__ a, float* __restrict__ 
 // The FP64 work on one diagonal block in a single CTA: Cholesky of the FP32 block
 // (lower triangle; rows / columns >= valid replaced by the identity) together with
 // X = L^-1, by one right-looking sweep over 32-column panels p:
-//   - warp 0 factors the 32 x 32 diagonal block in registers (lane = row) and
-//     inverts it (lane = column of X_pp);
-//   - block row p of X is X_pp B_p, B = the identity less the updates below;
-//     the panel rows below the diagonal become row X_pp^T;
-//   - rank-32 updates in 4 x 4 register tiles: the trailing lower triangle of S,
-//     S_rc -= L_rp L_cp^T, and the rows of B below, B_r -= L_rp X_p.
+//   - the panel's 32 x 32 diagonal block D_p is factored by warp 0 in registers,
+//     column by column, and inverted in the same pass (lane = row of L_pp and
+//     column of X_pp = L_pp^-1; each column of L_pp is broadcast once for both);
+//   - block row p of X is X_pp B_p (B = the identity less the updates below) and
+//     the panel rows below the diagonal block become row X_pp^T;
+//   - rank-32 updates in 32 x 32 warp tiles on the FP64 tensor pipe (DMMA): the
+//     trailing lower triangle, S_rc -= L_rp L_cp^T, and the rows of B below,
+//     B_r -= L_rp X_p.  Warp 1 first computes the diagonal block of panel p+1 (the
+//     corner of the trailing triangle) and hands it to warp 0, which factors it
+//     while warps 1..7 update the rest.
 // S (the working matrix) and B (held transposed in Y, which ends as X^T) stay in
-// global memory (L2-resident); the panel and block row p are staged in shared
-// memory, and column block p of L is written out from there.  Outputs: blk = float(L) (upper triangle zero), Ld = L, Y = X^T,
-// invHi = float(X), invLo = invHi - tf32(invHi).  A pivot that is not > 0 on a
-// valid row records its global row in *info.
-constexpr int kChainThreads = 512;
+// global memory (L2-resident; S is read from the FP32 block directly at panel 0);
+// the panel is staged in shared memory k-major, block row p of B / X as [a][c].
+// Outputs: the diagonal of L in Ld (nothing reads the rest of L, and the FP32 block
+// keeps its input), Y = X^T, invHi = float(X), invLo = invHi - tf32(invHi).
+// A pivot that is not > 0 on a valid row records its global row in *info.
+constexpr int kChainThreads = 256;
 
 template <int BSZ>
 struct ChainSmem {
     static constexpr int kP = BSZ / 32;       // panels
-    static constexpr int kPs = 33;            // panel row stride (doubles)
-    static constexpr int kXr = BSZ + 1;       // block-row stride (doubles)
-    static constexpr int kPanel = BSZ * kPs;  // panel rows
-    static constexpr int kRow = 32 * kXr;     // block row p of B / X
-    static constexpr int kXpp = 32 * kPs;     // X_pp
-    static constexpr size_t kBytes = (size_t)(kPanel + kRow + kXpp + 2 * 32 + 32) * sizeof(double);
+    static constexpr int kLt = BSZ - 32 + 4;  // k-major panel stride (rows below the diagonal block)
+    static constexpr int kXr = BSZ + 4;       // block-row stride
+    static constexpr int kD = 33;             // diagonal block / inverse stride
+    static constexpr size_t kBytes = (size_t)(32 * kLt + 32 * kXr + 2 * 32 * kD + 64) * sizeof(double);
 };
+
+// two / four consecutive entries (r, c..) of the working matrix: the FP32 block with
+// the identity outside the valid range (panel 0), else S
+template <int BSZ>
+__device__ __forceinline__ void chain_src4(const float* __restrict__ blk, const double* __restrict__ S, bool first,
+                                           int valid, int r, int c, double v[4]) {
+    if (first) {
+        const float4 f = *reinterpret_cast<const float4*>(blk + (size_t)r * BSZ + c);
+        const float fv[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[q] = (r >= valid || c + q >= valid) ? (r == c + q ? 1.0 : 0.0) : (double)fv[q];
+    } else {
+        const double2 a = *reinterpret_cast<const double2*>(S + (size_t)r * BSZ + c);
+        const double2 b = *reinterpret_cast<const double2*>(S + (size_t)r * BSZ + c + 2);
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = b.x;
+        v[3] = b.y;
+    }
+}
+
+template <int BSZ>
+__device__ __forceinline__ double2 chain_src2(const float* __restrict__ blk, const double* __restrict__ S, bool first,
+                                              int valid, int r, int c) {
+    if (first) {
+        const float2 f = *reinterpret_cast<const float2*>(blk + (size_t)r * BSZ + c);
+        return make_double2((r >= valid || c >= valid) ? (r == c ? 1.0 : 0.0) : (double)f.x,
+                            (r >= valid || c + 1 >= valid) ? (r == c + 1 ? 1.0 : 0.0) : (double)f.y);
+    }
+    return *reinterpret_cast<const double2*>(S + (size_t)r * BSZ + c);
+}
+
+// warp 0: D (32 x 32, stride kD, lower triangle read) -> L_pp in D (upper part
+// zero) and Xp = L_pp^-1.  d0 = the block's first row within the diagonal block
+// of the matrix.
+__device__ __forceinline__ void chain_diag(double* __restrict__ D, double* __restrict__ Xp,
+                                           double* __restrict__ colb, int lane, int d0, int valid,
+                                           long long* __restrict__ info, long long row_base) {
+    constexpr int kD = 33;
+    double x[32], z[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        x[j] = j <= lane ? D[lane * kD + j] : 0.0;
+        z[j] = j == lane ? 1.0 : 0.0;
+    }
+    // the pivot of step k+1 is taken from lane k+1 as soon as that lane has its own
+    // L[k+1][k], ahead of the column broadcast through shared memory
+    double piv = __shfl_sync(0xffffffffu, x[0], 0);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+        if (lane == 0 && d0 + k < valid && !(piv > 0.0)) atomicMin(info, row_base + d0 + k);
+        const double ri = rsqrt(piv);
+        const double lk = lane == k ? piv * ri : (lane > k ? x[k] * ri : 0.0);  // L[lane][k]
+        const double zk = z[k] * ri;                                            // X[k][lane]
+        x[k] = lk;
+        z[k] = zk;
+        if (k + 1 < 32) piv = __shfl_sync(0xffffffffu, x[k + 1] - lk * lk, k + 1);
+        double* cb = colb + 32 * (k & 1);
+        cb[lane] = lk;
+        __syncwarp();
+#pragma unroll
+        for (int j = k + 1; j < 32; ++j) {
+            const double ljk = cb[j];
+            x[j] = x[j] - lk * ljk;
+            z[j] = z[j] - ljk * zk;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        D[lane * kD + j] = x[j];
+        Xp[j * kD + lane] = z[j];
+    }
+}
+
+// one 32 x 32 warp tile of sum_k A[m][k] B[k][n] over K = 32 on the FP64 tensor
+// pipe: A[m][k] = pa[k * lda + m], B[k][n] = pb[k * ldb + n]; lane holds rows
+// 8 mi + lane/4, columns 8 ni + 2 (lane%4) + {0, 1}
+__device__ __forceinline__ void chain_wtile(const double* __restrict__ pa, int lda, const double* __restrict__ pb,
+                                            int ldb, int lane, double (&acc)[4][4][2]) {
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+#pragma unroll
+    for (int k0 = 0; k0 < 32; k0 += 4) {
+        double a[4], b[4];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi) a[mi] = pa[(k0 + t) * lda + 8 * mi + g];
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) b[ni] = pb[(k0 + t) * ldb + 8 * ni + g];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) dmma884(acc[mi][ni], a[mi], b[ni]);
+    }
+}
+
+__device__ __forceinline__ void chain_bar(int id, int count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// block row p of X from shared memory -> Y (transposed; zero before column c0 in
+// the panel's rows of Y) and invHi / invLo (zero after column w when `zero_upper`:
+// the planes are shared by all diagonal blocks and only the first writes the part
+// above the block diagonal).  Threads `t0`, `t0 + nt`, ... take part.
+template <int BSZ>
+__device__ __forceinline__ void chain_outputs(double* __restrict__ Y, float* __restrict__ invHi,
+                                              float* __restrict__ invLo, const double* __restrict__ Xr, int c0,
+                                              bool zero_upper, int t0, int nt) {
+    using CS = ChainSmem<BSZ>;
+    constexpr int n = BSZ, kXr = CS::kXr;
+    const int w = c0 + 32;
+    for (int e = t0; e < w * 8; e += nt) {
+        const int c = e % w, a4 = e / w;
+        double v[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[q] = Xr[(4 * a4 + q) * kXr + c];
+        *reinterpret_cast<double2*>(Y + (size_t)c * n + c0 + 4 * a4) = make_double2(v[0], v[1]);
+        *reinterpret_cast<double2*>(Y + (size_t)c * n + c0 + 4 * a4 + 2) = make_double2(v[2], v[3]);
+    }
+    for (int e = t0; e < 32 * c0 / 2; e += nt) {
+        const int c = c0 + (2 * e) / c0, r = (2 * e) % c0;
+        *reinterpret_cast<double2*>(Y + (size_t)c * n + r) = make_double2(0.0, 0.0);
+    }
+    const int cw = zero_upper ? n : w;  // columns written
+    for (int e = t0; e < 8 * cw; e += nt) {
+        const int a = e / (cw / 4), c = 4 * (e % (cw / 4));
+        float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (c < w) {
+            const double* xr = Xr + a * kXr + c;
+            f = make_float4((float)xr[0], (float)xr[1], (float)xr[2], (float)xr[3]);
+        }
+        const size_t o = (size_t)(c0 + a) * n + c;
+        *reinterpret_cast<float4*>(invHi + o) = f;
+        *reinterpret_cast<float4*>(invLo + o) =
+            make_float4(f.x - tf32_trunc(f.x), f.y - tf32_trunc(f.y), f.z - tf32_trunc(f.z), f.w - tf32_trunc(f.w));
+    }
+}
 
 template <int BSZ>
 __global__ void __launch_bounds__(kChainThreads, 1)
-    diag_chain_kernel(float* __restrict__ blk, double* __restrict__ S, double* __restrict__ Y,
+    diag_chain_kernel(const float* __restrict__ blk, double* __restrict__ S, double* __restrict__ Y,
                       double* __restrict__ Ld, float* __restrict__ invHi, float* __restrict__ invLo, int valid,
-                      long long* __restrict__ info, long long row_base) {
+                      int zero_upper, long long* __restrict__ info, long long row_base) {
     using CS = ChainSmem<BSZ>;
-    constexpr int n = BSZ;
+    constexpr int n = BSZ, kLt = CS::kLt, kXr = CS::kXr, kD = CS::kD;
+    constexpr int kIt = (n * 8 + kChainThreads - 1) / kChainThreads;  // staging steps a thread
     extern __shared__ double csm[];
-    double* Ps = csm;                // panel rows (row rr = global row c0 + rr)
-    double* Xr = Ps + CS::kPanel;    // block row p: B_p, then X_p (a x c)
-    double* Xp = Xr + CS::kRow;      // X_pp
-    double* colb = Xp + CS::kXpp;    // 2 x 32 column broadcast
-    double* dinv = colb + 64;        // 1 / L_kk of the diagonal block
+    double* PsT = csm;               // [k][rr - 32]: panel rows below the diagonal block
+    double* Xr = PsT + 32 * kLt;     // [a][c]: block row p of B, then of X
+    double* D = Xr + 32 * kXr;       // diagonal block of the current panel (L after warp 0)
+    double* Xp = D + 32 * kD;        // its inverse
+    double* colb = Xp + 32 * kD;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    // phase 0: S = lower triangle of the block, B (in Y) = identity; the blocks of
-    // L (blk, Ld) and X (invHi, invLo) above the block diagonal are zero.  Four
-    // elements per step, eight steps in flight per thread.
-    constexpr int kQuads = n * n / 4;
-#pragma unroll 1
-    for (int e0 = tid; e0 < kQuads; e0 += 8 * kChainThreads) {
-        float4 v[8];
+    if (warp == 0) {  // D_0 from the FP32 block
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int e = e0 + u * kChainThreads;
-            v[u] = e < kQuads ? reinterpret_cast<const float4*>(blk)[e] : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int j4 = 0; j4 < 8; ++j4) {
+            double v[4];
+            chain_src4<BSZ>(blk, S, true, valid, lane, 4 * j4, v);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) D[lane * kD + 4 * j4 + q] = v[q];
         }
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int e = e0 + u * kChainThreads;
-            if (e >= kQuads) break;
-            const int r = (4 * e) / n, c = (4 * e) % n;  // 4 consecutive columns c..c+3 of row r
-            const float f[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
-            double sv[4], yv[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int cc = c + q;
-                sv[q] = (r >= valid || cc >= valid) ? (r == cc ? 1.0 : 0.0) : (double)f[q];
-                yv[q] = r == cc ? 1.0 : 0.0;
-            }
-            double2* S2 = reinterpret_cast<double2*>(S + (size_t)4 * e);
-            double2* Y2 = reinterpret_cast<double2*>(Y + (size_t)4 * e);
-            if (c <= r) {  // the quad lies in the lower triangle up to the diagonal block
-                S2[0] = make_double2(sv[0], sv[1]);
-                S2[1] = make_double2(sv[2], sv[3]);
-            }
-            Y2[0] = make_double2(yv[0], yv[1]);
-            Y2[1] = make_double2(yv[2], yv[3]);
-            if ((r >> 5) < (c >> 5)) {
-                reinterpret_cast<float4*>(blk)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-                reinterpret_cast<double2*>(Ld + (size_t)4 * e)[0] = make_double2(0.0, 0.0);
-                reinterpret_cast<double2*>(Ld + (size_t)4 * e)[1] = make_double2(0.0, 0.0);
-                reinterpret_cast<float4*>(invHi)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-                reinterpret_cast<float4*>(invLo)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-        }
+        __syncwarp();
+        chain_diag(D, Xp, colb, lane, 0, valid, info, row_base);
     }
     __syncthreads();
 
     for (int p = 0; p < CS::kP; ++p) {
-        const int c0 = 32 * p, rows = n - c0, w = c0 + 32;
-        // panel rows (16 pairs a row) and B_p[a][c] = Y[c][c0 + a] (16 pairs a column):
-        // at most n * 16 / kChainThreads pairs of each per thread, all loads in flight
+        const int c0 = 32 * p, mb = n - c0 - 32, w = c0 + 32;
+        const bool first = p == 0;
         {
-            constexpr int kU = n * 16 / kChainThreads;
-            double2 v[kU];
+            // panel rows below the diagonal block, four columns a step (rows fastest),
+            // all loads of a thread in flight before the shared stores
+            double v[kIt][4];
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
+            for (int u = 0; u < kIt; ++u) {
                 const int e = tid + u * kChainThreads;
-                const int rr = e >> 4, k2 = e & 15;
-                v[u] = rr < rows ? *reinterpret_cast<const double2*>(S + (size_t)(c0 + rr) * n + c0 + 2 * k2)
-                                 : make_double2(0.0, 0.0);
+                if (e < mb * 8) chain_src4<BSZ>(blk, S, first, valid, c0 + 32 + e % mb, c0 + 4 * (e / mb), v[u]);
             }
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
+            for (int u = 0; u < kIt; ++u) {
                 const int e = tid + u * kChainThreads;
-                const int rr = e >> 4, k = 2 * (e & 15);
-                if (rr < rows) {
-                    Ps[rr * CS::kPs + k] = k <= rr ? v[u].x : 0.0;
-                    Ps[rr * CS::kPs + k + 1] = k + 1 <= rr ? v[u].y : 0.0;
+                if (e < mb * 8) {
+                    const int rr = e % mb, k4 = e / mb;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) PsT[(4 * k4 + q) * kLt + rr] = v[u][q];
+                }
+            }
+            // B_p[a][c]: columns before the panel from Y[c][c0 + a], the panel's own the identity
+#pragma unroll
+            for (int u = 0; u < kIt; ++u) {
+                const int e = tid + u * kChainThreads;
+                const int c = e % w, a4 = e / w;
+                if (e < w * 8) {
+                    if (c < c0) {
+                        const double2 x0 = *reinterpret_cast<const double2*>(Y + (size_t)c * n + c0 + 4 * a4);
+                        const double2 x1 = *reinterpret_cast<const double2*>(Y + (size_t)c * n + c0 + 4 * a4 + 2);
+                        v[u][0] = x0.x;
+                        v[u][1] = x0.y;
+                        v[u][2] = x1.x;
+                        v[u][3] = x1.y;
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) v[u][q] = (c - c0 == 4 * a4 + q) ? 1.0 : 0.0;
+                    }
                 }
             }
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
+            for (int u = 0; u < kIt; ++u) {
                 const int e = tid + u * kChainThreads;
-                const int c = e >> 4, k2 = e & 15;
-                v[u] = c < w ? *reinterpret_cast<const double2*>(Y + (size_t)c * n + c0 + 2 * k2)
-                             : make_double2(0.0, 0.0);
-            }
+                if (e < w * 8) {
+                    const int c = e % w, a4 = e / w;
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                const int e = tid + u * kChainThreads;
-                const int c = e >> 4, a = 2 * (e & 15);
-                if (c < w) {
-                    Xr[a * CS::kXr + c] = v[u].x;
-                    Xr[(a + 1) * CS::kXr + c] = v[u].y;
+                    for (int q = 0; q < 4; ++q) Xr[(4 * a4 + q) * kXr + c] = v[u][q];
                 }
             }
-        }
-        __syncthreads();
-        if (warp == 0) {
-            double x[32];
-#pragma unroll
-            for (int j = 0; j < 32; ++j) x[j] = Ps[lane * CS::kPs + j];
-#pragma unroll
-            for (int k = 0; k < 32; ++k) {
-                const double piv = __shfl_sync(0xffffffffu, x[k], k);
-                if (lane == 0 && c0 + k < valid && !(piv > 0.0)) atomicMin(info, row_base + c0 + k);
-                const double sq = sqrt(piv);
-                const double ri = 1.0 / sq;
-                x[k] = lane == k ? sq : (lane > k ? x[k] * ri : 0.0);
-                if (lane == 0) dinv[k] = ri;
-                double* cb = colb + 32 * (k & 1);
-                cb[lane] = x[k];
-                __syncwarp();
-#pragma unroll
-                for (int j = k + 1; j < 32; ++j) x[j] = x[j] - x[k] * cb[j];
-            }
-#pragma unroll
-            for (int j = 0; j < 32; ++j) Ps[lane * CS::kPs + j] = x[j];
-            __syncwarp();
-            // column `lane` of X_pp
-            double z[32];
-#pragma unroll
-            for (int r = 0; r < 32; ++r) {
-                double v = r == lane ? 1.0 : 0.0;
-#pragma unroll
-                for (int k = 0; k < r; ++k) v = v - Ps[r * CS::kPs + k] * z[k];
-                z[r] = v * dinv[r];
-            }
-#pragma unroll
-            for (int r = 0; r < 32; ++r) Xp[r * CS::kPs + lane] = z[r];
         }
         __syncthreads();
         if (tid < w) {
             // column tid of block row p: X_p = X_pp B_p
-            double b[32];
-#pragma unroll
-            for (int a = 0; a < 32; ++a) b[a] = Xr[a * CS::kXr + tid];
+            double b[32], v[32];
 #pragma unroll
             for (int a = 0; a < 32; ++a) {
-                double v = 0.0;
-#pragma unroll
-                for (int q = 0; q <= a; ++q) v = fma(Xp[a * CS::kPs + q], b[q], v);
-                Xr[a * CS::kXr + tid] = v;
+                b[a] = Xr[a * kXr + tid];
+                v[a] = 0.0;
             }
-        } else if (tid < w + rows - 32) {
+#pragma unroll
+            for (int q = 0; q < 32; ++q)
+#pragma unroll
+                for (int a = q; a < 32; ++a) v[a] = fma(Xp[a * kD + q], b[q], v[a]);
+#pragma unroll
+            for (int a = 0; a < 32; ++a) Xr[a * kXr + tid] = v[a];
+        } else if (tid < w + mb) {
             // panel row below the diagonal block: row X_pp^T
-            double* row = Ps + (32 + tid - w) * CS::kPs;
-            double x[32];
+            const int rr = tid - w;
+            double x[32], v[32];
 #pragma unroll
-            for (int k = 0; k < 32; ++k) x[k] = row[k];
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                double v = 0.0;
-#pragma unroll
-                for (int k = 0; k <= j; ++k) v = fma(x[k], Xp[j * CS::kPs + k], v);
-                row[j] = v;
+            for (int k = 0; k < 32; ++k) {
+                x[k] = PsT[k * kLt + rr];
+                v[k] = 0.0;
             }
+#pragma unroll
+            for (int k = 0; k < 32; ++k)
+#pragma unroll
+                for (int j = k; j < 32; ++j) v[j] = fma(x[k], Xp[j * kD + k], v[j]);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) PsT[j * kLt + rr] = v[j];
         }
         __syncthreads();
-        // column block p of L is final (nothing reads it from S again): the FP32
-        // working copy and Ld
-        for (int e = tid; e < rows * 32; e += kChainThreads) {
-            const int rr = e >> 5, k = e & 31;
-            const double l = Ps[rr * CS::kPs + k];
-            const size_t o = (size_t)(c0 + rr) * n + c0 + k;
-            blk[o] = (float)l;
-            Ld[o] = l;
+        // the diagonal of L -> Ld (D is rewritten below); block row p of X goes out
+        // during the updates
+        if (tid < 32) Ld[(size_t)(c0 + tid) * n + c0 + tid] = D[tid * kD + tid];
+        if (mb == 0) {
+            chain_outputs<BSZ>(Y, invHi, invLo, Xr, c0, zero_upper != 0, tid, kChainThreads);
+            break;
         }
-        for (int e = tid; e < 32 * w; e += kChainThreads) {
-            const int c = e >> 5, a = e & 31;
-            Y[(size_t)c * n + c0 + a] = Xr[a * CS::kXr + c];
-        }
-        for (int e = tid; e < 32 * w; e += kChainThreads) {
-            const int a = e / w, c = e % w;
-            const float f = (float)Xr[a * CS::kXr + c];
-            invHi[(size_t)(c0 + a) * n + c] = f;
-            invLo[(size_t)(c0 + a) * n + c] = f - tf32_trunc(f);
-        }
-        // rank-32 updates in 4 x 4 tiles: the trailing lower triangle of S (tiles
-        // t < ntri) and the rows of B below block row p (t >= ntri; B_rc in Y[c][r])
-        const int q4 = (rows - 32) >> 2, wq = w >> 2;
-        const int ntri = q4 * (q4 + 1) / 2;
-        const int ntiles = ntri + q4 * wq;
-        for (int t = tid; t < ntiles; t += kChainThreads) {
-            const double* pa;
-            const double* pb;
-            int sb, R, C;
-            if (t < ntri) {
-                R = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
-                while (R * (R + 1) / 2 > t) --R;
-                while ((R + 1) * (R + 2) / 2 <= t) ++R;
-                C = t - R * (R + 1) / 2;
-                pb = Ps + (32 + 4 * C) * CS::kPs;
-                sb = CS::kPs;
-            } else {
-                R = (t - ntri) / wq;
-                C = (t - ntri) % wq;
-                pb = Xr + 4 * C;  // X_p[k][4C + j] at pb[k * kXr + j]
-                sb = 1;
-            }
-            pa = Ps + (32 + 4 * R) * CS::kPs;
-            double acc[4][4] = {};
-#pragma unroll 8
-            for (int k = 0; k < 32; ++k) {
-                double av[4], bv[4];
+        __syncthreads();  // D, Xp are rewritten below
+        if (warp == 0) {
+            chain_bar(1, 64);  // warp 1 has written D of panel p+1
+            chain_diag(D, Xp, colb, lane, c0 + 32, valid, info, row_base);
+        } else {
+            // 32 x 32 warp tiles over warps 1..7: the trailing lower triangle (its
+            // corner, the diagonal block of panel p+1, first and into D), then the rows
+            // of B below block row p (in Y[c][r]; the panel's own columns are written
+            // for the first time)
+            const int g = lane >> 2, t = lane & 3;
+            const int q = mb >> 5, wq = w >> 5;
+            const int ntri = q * (q + 1) / 2;
+            const int ntiles = ntri + q * wq;
+            // warp 4 shares warp 0's scheduler and stays off the tile work
+            constexpr int kTw = kChainThreads / 32 - 2;
+            const int tw = warp < 4 ? warp - 1 : warp - 2;
+            double acc[4][4][2];
+            for (int u = tw; u < ntiles && warp != 4; u += kTw) {
+                if (u < ntri) {
+                    int R = (int)((sqrtf(8.0f * u + 1.0f) - 1.0f) * 0.5f);
+                    while (R * (R + 1) / 2 > u) --R;
+                    while ((R + 1) * (R + 2) / 2 <= u) ++R;
+                    const int C = u - R * (R + 1) / 2;
+                    chain_wtile(PsT + 32 * R, kLt, PsT + 32 * C, kLt, lane, acc);
+                    const int r0 = c0 + 32 + 32 * R, cc0 = c0 + 32 + 32 * C;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) av[i] = pa[i * CS::kPs + k];
-                if (t < ntri) {
+                    for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) bv[j] = pb[j * sb + k];
+                        for (int ni = 0; ni < 4; ++ni) {
+                            const int r = r0 + 8 * mi + g, c = cc0 + 8 * ni + 2 * t;
+                            const double2 sv = chain_src2<BSZ>(blk, S, first, valid, r, c);
+                            const double2 o = make_double2(sv.x - acc[mi][ni][0], sv.y - acc[mi][ni][1]);
+                            if (u == 0) {
+                                D[(r - r0) * kD + (c - cc0)] = o.x;
+                                D[(r - r0) * kD + (c - cc0) + 1] = o.y;
+                            } else {
+                                *reinterpret_cast<double2*>(S + (size_t)r * n + c) = o;
+                            }
+                        }
+                    if (u == 0) chain_bar(1, 64);  // D of panel p+1 is ready for warp 0
                 } else {
+                    const int R = (u - ntri) % q, C = (u - ntri) / q;
+                    chain_wtile(PsT + 32 * R, kLt, Xr + 32 * C, kXr, lane, acc);
+                    const bool fresh = C == p;
+                    const int r0 = c0 + 32 + 32 * R;
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) bv[j] = pb[k * CS::kXr + j];
+                    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                            for (int i = 0; i < 2; ++i) {
+                                double* o = Y + (size_t)(32 * C + 8 * ni + 2 * t + i) * n + r0 + 8 * mi + g;
+                                *o = (fresh ? 0.0 : *o) - acc[mi][ni][i];
+                            }
                 }
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
             }
-            const int r0 = c0 + 32 + 4 * R;
-            if (t < ntri) {
-                double* out = S + (size_t)r0 * n + c0 + 32 + 4 * C;
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) out[(size_t)i * n + j] -= acc[i][j];
-            } else {
-                double* out = Y + (size_t)(4 * C) * n + r0;  // B[r0 + i][4C + j] = Y[4C + j][r0 + i]
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) out[(size_t)j * n + i] -= acc[i][j];
-            }
+            chain_outputs<BSZ>(Y, invHi, invLo, Xr, c0, zero_upper != 0, tid - 32, kChainThreads - 32);
         }
         __syncthreads();
     }
@@ -1012,12 +1094,12 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         ctx->launches += 1;
         if (bsz == 256)
             diag_chain_kernel<256><<<1, kChainThreads, ChainSmem<256>::kBytes, st_>>>(
-                dblk, w.S, w.Yinv + (size_t)k * bb, w.Ld + (size_t)k * bb, invHi, invHi + bb, valid, ctx->d_info,
-                (long long)k * bsz);
+                dblk, w.S, w.Yinv + (size_t)k * bb, w.Ld + (size_t)k * bb, invHi, invHi + bb, valid, k == 0,
+                ctx->d_info, (long long)k * bsz);
         else
             diag_chain_kernel<128><<<1, kChainThreads, ChainSmem<128>::kBytes, st_>>>(
-                dblk, w.S, w.Yinv + (size_t)k * bb, w.Ld + (size_t)k * bb, invHi, invHi + bb, valid, ctx->d_info,
-                (long long)k * bsz);
+                dblk, w.S, w.Yinv + (size_t)k * bb, w.Ld + (size_t)k * bb, invHi, invHi + bb, valid, k == 0,
+                ctx->d_info, (long long)k * bsz);
         HS_CHECK_LAUNCH("diag_chain");
         const double nn = bsz;
         prof_end(ctx, st_, HS_KERNEL_POTRF, 2.0 * nn * nn * nn / 3.0, nn * nn * (4.0 + 8.0 * 4.0 + 4.0 + 4.0));
