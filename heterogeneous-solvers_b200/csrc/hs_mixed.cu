@@ -144,17 +144,13 @@ int grid_n(int64_t n, int sms) {
 }  // namespace
 
 // b <- (L L^T)^-1 b with the mixed factor: FP32 off-diagonal blocks, FP64
-// inverse diagonal blocks; one launch per block column and direction.  The
-// forward sweep reduces b in place and writes L^-1 b into tmp; the backward
-// sweep reduces tmp in place and writes the result into b.
-hs_status mixed_apply(hs_ctx ctx, const MixedWork& w, double* b, double* tmp, cudaStream_t s) {
-    const int nb = ctx->nb;
-    hs_status st;
-    for (int j = -1; j < nb - 1; ++j)
-        if ((st = launch_mixed_sweep(ctx, w.A32, w.Yinv, b, tmp, j, 1, s)) != HS_OK) return st;
-    for (int j = nb; j >= 1; --j)
-        if ((st = launch_mixed_sweep(ctx, w.A32, w.Yinv, tmp, b, j, 0, s)) != HS_OK) return st;
-    return HS_OK;
+// inverse diagonal blocks; one cooperative launch a direction.  The forward sweep
+// reads b and writes L^-1 b into tmp; the backward sweep reads tmp and writes the
+// result into b.
+hs_status mixed_apply(hs_ctx ctx, MixedWork& w, double* b, double* tmp, cudaStream_t s) {
+    hs_status st = launch_mixed_sweep_whole(ctx, w.A32, w.Yinv, b, tmp, 1, ++w.epoch, w.flags, w.err + 1, s);
+    if (st != HS_OK) return st;
+    return launch_mixed_sweep_whole(ctx, w.A32, w.Yinv, tmp, b, 0, ++w.epoch, w.flags, w.err + 1, s);
 }
 
 namespace {
@@ -196,6 +192,8 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     MixedWork w;
     st = mixed_bind(ctx, ctx->mixed, &w);
     if (st != HS_OK) return st;
+    HS_CUDA(cudaMemsetAsync(w.flags, 0, (size_t)nb * sizeof(unsigned), s));
+    HS_CUDA(cudaMemsetAsync(w.err + 1, 0, sizeof(int), s));
     st = ensure_scratch(ctx, kSmallScratch + (size_t)nb * nb * bsz * sizeof(double));
     if (st != HS_OK) return st;
     double* part = static_cast<double*>(ctx->scratch);
@@ -379,6 +377,7 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     cudaEventElapsedTime(&ms, ev.e[1], ev.e[2]);
     R.refine_ms = ms;
     R.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if ((st = mixed_check_error(ctx, w)) != HS_OK) return st;
     if (!converged) {
         set_error("hs_mixed_solve: backward error " + std::to_string(R.backward_error) + " above the target " +
                   std::to_string(tol) + " after refinement and preconditioned CG");

@@ -17,7 +17,9 @@ struct MixedWork {
     double* Yinv = nullptr; // FP64 inverse diagonal blocks, Y_k = L_kk^-T (nb blocks)
     double* S = nullptr;    // FP64 scratch block (POTRF)
     __nv_bfloat16* P16 = nullptr;  // BF16 split of a panel group: panel p hi blocks 2p nb.., lo (2p+1) nb..
-    int* err = nullptr;     // tensor-core tile timeout flag
+    int* err = nullptr;     // [0] tensor-core tile timeout, [1] triangular-sweep timeout
+    unsigned* flags = nullptr;  // per block row: epoch of the sweep that published it
+    unsigned epoch = 0;         // last sweep launched (flags are cleared when it restarts at 0)
     CUtensorMap mA128, mAB, mL128, mLB;  // 128-byte swizzle, 32-wide K boxes (TRSM)
     CUtensorMap mU128, mUB, mV128, mVB;  // K boxes of 128 bytes over A32 / LO (TF32 update)
     CUtensorMap mP128, mPB;              // K boxes of 128 bytes over P16 (BF16 update)
@@ -30,6 +32,8 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w);
 hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift = 0.0,
                        int precision = HS_PRECISION_TF32X3);
 hs_status mixed_check_error(hs_ctx ctx, const MixedWork& w);
+// b <- (L L^T)^-1 b with the mixed factor (tmp: intermediate)
+hs_status mixed_apply(hs_ctx ctx, MixedWork& w, double* b, double* tmp, cudaStream_t s);
 // the mixed-precision solve behind hs_mixed_solve (workspace kept by the context)
 hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,
                            int max_steps, hs_mixed_report* out);
@@ -40,6 +44,11 @@ hs_status launch_trsm_on(hs_ctx ctx, const double* L, int n, double* B, int item
 // one launch of a forward / backward sweep with the mixed factor (k_vector.cu)
 hs_status launch_mixed_sweep(hs_ctx ctx, const float* A32, const double* Y, double* work, double* out, int j,
                              int forward, cudaStream_t s);
+// a whole forward / backward sweep in one cooperative launch: out = L^-1 in or
+// L^-T in (block rows published through flags[] with value `epoch`; *err = 2 on a
+// wait that timed out)
+hs_status launch_mixed_sweep_whole(hs_ctx ctx, const float* A32, const double* Y, const double* in, double* out,
+                                   int forward, unsigned epoch, unsigned* flags, int* err, cudaStream_t s);
 // column update reading FP32 blocks (accumulation in FP64)
 hs_status launch_column_update_f32(hs_ctx ctx, const float* A32, double* b, int blockStart, int blockCount,
                                    int blockRow, int blockID, int transposed, cudaStream_t s);

@@ -1030,7 +1030,8 @@ size_t mixed_workspace_bytes(int64_t N, int bsz) {
     bytes += (size_t)nb * bb * 8;        // Yinv
     bytes += (size_t)2 * kPanelGroup * nb * bb * 2;  // BF16 split of a group's panels (hi / lo each)
     bytes += bb * 8;                     // S
-    bytes += 1024;                       // flags
+    bytes += 1024;                       // error flags
+    bytes += ((size_t)nb * 4 + 255) & ~size_t(255);  // sweep publication flags
     return bytes;
 }
 
@@ -1052,6 +1053,7 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
     w->S = reinterpret_cast<double*>(p);
     p += bb * 8;
     w->err = reinterpret_cast<int*>(p);
+    w->flags = reinterpret_cast<unsigned*>(p + 1024);
     hs_status st = make_map(&w->mA128, w->A32, bsz, (int64_t)T, 128);
     if (st == HS_OK) st = make_map(&w->mAB, w->A32, bsz, (int64_t)T, bsz);
     if (st == HS_OK) st = make_map(&w->mL128, w->LO, bsz, kPanelGroup * nb + 2, 128);
@@ -1209,10 +1211,14 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
 }
 
 hs_status mixed_check_error(hs_ctx ctx, const MixedWork& w) {
-    int e = 0;
-    HS_CUDA(cudaMemcpy(&e, w.err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (e) {
+    int e[2] = {0, 0};
+    HS_CUDA(cudaMemcpy(e, w.err, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e[0]) {
         set_error("mixed-precision factor: a tensor-core tile gave up waiting for its operands (timeout)");
+        return HS_ERR_TIMEOUT;
+    }
+    if (e[1]) {
+        set_error("mixed-precision solve: a triangular sweep gave up waiting for a block row (timeout)");
         return HS_ERR_TIMEOUT;
     }
     (void)ctx;

@@ -441,6 +441,151 @@ __global__ void __launch_bounds__(kThreads) mixed_sweep_kernel(const float* __re
     }
 }
 
+// Whole sweep in one launch.  CTA c owns block rows i = c, c + P, ... (P = grid)
+// and keeps their running right-hand sides in shared memory.  Forward (t = L^-1 b):
+// row i takes L_ij out_j off for j = 0 .. i-1 in that order, then its owner solves
+// out_i = Y_i^T t_i and publishes it; backward (L^-T) mirrors this with the
+// transposed blocks L_ji^T and descending columns.  Each row is reduced by one CTA
+// in column order, so the sums follow a fixed order.  Publication: the owner
+// stores out_i, fences, and sets flags[i] = epoch; readers wait for that value
+// (bounded: on timeout *err = 2 and the CTA stops) and read out_j past L1.
+// Needs all CTAs resident at once (cooperative launch).
+constexpr uint64_t kSweepWaitNs = 2000000000ull;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t sweep_clock_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+template <int BSZ>
+__global__ void __launch_bounds__(kThreads) mixed_sweep_whole_kernel(const float* __restrict__ A,
+                                                                     const double* __restrict__ Y,
+                                                                     const double* __restrict__ in,
+                                                                     double* __restrict__ out, int nb, int forward,
+                                                                     unsigned epoch, unsigned* __restrict__ flags,
+                                                                     int* __restrict__ err) {
+    extern __shared__ double ssm[];
+    const int P = gridDim.x, c = blockIdx.x, tid = threadIdx.x;
+    const int nown = (nb - c + P - 1) / P;  // rows c + P q, q < nown
+    double* smem = ssm;                     // 8 BSZ: BlockApply
+    double* xs = smem + 8 * BSZ;            // the published block of out
+    double* tmp = xs + BSZ;                 // one block product
+    double* wk = tmp + BSZ;                 // nown rows of running right-hand side
+    __shared__ int s_stop;
+    const size_t bb = (size_t)BSZ * BSZ;
+    for (int q = 0; q < nown; ++q)
+        for (int r = tid; r < BSZ; r += blockDim.x) wk[q * BSZ + r] = in[(size_t)(c + P * q) * BSZ + r];
+    if (tid == 0) s_stop = 0;
+    __syncthreads();
+
+    // the owner's diagonal solve of row i (running right-hand side in wk row q)
+    auto solve = [&](int i, int q) {
+        const double* Yi = Y + (size_t)i * bb;
+        if (forward)
+            BlockApply<BSZ, double>::run(Yi, nullptr, wk + q * BSZ, nullptr, out + (size_t)i * BSZ, 2, smem);
+        else
+            BlockApply<BSZ, double>::run(Yi, wk + q * BSZ, nullptr, out + (size_t)i * BSZ, nullptr, 1, smem);
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_release_u32(flags + i, epoch);
+        }
+    };
+    // wk row q -= (block (r, cc) or its transpose) xs
+    auto update = [&](int r, int cc, int q) {
+        const float* M = A + (size_t)block_id(r, cc, nb) * bb;
+        if (forward)
+            BlockApply<BSZ, float>::run(M, xs, nullptr, tmp, nullptr, 1, smem);
+        else
+            BlockApply<BSZ, float>::run(M, nullptr, xs, nullptr, tmp, 2, smem);
+        __syncthreads();
+        for (int e = tid; e < BSZ; e += blockDim.x) wk[q * BSZ + e] -= tmp[e];
+        __syncthreads();
+    };
+
+    // Greedy order: act on the CTA's smallest open row (forward; largest backward)
+    // that can progress: apply its next column once published, or solve it once
+    // every column is in.  Columns are published in order, so `known` (the last
+    // column seen published) settles most checks without a load.
+    int* nextc = reinterpret_cast<int*>(wk + nown * BSZ);  // per owned row: next column to apply
+    __shared__ int s_pick, s_col, s_known, s_xs;
+    if (tid == 0) {
+        for (int q = 0; q < nown; ++q) nextc[q] = forward ? 0 : nb - 1;
+        s_known = 0;  // columns seen published (forward: 0 .. known-1; backward: nb-known .. nb-1)
+        s_xs = -1;
+    }
+    __syncthreads();
+    int solved = 0;
+    while (solved < nown) {
+        if (tid == 0) {
+            int pick = -1, col = -1;
+            for (;;) {
+                bool open = false;
+                for (int qq = 0; qq < nown; ++qq) {
+                    const int q = forward ? qq : nown - 1 - qq;
+                    const int i = c + P * q;
+                    const int jn = nextc[q];
+                    if (jn < 0) continue;  // solved
+                    open = true;
+                    if (jn == i) {  // every column applied
+                        pick = q;
+                        col = -2;
+                        break;
+                    }
+                    if (forward ? (jn < s_known) : (jn > nb - 1 - s_known)) {
+                        pick = q;
+                        col = jn;
+                        break;
+                    }
+                }
+                if (pick >= 0 || !open) break;
+                // nothing to do: wait (bounded) for the next column in publication order
+                const int jw = forward ? s_known : nb - 1 - s_known;
+                const uint64_t deadline = sweep_clock_ns() + kSweepWaitNs;
+                while (ld_acquire_u32(flags + jw) != epoch) {
+                    if (sweep_clock_ns() > deadline || *reinterpret_cast<volatile int*>(err) != 0) {
+                        atomicExch(err, 2);
+                        s_stop = 1;
+                        break;
+                    }
+                }
+                if (s_stop) break;
+                ++s_known;
+            }
+            s_pick = pick;
+            s_col = col;
+        }
+        __syncthreads();
+        if (s_stop || s_pick < 0) break;
+        const int q = s_pick, i = c + P * q, j = s_col;
+        if (j == -2) {
+            solve(i, q);
+            if (tid == 0) nextc[q] = -1;
+            ++solved;
+            __syncthreads();
+            continue;
+        }
+        if (s_xs != j) {
+            for (int e = tid; e < BSZ; e += blockDim.x) xs[e] = __ldcg(out + (size_t)j * BSZ + e);
+            __syncthreads();
+            if (tid == 0) s_xs = j;
+        }
+        if (forward) update(i, j, q);
+        else update(j, i, q);
+        if (tid == 0) nextc[q] = forward ? j + 1 : j - 1;
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ TRSV
 // Blocked substitution on one diagonal block: 32-row chunks, warp 0 solves the
 // chunk's triangle (column oriented, as the reference), all warps then apply
@@ -666,6 +811,36 @@ hs_status launch_mixed_sweep(hs_ctx ctx, const float* A32, const double* Y, doub
     HS_CHECK_LAUNCH("mixed_sweep");
     prof_end(ctx, s, HS_KERNEL_COLUPD, 2.0 * (others + 2) * (double)bsz * bsz,
              (double)(others + 1) * bsz * bsz * 4.0 + (double)bsz * bsz * 8.0 + 24.0 * (others + 1) * bsz);
+    return HS_OK;
+}
+
+hs_status launch_mixed_sweep_whole(hs_ctx ctx, const float* A32, const double* Y, const double* in, double* out,
+                                   int forward, unsigned epoch, unsigned* flags, int* err, cudaStream_t s) {
+    const int bsz = ctx->bsz, nb = ctx->nb;
+    HS_REQUIRE(bsz == 128 || bsz == 256, "the mixed sweep supports matrixBlockSize 128 or 256");
+    int dev = 0, per_sm = 0;
+    HS_CUDA(cudaGetDevice(&dev));
+    const void* fn = bsz == 256 ? (const void*)mixed_sweep_whole_kernel<256> : (const void*)mixed_sweep_whole_kernel<128>;
+    // rows per CTA for the grid used (at least one row each); shared memory for them
+    auto smem_for = [&](int grid) {
+        const int nown = (nb + grid - 1) / grid;
+        return (size_t)(10 + nown) * bsz * sizeof(double) + (size_t)nown * sizeof(int);
+    };
+    int grid = nb < 2 * ctx->num_sms ? nb : 2 * ctx->num_sms;
+    HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem_for(grid)));
+    if (grid > per_sm * ctx->num_sms) grid = per_sm * ctx->num_sms;
+    HS_REQUIRE(grid >= 1, "the mixed sweep does not fit on the device");
+    const size_t smem = smem_for(grid);
+    HS_REQUIRE(smem <= 200 * 1024, "matrix too large for the single-launch mixed sweep");
+    if (smem > 48 * 1024) HS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    void* args[] = {(void*)&A32, (void*)&Y, (void*)&in, (void*)&out, (void*)&nb, (void*)&forward,
+                    (void*)&epoch, (void*)&flags, (void*)&err};
+    prof_begin(ctx, s, HS_KERNEL_COLUPD);
+    ctx->launches += 1;
+    HS_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, s));
+    const double T = (double)nb * (nb - 1) / 2.0;
+    prof_end(ctx, s, HS_KERNEL_COLUPD, 2.0 * (T + nb) * bsz * bsz, (T * 4.0 + nb * 8.0) * bsz * bsz);
+    (void)dev;
     return HS_OK;
 }
 
