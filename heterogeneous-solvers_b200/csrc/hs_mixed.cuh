@@ -41,9 +41,6 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
 // TRSM of `items` bsz x bsz FP64 blocks stored contiguously at B against the
 // lower triangle L (bsz x bsz): B <- B L^-T
 hs_status launch_trsm_on(hs_ctx ctx, const double* L, int n, double* B, int items, cudaStream_t s);
-// one launch of a forward / backward sweep with the mixed factor (k_vector.cu)
-hs_status launch_mixed_sweep(hs_ctx ctx, const float* A32, const double* Y, double* work, double* out, int j,
-                             int forward, cudaStream_t s);
 // a whole forward / backward sweep in one cooperative launch: out = L^-1 in or
 // L^-T in (block rows published through flags[] with value `epoch`; *err = 2 on a
 // wait that timed out)

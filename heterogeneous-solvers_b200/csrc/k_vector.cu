@@ -355,92 +355,6 @@ __global__ void __launch_bounds__(kThreads) column_update_f32_kernel(const float
     for (int r = threadIdx.x; r < BSZ; r += blockDim.x) bi[r] -= out[r];
 }
 
-// One launch of a triangular sweep with the mixed-precision factor: FP32
-// off-diagonal blocks, FP64 inverse diagonal blocks Y_i = L_ii^-T.  `work` is
-// the right-hand side being reduced in place, `out` receives the solved blocks.
-// forward, column j: the first kSweepDiag CTAs form t = work_{j+1} - L_{j+1,j} out_j
-// (each CTA the whole of t) and each writes a quarter of out_{j+1} = Y_{j+1}^T t;
-// the other CTAs update work_i -= L_ij out_j for i = j+2..nb-1.  j = -1 only
-// solves block 0 (t = work_0).
-// backward, column j: the diagonal CTAs form t = work_{j-1} - L_{j,j-1}^T out_j
-// and write out_{j-1} = Y_{j-1} t; the others update work_i -= L_ji^T out_j for
-// i < j-1.  j = nb only solves block nb-1.
-constexpr int kSweepDiag = 4;
-
-template <int BSZ>
-__global__ void __launch_bounds__(kThreads) mixed_sweep_kernel(const float* __restrict__ A, const double* __restrict__ Y,
-                                                               double* __restrict__ work, double* __restrict__ out,
-                                                               int nb, int j, int forward) {
-    __shared__ double smem[8 * BSZ];
-    __shared__ double tv[BSZ];
-    __shared__ double red[kThreads];
-    const size_t bb = (size_t)BSZ * BSZ;
-    const int g = blockIdx.x;
-    if (g >= kSweepDiag) {
-        // off-diagonal update of one block row
-        const int gg = g - kSweepDiag;
-        if (forward) {
-            const int i = j + 2 + gg;
-            BlockApply<BSZ, float>::run(A + (size_t)block_id(i, j, nb) * bb, out + (size_t)j * BSZ, nullptr, tv,
-                                        nullptr, 1, smem);
-            __syncthreads();
-            for (int r = threadIdx.x; r < BSZ; r += blockDim.x) work[(size_t)i * BSZ + r] -= tv[r];
-        } else {
-            const int i = gg;
-            BlockApply<BSZ, float>::run(A + (size_t)block_id(j, i, nb) * bb, nullptr, out + (size_t)j * BSZ, nullptr,
-                                        tv, 2, smem);
-            __syncthreads();
-            for (int r = threadIdx.x; r < BSZ; r += blockDim.x) work[(size_t)i * BSZ + r] -= tv[r];
-        }
-        return;
-    }
-    // diagonal CTA: t for the block that becomes final, then a quarter of its solve
-    const int i = forward ? j + 1 : (j == nb ? nb - 1 : j - 1);
-    const bool update = forward ? (j >= 0) : (j < nb);
-    if (update) {
-        if (forward)
-            BlockApply<BSZ, float>::run(A + (size_t)block_id(i, j, nb) * bb, out + (size_t)j * BSZ, nullptr, tv,
-                                        nullptr, 1, smem);
-        else
-            BlockApply<BSZ, float>::run(A + (size_t)block_id(j, i, nb) * bb, nullptr, out + (size_t)j * BSZ, nullptr,
-                                        tv, 2, smem);
-        __syncthreads();
-        for (int r = threadIdx.x; r < BSZ; r += blockDim.x) tv[r] = work[(size_t)i * BSZ + r] - tv[r];
-    } else {
-        for (int r = threadIdx.x; r < BSZ; r += blockDim.x) tv[r] = work[(size_t)i * BSZ + r];
-    }
-    __syncthreads();
-    const double* Yi = Y + (size_t)i * bb;
-    constexpr int kSlice = BSZ / kSweepDiag;     // outputs of this CTA
-    constexpr int kGroups = kThreads / kSlice;   // row groups summed separately
-    const int c0 = g * kSlice;
-    const int lc = threadIdx.x % kSlice, grp = threadIdx.x / kSlice;
-    if (forward) {
-        // out[c] = sum_r Y[r][c] t[r], c in the slice: rows r = grp, grp + kGroups, ...
-        // (consecutive threads read consecutive columns of a row)
-        double acc = 0.0;
-        for (int r = grp; r < BSZ; r += kGroups) acc = fma(Yi[(size_t)r * BSZ + c0 + lc], tv[r], acc);
-        red[threadIdx.x] = acc;
-        __syncthreads();
-        if (threadIdx.x < kSlice) {
-            double v = 0.0;
-            for (int q = 0; q < kGroups; ++q) v += red[q * kSlice + threadIdx.x];
-            out[(size_t)i * BSZ + c0 + threadIdx.x] = v;
-        }
-    } else {
-        // out[r] = sum_c Y[r][c] t[c], r in the slice: one warp per row, lanes over c
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        for (int r = c0 + warp; r < c0 + kSlice; r += kThreads / 32) {
-            const double* row = Yi + (size_t)r * BSZ;
-            double acc = 0.0;
-#pragma unroll
-            for (int c = lane; c < BSZ; c += 32) acc = fma(row[c], tv[c], acc);
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane == 0) out[(size_t)i * BSZ + r] = acc;
-        }
-    }
-}
-
 // Whole sweep in one launch.  CTA c owns block rows i = c, c + P, ... (P = grid)
 // and keeps their running right-hand sides in shared memory.  Forward (t = L^-1 b):
 // row i takes L_ij out_j off for j = 0 .. i-1 in that order, then its owner solves
@@ -789,28 +703,6 @@ hs_status launch_column_update(hs_ctx ctx, const double* A, double* b, int block
     HS_CHECK_LAUNCH("column_update");
     prof_end(ctx, s, HS_KERNEL_COLUPD, 2.0 * blockCount * (double)bsz * bsz,
              (double)blockCount * bsz * bsz * 8.0 + 24.0 * blockCount * bsz);
-    return HS_OK;
-}
-
-hs_status launch_mixed_sweep(hs_ctx ctx, const float* A32, const double* Y, double* work, double* out, int j,
-                             int forward, cudaStream_t s) {
-    const int bsz = ctx->bsz, nb = ctx->nb;
-    HS_REQUIRE(bsz == 128 || bsz == 256, "the mixed sweep supports matrixBlockSize 128 or 256");
-    int others;  // off-diagonal block rows updated besides the one solved
-    if (forward) others = (j < 0) ? 0 : nb - j - 2;
-    else others = (j >= nb) ? 0 : j - 1;
-    if (others < 0) others = 0;
-    if (forward ? (j >= nb - 1) : (j <= 0)) return HS_OK;
-    const int grid = kSweepDiag + others;
-    prof_begin(ctx, s, HS_KERNEL_COLUPD);
-    ctx->launches += 1;
-    if (bsz == 256)
-        mixed_sweep_kernel<256><<<grid, kThreads, 0, s>>>(A32, Y, work, out, nb, j, forward);
-    else
-        mixed_sweep_kernel<128><<<grid, kThreads, 0, s>>>(A32, Y, work, out, nb, j, forward);
-    HS_CHECK_LAUNCH("mixed_sweep");
-    prof_end(ctx, s, HS_KERNEL_COLUPD, 2.0 * (others + 2) * (double)bsz * bsz,
-             (double)(others + 1) * bsz * bsz * 4.0 + (double)bsz * bsz * 8.0 + 24.0 * (others + 1) * bsz);
     return HS_OK;
 }
 
