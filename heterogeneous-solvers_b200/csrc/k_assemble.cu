@@ -76,6 +76,79 @@ __global__ void __launch_bounds__(256) rbf_assemble_kernel(double* __restrict__ 
     }
 }
 
+// The same entries, 4 x 4 per thread (bsz a multiple of 4 with bsz / 4 dividing
+// 256): each X value read from shared memory serves four entries, which takes the
+// kernel off the shared-memory bandwidth it was bound by with two entries a thread.
+// Thread t takes columns 4 (t % G) .. +3 (G = bsz / 4 column groups) and rows
+// 4 (t / G) + R p .. +3 in pass p (R = 4 * 256 / G rows a pass); a warp shares its
+// rows (broadcast reads) and writes 32 x 32 contiguous bytes per row.  Per entry the
+// distance is summed over k ascending exactly as in rbf_assemble_kernel.
+__global__ void __launch_bounds__(256) rbf_assemble_tile_kernel(double* __restrict__ A,
+                                                                const double* __restrict__ X, int64_t N, int d,
+                                                                int bsz, int nb, int ard,
+                                                                const double* __restrict__ wsc, double sf2,
+                                                                double sn2, double iso_scale) {
+    extern __shared__ double sm[];
+    double* Xi = sm;                      // bsz x d
+    double* XjT = sm + (size_t)bsz * d;   // d x bsz
+    __shared__ double w[kMaxD];
+    int ib, jb;
+    block_coords(blockIdx.x, nb, &ib, &jb);
+    const int64_t i0 = (int64_t)ib * bsz, j0 = (int64_t)jb * bsz;
+    for (int e = threadIdx.x; e < bsz * d; e += blockDim.x) {
+        const int r = e / d, k = e % d;
+        Xi[e] = (i0 + r < N) ? X[(i0 + r) * d + k] : 0.0;
+        XjT[(size_t)k * bsz + r] = (j0 + r < N) ? X[(j0 + r) * d + k] : 0.0;
+    }
+    if (threadIdx.x < d) w[threadIdx.x] = ard ? wsc[threadIdx.x] : 1.0;
+    __syncthreads();
+    double* blk = A + (size_t)blockIdx.x * bsz * bsz;
+    const int G = bsz >> 2;
+    const int cg = threadIdx.x % G, rg = threadIdx.x / G;
+    const int rows_pass = 4 * (256 / G);
+    const int jl = 4 * cg;
+    for (int il0 = 4 * rg; il0 < bsz; il0 += rows_pass) {
+        double acc[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+        for (int k = 0; k < d; ++k) {
+            const double2 xa = *reinterpret_cast<const double2*>(XjT + (size_t)k * bsz + jl);
+            const double2 xb = *reinterpret_cast<const double2*>(XjT + (size_t)k * bsz + jl + 2);
+            const double xj[4] = {xa.x, xa.y, xb.x, xb.y};
+            const double wk = w[k];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const double xi = Xi[(size_t)(il0 + r) * d + k];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const double t = ard ? (xi - xj[c]) * wk : xi - xj[c];
+                    acc[r][c] += t * t;
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int64_t ig = i0 + il0 + r;
+            double v[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int64_t jg = j0 + jl + c;
+                double e = 0.0;
+                if (ig < N && jg < N) {
+                    e = sf2 * exp(ard ? -0.5 * acc[r][c] : iso_scale * acc[r][c]);
+                    if (ig == jg) e += sn2;
+                }
+                v[c] = e;
+            }
+            double* o = blk + (size_t)(il0 + r) * bsz + jl;
+            __stcs(reinterpret_cast<double2*>(o), make_double2(v[0], v[1]));
+            __stcs(reinterpret_cast<double2*>(o + 2), make_double2(v[2], v[3]));
+        }
+    }
+}
+
 // odd block sizes (tests only): one entry per thread, plain stores
 __global__ void rbf_assemble_odd_kernel(double* __restrict__ A, const double* __restrict__ X, int64_t N, int d,
                                         int bsz, int nb, int ard, const double* __restrict__ wsc, double sf2,
@@ -130,7 +203,13 @@ hs_status launch_rbf_assemble(hs_ctx ctx, double* A, const double* X, int d, con
     const size_t smem = (size_t)2 * bsz * d * sizeof(double);
     prof_begin(ctx, s, HS_KERNEL_ASSEMBLE);
     ctx->launches += 1;
-    if (bsz % 2 == 0 && smem <= 200 * 1024) {
+    if (bsz % 4 == 0 && 256 % (bsz / 4) == 0 && smem <= 200 * 1024) {
+        if (smem > 48 * 1024)
+            HS_CUDA(cudaFuncSetAttribute(rbf_assemble_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+        rbf_assemble_tile_kernel<<<(unsigned)T, 256, smem, s>>>(A, X, ctx->N, d, bsz, nb, ard, wdev, sf2, sn2,
+                                                                iso_scale);
+    } else if (bsz % 2 == 0 && smem <= 200 * 1024) {
         if (smem > 48 * 1024)
             HS_CUDA(cudaFuncSetAttribute(rbf_assemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         rbf_assemble_kernel<<<(unsigned)T, 256, smem, s>>>(A, X, ctx->N, d, bsz, nb, ard, wdev, sf2, sn2, iso_scale);
