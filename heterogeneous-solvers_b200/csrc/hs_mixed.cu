@@ -67,26 +67,6 @@ __global__ void sum_pairs_kernel(const double* __restrict__ part, int n, double*
     }
 }
 
-// squared Frobenius norm of the packed symmetric matrix (off-diagonal blocks twice)
-__global__ void fro2_kernel(const double* __restrict__ A, int bsz, int nb, int64_t T, double* __restrict__ part) {
-    __shared__ double sh[32];
-    double acc = 0.0;
-    const int64_t bb = (int64_t)bsz * bsz;
-    for (int64_t blk = blockIdx.x; blk < T; blk += gridDim.x) {
-        int bi, bj;
-        block_coords(blk, nb, &bi, &bj);
-        const double w = (bi == bj) ? 1.0 : 2.0;
-        double s = 0.0;
-        for (int64_t e = threadIdx.x; e < bb; e += blockDim.x) {
-            const double v = A[blk * bb + e];
-            s += v * v;
-        }
-        acc += w * s;
-    }
-    const double t = cta_sum2(acc, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = t;
-}
-
 __global__ void sum_kernel(const double* __restrict__ part, int n, double* __restrict__ out) {
     __shared__ double sh[32];
     double a = 0.0;
@@ -203,18 +183,6 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     Events ev;
     for (auto& e : ev.e) HS_CUDA(cudaEventCreate(&e));
 
-    // ||K||_F
-    {
-        const int64_t T = total_blocks(nb);
-        const int fg = (int)(T < 1024 ? T : 1024);
-        ctx->launches += 2;
-        fro2_kernel<<<fg, kThreads, 0, s>>>(K, bsz, nb, T, part);
-        sum_kernel<<<1, kThreads, 0, s>>>(part, fg, scal);
-        HS_CHECK_LAUNCH("fro2");
-        HS_CUDA(cudaMemcpyAsync((void*)(h + 8), scal, sizeof(double), cudaMemcpyDeviceToHost, s));
-        HS_CUDA(cudaStreamSynchronize(s));
-        R.norm_k_fro = std::sqrt(h[8]);
-    }
     // factor (a non-positive FP64 pivot of the FP32 matrix is recorded in ctx->d_info);
     // on breakdown, factor K + shift*I with a growing shift and use it as a CG preconditioner
     double shift = 0.0;
@@ -223,7 +191,8 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     for (int attempt = 1;; ++attempt) {
         ctx->launches += 1;
         set_i64_dev(ctx->d_info, INT64_MAX, s);
-        st = mixed_factor(ctx, K, w, s, shift, prec);
+        // the first attempt's conversion to FP32 also sums ||K||_F^2
+        st = mixed_factor(ctx, K, w, s, shift, prec, attempt == 1 ? part : nullptr);
         if (st != HS_OK) return st;
         HS_CUDA(cudaStreamSynchronize(s));
         if (ctx->side) HS_CUDA(cudaStreamSynchronize(ctx->side));
@@ -255,6 +224,15 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
         } else {
             shift *= 10.0;  // 1e-6 .. 1e-1 x the largest diagonal entry
         }
+    }
+    {
+        const int fg = mixed_fro_grid(total_blocks(nb));
+        ctx->launches += 1;
+        sum_kernel<<<1, kThreads, 0, s>>>(part, fg, scal);
+        HS_CHECK_LAUNCH("fro2");
+        HS_CUDA(cudaMemcpyAsync((void*)(h + 8), scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        HS_CUDA(cudaStreamSynchronize(s));
+        R.norm_k_fro = std::sqrt(h[8]);
     }
     HS_CUDA(cudaEventRecord(ev.e[1], s));
     // log|K| from the FP64 diagonal blocks

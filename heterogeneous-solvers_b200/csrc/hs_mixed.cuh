@@ -29,8 +29,11 @@ struct MixedWork {
 size_t mixed_workspace_bytes(int64_t N, int bsz);
 hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w);
 // shift != 0: factor K + shift*I
+// fro_part (non-null): also the squared Frobenius norm of K (off-diagonal blocks twice)
+// as mixed_fro_grid(blocks) CTA partials
 hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift = 0.0,
-                       int precision = HS_PRECISION_TF32X3);
+                       int precision = HS_PRECISION_TF32X3, double* fro_part = nullptr);
+int mixed_fro_grid(int64_t blocks);
 hs_status mixed_check_error(hs_ctx ctx, const MixedWork& w);
 // b <- (L L^T)^-1 b with the mixed factor (tmp: intermediate)
 hs_status mixed_apply(hs_ctx ctx, MixedWork& w, double* b, double* tmp, cudaStream_t s);

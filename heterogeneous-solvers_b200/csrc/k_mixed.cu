@@ -536,6 +536,45 @@ __global__ void f64_to_f32_kernel(const double* __restrict__ in, float* __restri
     if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) out[n - 1] = (float)in[n - 1];
 }
 
+// sum over the CTA (fixed order: warps by shuffle butterfly, then warp 0 in order);
+// the total is valid in thread 0
+__device__ __forceinline__ double cta_total(double v, double* sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int wp = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[wp] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += sh[i];
+    return t;
+}
+
+// the same conversion a stored block at a time, with the squared Frobenius norm of
+// the symmetric matrix (off-diagonal blocks twice) summed on the way: CTA partials
+// in part[blockIdx.x], blocks in a fixed order, so the norm is reproducible
+__global__ void f64_to_f32_fro2_kernel(const double* __restrict__ in, float* __restrict__ out, int bsz, int nb,
+                                       int64_t T, double* __restrict__ part) {
+    __shared__ double sh[32];
+    double acc = 0.0;
+    const int64_t bb2 = (int64_t)bsz * bsz / 2;
+    for (int64_t blk = blockIdx.x; blk < T; blk += gridDim.x) {
+        int bi, bj;
+        block_coords(blk, nb, &bi, &bj);
+        const double2* src = reinterpret_cast<const double2*>(in) + blk * bb2;
+        float2* dst = reinterpret_cast<float2*>(out) + blk * bb2;
+        double sq = 0.0;
+        for (int64_t e = threadIdx.x; e < bb2; e += blockDim.x) {
+            const double2 v = __ldcs(src + e);
+            dst[e] = make_float2((float)v.x, (float)v.y);
+            sq += v.x * v.x;
+            sq += v.y * v.y;
+        }
+        acc += ((bi == bj) ? 1.0 : 2.0) * sq;
+    }
+    const double t = cta_total(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
 // BF16 split of the panel: P[i] = bf16(x), P[lo_off + i] = bf16(x - P[i]) (round to nearest)
 __global__ void panel_split_bf16_kernel(const float* __restrict__ x, __nv_bfloat16* __restrict__ P, int64_t n,
                                         int64_t lo_off) {
@@ -1068,7 +1107,10 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
     return st;
 }
 
-hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift, int precision) {
+int mixed_fro_grid(int64_t blocks) { return (int)(blocks < 1024 ? blocks : 1024); }
+
+hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift, int precision,
+                       double* fro_part) {
     const int bsz = ctx->bsz, nb = ctx->nb;
     HS_REQUIRE(bsz == 128 || bsz == 256, "the mixed-precision factor supports matrixBlockSize 128 or 256");
     hs_status st = bsz == 256 ? tc_attrs<256>() : tc_attrs<128>();
@@ -1077,7 +1119,11 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
     const int64_t T = total_blocks(nb);
     ctx->launches += 2;
     set_int_kernel<<<1, 1, 0, s>>>(w.err, 0);
-    f64_to_f32_kernel<<<grid_for_elems(T * (int64_t)bb / 2, ctx->num_sms), 256, 0, s>>>(K64, w.A32, T * (int64_t)bb);
+    if (fro_part && bsz % 2 == 0)
+        f64_to_f32_fro2_kernel<<<mixed_fro_grid(T), 256, 0, s>>>(K64, w.A32, bsz, nb, T, fro_part);
+    else
+        f64_to_f32_kernel<<<grid_for_elems(T * (int64_t)bb / 2, ctx->num_sms), 256, 0, s>>>(K64, w.A32,
+                                                                                          T * (int64_t)bb);
     HS_CHECK_LAUNCH("f64_to_f32");
     if (shift != 0.0) {
         ctx->launches += 1;
