@@ -261,6 +261,7 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     double rn = 0, xn = 0, prev = INFINITY;
     bool converged = false;
     int steps = 0;
+    bool r_fresh = false;  // r holds b - K x for the current x
     // a shifted factor is only a preconditioner: no refinement, straight to CG
     const int ref_steps = shift > 0.0 ? 0 : max_steps;
     for (; steps < ref_steps; ++steps) {
@@ -274,7 +275,10 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
         }
         // a step that shrinks the residual by less than 8x means a poor contraction:
         // conjugate gradients with the same preconditioner converges faster from here
-        if (rn > 0.125 * prev) break;
+        if (rn > 0.125 * prev) {
+            r_fresh = true;
+            break;
+        }
         prev = rn;
         // d = M^-1 r; x += d
         HS_CUDA(cudaMemcpyAsync(d, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -288,8 +292,10 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     if (!converged) {
         // conjugate gradients preconditioned by the low-precision factor, from the current x
         R.fallback_pcg = 1;
-        st = residual(&rn, &xn);  // r = b - K x
-        if (st != HS_OK) return st;
+        if (!r_fresh) {
+            st = residual(&rn, &xn);  // r = b - K x
+            if (st != HS_OK) return st;
+        }
         if (steps == 0) R.initial_backward_error = rn / (R.norm_k_fro * xn);
         HS_CUDA(cudaMemcpyAsync(z, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         st = mixed_apply(ctx, w, z, tmp, s);
@@ -310,7 +316,8 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
             const double alpha = rho / h[13];
             if ((st = launch_vec(ctx, 3, x, p, alpha, x, 0, n, s)) != HS_OK) return st;
             if ((st = launch_vec(ctx, 3, r, q, -alpha, r, 0, n, s)) != HS_OK) return st;
-            if ((it + 1) % 10 == 0) {
+            const bool true_res = (it + 1) % 10 == 0;
+            if (true_res) {
                 st = residual(&rn, &xn);  // true residual keeps r honest
                 if (st != HS_OK) return st;
             } else {
@@ -323,10 +330,12 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
             }
             R.backward_error = rn / (R.norm_k_fro * xn);
             if (R.backward_error <= tol) {
-                // confirm with the true residual before stopping
-                st = residual(&rn, &xn);
-                if (st != HS_OK) return st;
-                R.backward_error = rn / (R.norm_k_fro * xn);
+                // confirm with the true residual before stopping (unless it is the true one)
+                if (!true_res) {
+                    st = residual(&rn, &xn);
+                    if (st != HS_OK) return st;
+                    R.backward_error = rn / (R.norm_k_fro * xn);
+                }
                 if (R.backward_error <= tol) {
                     converged = true;
                     ++it;

@@ -232,7 +232,7 @@ __device__ __forceinline__ void block_apply(const double* M, int bsz, const doub
 // grid: one CTA per sub-rectangle position (I, J); the CTA owning the stored
 // block computes every part of it the rectangle needs.
 template <int BSZ>
-__global__ void __launch_bounds__(kThreads) symv_partials(const double* __restrict__ A, const double* __restrict__ b,
+__global__ void __launch_bounds__(kThreads, 2) symv_partials(const double* __restrict__ A, const double* __restrict__ b,
                                                           double* __restrict__ P, int bsz, int nb, int bi0,
                                                           int bj0, int nbi, int nbj) {
     __shared__ double smem[(BSZ > 0 ? 8 * BSZ : 1)];
