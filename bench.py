@@ -73,6 +73,11 @@ def parse_args():
     ap.add_argument("--sweep", action="store_true",
                     help="conditioning sweep: mixed vs FP64 solve for sn2 in {1e-1, 1e-3, 1e-6} (one JSON line)")
     ap.add_argument("--lml-steps", type=int, default=3)
+    ap.add_argument("--fit", action="store_true",
+                    help="hyperparameter fit: L-BFGS on the FP64 NLML + gradient (ARD RBF, d=8) at --fit-n, "
+                         "--fit-steps iterations (one JSON line)")
+    ap.add_argument("--fit-n", type=int, default=65536)
+    ap.add_argument("--fit-steps", type=int, default=30)
     return ap.parse_args()
 
 
@@ -245,6 +250,32 @@ def bench_lml(hs, torch, device, N, steps):
             "useful_tflops_whole": (N ** 3 / 3 + 2 * N ** 3 / 3) / (t_ms * 1e-3) / 1e12}
 
 
+def run_fit(hs, torch, device, N, steps):
+    """Hyperparameter fit of an ARD RBF GP by L-BFGS (hs.fit_hyperparameters: scipy's
+    L-BFGS-B over the library's FP64 NLML and analytic gradient): X ~ U[0,1]^(N x 8),
+    y = sin(sum_k x_k) + N(0, 0.1^2), theta0 = [log l_k = 0, log sf2 = 0, log sn2 = log 1e-2],
+    at most `steps` iterations.  Wall time of the whole fit and of every NLML + gradient."""
+    import numpy as np
+    d, bsz = 8, 256
+    rng = np.random.default_rng(5)
+    X = rng.random((N, d))
+    y = np.sin(X.sum(axis=1)) + 0.1 * rng.standard_normal(N)
+    theta0 = np.concatenate([np.zeros(d), [0.0, np.log(1e-2)]])
+    c = hs.Context(device=device, N=N, matrixBlockSize=bsz)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = hs.fit_hyperparameters(c, X, y, theta0, maxiter=steps)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    c.close()
+    ev = np.asarray(res["eval_seconds"])
+    return {"workload": f"L-BFGS hyperparameter fit, ARD RBF, N={N}, d={d}, bsz={bsz}, FP64 NLML + gradient",
+            "max_iterations": steps, "iterations": res["iterations"], "evaluations": res["evaluations"],
+            "fit_seconds": wall, "eval_seconds_median": float(np.median(ev)), "eval_seconds_max": float(ev.max()),
+            "nlml_initial": res["nlml_trace"][0], "nlml_final": res["nlml"],
+            "theta_final": [float(v) for v in res["theta"]], "message": res["message"]}
+
+
 def run_sweep(args, hs, torch, ctx, Xd, bd, A, N, cfg, device):
     """Mixed (3xTF32 factor + FP64 refinement / PCG) against FP64 factor + solve on the
     same RBF system for sn2 in {1e-1, 1e-3, 1e-6}: times, backward errors, refinement
@@ -335,6 +366,15 @@ def main():
     torch.cuda.set_device(device)
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", device))
+
+    if args.fit:
+        fit = run_fit(hs, torch, device, args.fit_n, args.fit_steps)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "mode": "hyperparameter fit", "n_gpus": world, "data": "synthetic",
+                              "fit": fit}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     cfg = dict(wl.CONFIGS[WORKLOAD])
     N = args.n or cfg["N"]
