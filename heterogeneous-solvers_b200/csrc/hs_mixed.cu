@@ -109,6 +109,14 @@ __global__ void maxdiag_kernel(const double* __restrict__ A, int bsz, int nb, in
     }
 }
 
+// out[i] = float(in[i]), n even
+__global__ void f64_to_f32_copy_kernel(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n / 2; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = reinterpret_cast<const double2*>(in)[i];
+        reinterpret_cast<float2*>(out)[i] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
 // x += d
 __global__ void add_kernel(double* __restrict__ x, const double* __restrict__ d, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -128,9 +136,9 @@ int grid_n(int64_t n, int sms) {
 // reads b and writes L^-1 b into tmp; the backward sweep reads tmp and writes the
 // result into b.
 hs_status mixed_apply(hs_ctx ctx, MixedWork& w, double* b, double* tmp, cudaStream_t s) {
-    hs_status st = launch_mixed_sweep_whole(ctx, w.A32, w.Yinv, b, tmp, 1, ++w.epoch, w.flags, w.err + 1, s);
+    hs_status st = launch_mixed_sweep_whole(ctx, w.A32, w.Y32, b, tmp, 1, ++w.epoch, w.flags, w.err + 1, s);
     if (st != HS_OK) return st;
-    return launch_mixed_sweep_whole(ctx, w.A32, w.Yinv, tmp, b, 0, ++w.epoch, w.flags, w.err + 1, s);
+    return launch_mixed_sweep_whole(ctx, w.A32, w.Y32, tmp, b, 0, ++w.epoch, w.flags, w.err + 1, s);
 }
 
 namespace {
@@ -225,6 +233,13 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
             shift *= 10.0;  // 1e-6 .. 1e-1 x the largest diagonal entry
         }
     }
+    // the sweeps read the inverse diagonal blocks in FP32 (their rounding is far below
+    // the factor's own error), from the BF16 panel area the factor no longer needs
+    w.Y32 = reinterpret_cast<float*>(w.P16);
+    ctx->launches += 1;
+    f64_to_f32_copy_kernel<<<grid_n((int64_t)nb * bsz * bsz / 2, ctx->num_sms), kThreads, 0, s>>>(
+        w.Yinv, w.Y32, (int64_t)nb * bsz * bsz);
+    HS_CHECK_LAUNCH("Y32");
     {
         const int fg = mixed_fro_grid(total_blocks(nb));
         ctx->launches += 1;

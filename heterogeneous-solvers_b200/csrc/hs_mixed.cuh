@@ -20,6 +20,7 @@ struct MixedWork {
     int* err = nullptr;     // [0] tensor-core tile timeout, [1] triangular-sweep timeout
     unsigned* flags = nullptr;  // per block row: epoch of the sweep that published it
     unsigned epoch = 0;         // last sweep launched (flags are cleared when it restarts at 0)
+    float* Y32 = nullptr;       // FP32 copy of Yinv for the sweeps, in the P16 area once the factor is done
     CUtensorMap mA128, mAB, mL128, mLB;  // 128-byte swizzle, 32-wide K boxes (TRSM)
     CUtensorMap mU128, mUB, mV128, mVB;  // K boxes of 128 bytes over A32 / LO (TF32 update)
     CUtensorMap mP128, mPB;              // K boxes of 128 bytes over P16 (BF16 update)
@@ -47,7 +48,7 @@ hs_status launch_trsm_on(hs_ctx ctx, const double* L, int n, double* B, int item
 // a whole forward / backward sweep in one cooperative launch: out = L^-1 in or
 // L^-T in (block rows published through flags[] with value `epoch`; *err = 2 on a
 // wait that timed out)
-hs_status launch_mixed_sweep_whole(hs_ctx ctx, const float* A32, const double* Y, const double* in, double* out,
+hs_status launch_mixed_sweep_whole(hs_ctx ctx, const float* A32, const float* Y, const double* in, double* out,
                                    int forward, unsigned epoch, unsigned* flags, int* err, cudaStream_t s);
 // column update reading FP32 blocks (accumulation in FP64)
 hs_status launch_column_update_f32(hs_ctx ctx, const float* A32, double* b, int blockStart, int blockCount,

@@ -382,7 +382,7 @@ __device__ __forceinline__ uint64_t sweep_clock_ns() {
 
 template <int BSZ>
 __global__ void __launch_bounds__(kThreads) mixed_sweep_whole_kernel(const float* __restrict__ A,
-                                                                     const double* __restrict__ Y,
+                                                                     const float* __restrict__ Y,
                                                                      const double* __restrict__ in,
                                                                      double* __restrict__ out, int nb, int forward,
                                                                      unsigned epoch, unsigned* __restrict__ flags,
@@ -403,11 +403,11 @@ __global__ void __launch_bounds__(kThreads) mixed_sweep_whole_kernel(const float
 
     // the owner's diagonal solve of row i (running right-hand side in wk row q)
     auto solve = [&](int i, int q) {
-        const double* Yi = Y + (size_t)i * bb;
+        const float* Yi = Y + (size_t)i * bb;
         if (forward)
-            BlockApply<BSZ, double>::run(Yi, nullptr, wk + q * BSZ, nullptr, out + (size_t)i * BSZ, 2, smem);
+            BlockApply<BSZ, float>::run(Yi, nullptr, wk + q * BSZ, nullptr, out + (size_t)i * BSZ, 2, smem);
         else
-            BlockApply<BSZ, double>::run(Yi, wk + q * BSZ, nullptr, out + (size_t)i * BSZ, nullptr, 1, smem);
+            BlockApply<BSZ, float>::run(Yi, wk + q * BSZ, nullptr, out + (size_t)i * BSZ, nullptr, 1, smem);
         __syncthreads();
         if (tid == 0) {
             __threadfence();
@@ -706,7 +706,7 @@ hs_status launch_column_update(hs_ctx ctx, const double* A, double* b, int block
     return HS_OK;
 }
 
-hs_status launch_mixed_sweep_whole(hs_ctx ctx, const float* A32, const double* Y, const double* in, double* out,
+hs_status launch_mixed_sweep_whole(hs_ctx ctx, const float* A32, const float* Y, const double* in, double* out,
                                    int forward, unsigned epoch, unsigned* flags, int* err, cudaStream_t s) {
     const int bsz = ctx->bsz, nb = ctx->nb;
     HS_REQUIRE(bsz == 128 || bsz == 256, "the mixed sweep supports matrixBlockSize 128 or 256");
