@@ -59,6 +59,10 @@ struct TcArgs {
     // at 2 p nb + r - (k + p) - 1, lo nb slots further)
     int npanels;
     int first_col;
+    // TRSM with BF16 split products downstream: the epilogue writes L's BF16 hi / lo
+    // split (P16 slots 2 lo_base + r - k - 1 and nb further) instead of its TF32 low part
+    __nv_bfloat16* P16;
+    int bf16;
 };
 
 // CTA-uniform early exit once a diagonal POTRF has recorded a non-positive pivot:
@@ -192,21 +196,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (lane == 0) atomicExch(a.err, 1);
     } else {
         const int row = warp * 32 + lane;
-        float* outp;
-        float* lop = nullptr;
-        if (MODE == MODE_TRSM) {
-            outp = a.A32 + (size_t)blkA * bb + (size_t)(ti * 128 + row) * BSZ;
-            lop = a.LO + (size_t)gA * bb + (size_t)(ti * 128 + row) * BSZ;
-        } else {
-            outp = a.A32 + (size_t)block_id(r, c, a.nb) * bb + (size_t)(ti * 128 + row) * BSZ;
-        }
+        float* outp = a.A32 + (size_t)block_id(r, c, a.nb) * bb + (size_t)(ti * 128 + row) * BSZ;  // MODE_UPDATE
 #pragma unroll 1
         for (int j = 0; j < BSZ / 32; ++j) {
             uint32_t v[32];
             tmem_ld_32x32b_x32(taddr + ((uint32_t)(warp * 32) << 16) + j * 32, v);
             tmem_ld_wait();
-            float4* o4 = reinterpret_cast<float4*>(outp + j * 32);
             if (MODE == MODE_UPDATE) {
+                float4* o4 = reinterpret_cast<float4*>(outp + j * 32);
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     float4 cv = o4[q];
@@ -217,15 +214,40 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     o4[q] = cv;
                 }
             } else {
-                float4* l4 = reinterpret_cast<float4*>(lop + j * 32);
+                // staged through this warp's 32 x 33 shared tile (the operand ring is
+                // free once the MMAs are done), then written as whole 128-byte row
+                // segments: 8 lanes a row, 4 rows an instruction
+                float* stg = reinterpret_cast<float*>(smem) + warp * 32 * 33;
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const float x0 = __uint_as_float(v[4 * q + 0]), x1 = __uint_as_float(v[4 * q + 1]);
-                    const float x2 = __uint_as_float(v[4 * q + 2]), x3 = __uint_as_float(v[4 * q + 3]);
-                    o4[q] = make_float4(x0, x1, x2, x3);
-                    l4[q] = make_float4(x0 - tf32_trunc(x0), x1 - tf32_trunc(x1), x2 - tf32_trunc(x2),
+                for (int q = 0; q < 32; ++q) stg[lane * 33 + q] = __uint_as_float(v[q]);
+                __syncwarp();
+                const int c4 = (lane & 7) * 4;
+#pragma unroll 2
+                for (int it = 0; it < 8; ++it) {
+                    const int rr = it * 4 + (lane >> 3);
+                    const float* sr = stg + rr * 33 + c4;
+                    const float x0 = sr[0], x1 = sr[1], x2 = sr[2], x3 = sr[3];
+                    const size_t off = (size_t)(ti * 128 + warp * 32 + rr) * BSZ + j * 32 + c4;
+                    *reinterpret_cast<float4*>(a.A32 + (size_t)blkA * bb + off) = make_float4(x0, x1, x2, x3);
+                    if (a.bf16) {
+                        const __nv_bfloat162 h01 = __floats2bfloat162_rn(x0, x1), h23 = __floats2bfloat162_rn(x2, x3);
+                        const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+                        const __nv_bfloat162 l01 = __floats2bfloat162_rn(x0 - f01.x, x1 - f01.y);
+                        const __nv_bfloat162 l23 = __floats2bfloat162_rn(x2 - f23.x, x3 - f23.y);
+                        __nv_bfloat16* ph = a.P16 + (size_t)(2 * a.lo_base + (r - a.k - 1)) * bb + off;
+                        __nv_bfloat162* h2 = reinterpret_cast<__nv_bfloat162*>(ph);
+                        __nv_bfloat162* l2 = reinterpret_cast<__nv_bfloat162*>(ph + (size_t)a.nb * bb);
+                        h2[0] = h01;
+                        h2[1] = h23;
+                        l2[0] = l01;
+                        l2[1] = l23;
+                    } else {
+                        *reinterpret_cast<float4*>(a.LO + (size_t)gA * bb + off) =
+                            make_float4(x0 - tf32_trunc(x0), x1 - tf32_trunc(x1), x2 - tf32_trunc(x2),
                                         x3 - tf32_trunc(x3));
+                    }
                 }
+                __syncwarp();
             }
         }
     }
@@ -574,18 +596,6 @@ __global__ void f64_to_f32_fro2_kernel(const double* __restrict__ in, float* __r
     }
     const double t = cta_total(acc, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = t;
-}
-
-// BF16 split of the panel: P[i] = bf16(x), P[lo_off + i] = bf16(x - P[i]) (round to nearest)
-__global__ void panel_split_bf16_kernel(const float* __restrict__ x, __nv_bfloat16* __restrict__ P, int64_t n,
-                                        int64_t lo_off) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n / 2; i += (int64_t)gridDim.x * blockDim.x) {
-        const float2 v = reinterpret_cast<const float2*>(x)[i];
-        const __nv_bfloat162 hi = __floats2bfloat162_rn(v.x, v.y);
-        const float2 hf = __bfloat1622float2(hi);
-        reinterpret_cast<__nv_bfloat162*>(P)[i] = hi;
-        reinterpret_cast<__nv_bfloat162*>(P + lo_off)[i] = __floats2bfloat162_rn(v.x - hf.x, v.y - hf.y);
-    }
 }
 
 // diagonal shift of the FP32 copy (valid rows only)
@@ -1187,16 +1197,13 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         a.blockID = blockID;
         a.k = k;
         a.lo_base = set * nb;
+        // BF16 products downstream: the TRSM writes L's BF16 split itself
+        a.bf16 = precision == HS_PRECISION_BF16X3 ? 1 : 0;
+        a.P16 = w.P16;
         prof_begin(ctx, s, HS_KERNEL_TRSM);
         hs_status r = bsz == 256 ? tc_launch<256>(ctx, MODE_TRSM, w, a, m, s) : tc_launch<128>(ctx, MODE_TRSM, w, a, m, s);
         if (r != HS_OK) return r;
         prof_end(ctx, s, HS_KERNEL_TRSM, (double)m * 2.0 * bsz * bb, 4.0 * m * bb * 4.0);
-        if (precision == HS_PRECISION_BF16X3) {
-            ctx->launches += 1;
-            panel_split_bf16_kernel<<<grid_for_elems((int64_t)m * bb / 2, ctx->num_sms), 256, 0, s>>>(
-                dblk + bb, w.P16 + (size_t)2 * set * nb * bb, (int64_t)m * bb, (int64_t)nb * bb);
-            HS_CHECK_LAUNCH("panel_split_bf16");
-        }
         return HS_OK;
     };
     // trailing update with panels k .. k + npanels - 1: part 1 = column c0, part 2 =
