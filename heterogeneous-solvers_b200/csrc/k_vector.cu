@@ -379,6 +379,21 @@ __device__ __forceinline__ uint64_t sweep_clock_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
+// hint: bring `bytes` (a multiple of 16) at p (16-byte aligned) into L2
+__device__ __forceinline__ void sweep_prefetch_l2(const void* p, uint32_t bytes) {
+    const char* b = static_cast<const char*>(p);
+    for (uint32_t off = 0; off < bytes; off += 65536u) {
+        const uint32_t n = bytes - off < 65536u ? bytes - off : 65536u;
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b + off), "r"(n) : "memory");
+    }
+}
+// The bulk of a sweep's block products streams past L2 (evict-first loads) while
+// most CTAs work at once, so a row's last two block products — the one with the
+// block next to the diagonal, once the previous row is published, then the one
+// with its inverse diagonal block — run on the chain at a CTA's share of a busy
+// HBM.  Their blocks are hinted into L2 when the owner applies the column
+// kSweepAhead before the diagonal, so the chain reads them from L2.
+constexpr int kSweepAhead = 4;
 
 template <int BSZ>
 __global__ void __launch_bounds__(kThreads) mixed_sweep_whole_kernel(const float* __restrict__ A,
@@ -477,6 +492,18 @@ __global__ void __launch_bounds__(kThreads) mixed_sweep_whole_kernel(const float
             }
             s_pick = pick;
             s_col = col;
+            if (pick >= 0 && col >= 0) {
+                // row i's chain blocks: link block (i, i-1) forward, (i+1, i) backward
+                // (both exist: a row takes column picks only when it has a link), and Y_i
+                const int i = c + P * pick;
+                const int first = forward ? (i > kSweepAhead ? i - kSweepAhead : 0)
+                                          : (i + kSweepAhead < nb - 1 ? i + kSweepAhead : nb - 1);
+                if (col == first) {
+                    const int lr = forward ? i : i + 1, lc = lr - 1;
+                    sweep_prefetch_l2(A + (size_t)block_id(lr, lc, nb) * bb, (uint32_t)(bb * sizeof(float)));
+                    sweep_prefetch_l2(Y + (size_t)i * bb, (uint32_t)(bb * sizeof(float)));
+                }
+            }
         }
         __syncthreads();
         if (s_stop || s_pick < 0) break;
