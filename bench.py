@@ -2,7 +2,8 @@
 """Benchmark of the blocked SPD solve path for GP kernel matrices.
 
 One step = RBF assembly of the packed kernel matrix from device-resident
-inputs and the mixed-precision solve (3xTF32 tensor-core factor with FP64
+inputs and the mixed-precision solve (tensor-core factor whose trailing
+updates take FP16 split products of the scaled panel, 3xTF32 TRSM, FP64
 diagonal POTRF, FP64 iterative refinement to backward error <= 1e-14), at
 N = 131072, d = 16, l = 1, sf2 = 1, sn2 = 1e-2, matrix_bsz = 256 (68.85 GB
 packed FP64 matrix, larger than L2, so no flush is needed between steps).
@@ -66,7 +67,7 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
     ap.add_argument("--tol", type=float, default=1e-14, help="backward-error target of the mixed solve")
-    ap.add_argument("--precision", choices=["tf32x3", "bf16x3"], default="bf16x3",
+    ap.add_argument("--precision", choices=["tf32x3", "bf16x3", "f16x3"], default="f16x3",
                     help="split products of the headline mixed factor's tensor-core updates (the other variant "
                          "is timed as a leg of the same run)")
     ap.add_argument("--lml-n", type=int, default=16384, help="N of the NLML+gradient leg (0: skip)")
@@ -472,7 +473,7 @@ def main():
     bwd_mixed = backward_error(x_mixed)
 
     # ---------------- the other split variant of the mixed form on the same system
-    other = "tf32x3" if args.precision == "bf16x3" else "bf16x3"
+    other = {"f16x3": "bf16x3", "bf16x3": "f16x3", "tf32x3": "f16x3"}[args.precision]
     alt = None
     if not args.no_fp64:
         orep = hs._lib.MixedReport()
@@ -603,11 +604,13 @@ def main():
             "cuBLAS TF32 GEMM 8192^3 measured in this run, divided by the 3 TF32 products of one split FP32 "
             "product (TF32 is absent from MEASURED_PEAKS.json)"), "issued_tf32_tflops"
     else:
+        # FP16 and BF16 products run at the same tensor-core rate (kind::f16)
         bf = peaks.get("bf16_tflops_sustained") or 1400.0
+        name = "BF16" if args.precision == "bf16x3" else "FP16"
         peak3, peak_src, issued_key = bf / 3.0, (
             ("MEASURED_PEAKS.json bf16_tflops_sustained" if peaks.get("bf16_tflops_sustained") else
-             "fallback 1.4 PFLOP/s sustained bf16") + ", divided by the 3 BF16 products of one split product"), \
-            "issued_bf16_tflops"
+             "fallback 1.4 PFLOP/s sustained bf16") + f", divided by the 3 {name} products of one split product"), \
+            f"issued_{args.precision[:-2]}_tflops"
     roof = {"bound": "tensor", "achieved": useful, "peak": peak3 if useful else None, "unit": "TFLOP/s",
             "frac": useful / peak3 if useful else None, "traffic": traffic,
             "kernel": f"tc_update_kernel<256, {args.precision}> (split-product SYRK+GEMM trailing update, tcgen05, "
@@ -631,13 +634,17 @@ def main():
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": ("f32 (3xTF32 tensor-core factor) + f64 refinement" if args.precision == "tf32x3" else
-                      "f32 (BF16-split tensor-core updates, 3xTF32 TRSM) + f64 refinement"),
+            "dtype": {"tf32x3": "f32 (3xTF32 tensor-core factor) + f64 refinement",
+                      "bf16x3": "f32 (BF16-split tensor-core updates, 3xTF32 TRSM) + f64 refinement",
+                      "f16x3": "f32 (scaled FP16-split tensor-core updates, 3xTF32 TRSM) + f64 refinement",
+                      }[args.precision],
             "data": f"synthetic: X~U[0,1]^({N}x{d}) seed {cfg['seed']}+rank, y=sin(sum_k x_k)+N(0,0.1^2)",
             "config": dict(bench_config(N, world), implementation=(
                 "RBF assembly + mixed-precision Cholesky (" +
-                ("3xTF32 tensor-core TRSM/SYRK/GEMM" if args.precision == "tf32x3" else
-                 "BF16-split tensor-core SYRK/GEMM, 3xTF32 tensor-core TRSM") +
+                {"tf32x3": "3xTF32 tensor-core TRSM/SYRK/GEMM",
+                 "bf16x3": "BF16-split tensor-core SYRK/GEMM, 3xTF32 tensor-core TRSM",
+                 "f16x3": "FP16-split (panel scaled by a power of two) tensor-core SYRK/GEMM, 3xTF32 tensor-core "
+                          "TRSM"}[args.precision] +
                 f", FP64 POTRF) + FP64 iterative refinement / preconditioned CG to backward error <= {args.tol:g}")),
             "roofline": roof,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,

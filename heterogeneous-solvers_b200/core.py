@@ -28,7 +28,7 @@ __all__ = [
 ]
 
 # hs_precision
-PRECISIONS = {"fp64": 0, "tf32x3": 1, "bf16x3": 2}
+PRECISIONS = {"fp64": 0, "tf32x3": 1, "bf16x3": 2, "f16x3": 3}
 
 
 def block_id(i, j, nb):
@@ -736,14 +736,14 @@ class MatrixParser:
 
 
 # hs_gp_solve_host algorithms
-_ALGORITHMS = {"cholesky": 0, "cg": 1, "mixed": 2, "mixed_tf32x3": 2, "mixed_bf16x3": 3}
+_ALGORITHMS = {"cholesky": 0, "cg": 1, "mixed": 2, "mixed_tf32x3": 2, "mixed_bf16x3": 3, "mixed_f16x3": 4}
 
 
 def gp_solve_host(ctx, X, y, lengthscale=1.0, signal_variance=1.0, noise_variance=0.01, algorithm="cholesky",
                   epsilon=1e-10, iMax=100000, out=None):
     """End-to-end GP solve through host buffers (hs_gp_solve_host): host X
     (N x d) and y (N) in, host x = K^-1 y out, plus the phase report.
-    ``algorithm`` is "cholesky", "cg", "mixed" / "mixed_tf32x3" or "mixed_bf16x3"
+    ``algorithm`` is "cholesky", "cg", "mixed" / "mixed_tf32x3", "mixed_bf16x3" or "mixed_f16x3"
     (for the mixed forms, ``epsilon`` is the backward-error target and ``iMax``
     the refinement step limit).  X, y
     and ``out`` may be CPU torch tensors (pinned memory gives asynchronous

@@ -153,8 +153,8 @@ struct Events {
 
 hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,
                            int max_steps, hs_mixed_report* out) {
-    if (precision != HS_PRECISION_TF32X3 && precision != HS_PRECISION_BF16X3) {
-        set_error("hs_mixed_solve: precision must be HS_PRECISION_TF32X3 or HS_PRECISION_BF16X3");
+    if (precision != HS_PRECISION_TF32X3 && precision != HS_PRECISION_BF16X3 && precision != HS_PRECISION_F16X3) {
+        set_error("hs_mixed_solve: precision must be HS_PRECISION_TF32X3, HS_PRECISION_BF16X3 or HS_PRECISION_F16X3");
         return HS_ERR_UNSUPPORTED;
     }
     if (!(tol > 0.0) || max_steps < 1) {
@@ -196,11 +196,23 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     double shift = 0.0;
     int prec = precision;
     HS_CUDA(cudaEventRecord(ev.e[0], s));
+    // the largest diagonal entry (h[9]): the FP16 split's scale, and the unit of the shifts
+    bool have_maxdiag = false;
+    auto read_maxdiag = [&]() -> hs_status {
+        ctx->launches += 1;
+        maxdiag_kernel<<<1, 1024, 0, s>>>(K, bsz, nb, ctx->N, scal + 3);
+        HS_CHECK_LAUNCH("maxdiag");
+        HS_CUDA(cudaMemcpyAsync((void*)(h + 9), scal + 3, sizeof(double), cudaMemcpyDeviceToHost, s));
+        HS_CUDA(cudaStreamSynchronize(s));
+        have_maxdiag = true;
+        return HS_OK;
+    };
+    if (prec == HS_PRECISION_F16X3 && (st = read_maxdiag()) != HS_OK) return st;
     for (int attempt = 1;; ++attempt) {
         ctx->launches += 1;
         set_i64_dev(ctx->d_info, INT64_MAX, s);
         // the first attempt's conversion to FP32 also sums ||K||_F^2
-        st = mixed_factor(ctx, K, w, s, shift, prec, attempt == 1 ? part : nullptr);
+        st = mixed_factor(ctx, K, w, s, shift, prec, attempt == 1 ? part : nullptr, have_maxdiag ? h[9] + shift : 0.0);
         if (st != HS_OK) return st;
         HS_CUDA(cudaStreamSynchronize(s));
         if (ctx->side) HS_CUDA(cudaStreamSynchronize(ctx->side));
@@ -213,7 +225,7 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
         R.precision_used = prec;
         R.shift = shift;
         if (info < 0) break;
-        if (prec == HS_PRECISION_BF16X3) {  // the more accurate split products first
+        if (prec == HS_PRECISION_BF16X3 || prec == HS_PRECISION_F16X3) {  // the more accurate split products first
             prec = HS_PRECISION_TF32X3;
             continue;
         }
@@ -223,18 +235,14 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
             return HS_ERR_NOT_SPD;
         }
         if (shift == 0.0) {
-            ctx->launches += 1;
-            maxdiag_kernel<<<1, 1024, 0, s>>>(K, bsz, nb, ctx->N, scal + 3);
-            HS_CHECK_LAUNCH("maxdiag");
-            HS_CUDA(cudaMemcpyAsync((void*)(h + 9), scal + 3, sizeof(double), cudaMemcpyDeviceToHost, s));
-            HS_CUDA(cudaStreamSynchronize(s));
+            if (!have_maxdiag && (st = read_maxdiag()) != HS_OK) return st;
             shift = 1e-6 * h[9];
         } else {
             shift *= 10.0;  // 1e-6 .. 1e-1 x the largest diagonal entry
         }
     }
     // the sweeps read the inverse diagonal blocks in FP32 (their rounding is far below
-    // the factor's own error), from the BF16 panel area the factor no longer needs
+    // the factor's own error), from the 16-bit panel area the factor no longer needs
     w.Y32 = reinterpret_cast<float*>(w.P16);
     ctx->launches += 1;
     f64_to_f32_copy_kernel<<<grid_n((int64_t)nb * bsz * bsz / 2, ctx->num_sms), kThreads, 0, s>>>(

@@ -32,8 +32,10 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w);
 // shift != 0: factor K + shift*I
 // fro_part (non-null): also the squared Frobenius norm of K (off-diagonal blocks twice)
 // as mixed_fro_grid(blocks) CTA partials
+// maxdiag: the largest diagonal entry of the matrix factored (with its shift); it sets
+// the power-of-two scale of the FP16 split and is not read by the other precisions
 hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift = 0.0,
-                       int precision = HS_PRECISION_TF32X3, double* fro_part = nullptr);
+                       int precision = HS_PRECISION_TF32X3, double* fro_part = nullptr, double maxdiag = 0.0);
 int mixed_fro_grid(int64_t blocks);
 hs_status mixed_check_error(hs_ctx ctx, const MixedWork& w);
 // b <- (L L^T)^-1 b with the mixed factor (tmp: intermediate)

@@ -310,8 +310,9 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
         set_error("hs_gp_solve_host: null pointer");
         return HS_ERR_INVALID_ARG;
     }
-    if (algorithm < 0 || algorithm > 3) {
-        set_error("hs_gp_solve_host: algorithm must be 0 (cholesky), 1 (cg), 2 (mixed, 3xTF32) or 3 (mixed, BF16 split)");
+    if (algorithm < 0 || algorithm > 4) {
+        set_error("hs_gp_solve_host: algorithm must be 0 (cholesky), 1 (cg), 2 (mixed, 3xTF32), 3 (mixed, BF16 split) "
+                  "or 4 (mixed, FP16 split)");
         return HS_ERR_INVALID_ARG;
     }
     const int64_t N = ctx->N;
@@ -369,8 +370,8 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
     } else {
         // mixed precision: epsilon is the backward-error target, iMax the refinement step limit
         hs_mixed_report mr{};
-        st = mixed_solve_impl(ctx, Ad, bd, xd, algorithm == 3 ? HS_PRECISION_BF16X3 : HS_PRECISION_TF32X3, epsilon,
-                              (int)iMax, &mr);
+        const int prec = algorithm == 4 ? HS_PRECISION_F16X3 : algorithm == 3 ? HS_PRECISION_BF16X3 : HS_PRECISION_TF32X3;
+        st = mixed_solve_impl(ctx, Ad, bd, xd, prec, epsilon, (int)iMax, &mr);
         if (st != HS_OK) { cleanup(); return st; }
         iters = mr.refinement_steps + mr.pcg_iterations;
         HS_E2E(cudaEventRecord(ev[2], s));

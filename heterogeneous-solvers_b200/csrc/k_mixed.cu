@@ -11,6 +11,10 @@
 // (its top 19 bits), a_hi; a_lo = a - a_hi is exact in FP32 and kept in a
 // second buffer.  a*b ~ a_hi*b_hi + a_hi*b_lo + a_lo*b_hi: three MMAs per
 // k-step, accumulated in FP32, relative error ~2^-21 instead of TF32's 2^-11.
+// The trailing update can instead take 16-bit splits of the factored panel on
+// tcgen05 kind::f16 at twice the rate: BF16 (hi = bf16(a), lo = bf16(a - hi),
+// ~2^-16) or FP16 of the panel scaled by a power of two s (hi = fp16(s a),
+// lo = fp16(s a - hi), ~2^-22), the accumulator being multiplied by s^-2.
 //
 // Kernel structure (one 128 x bsz output tile per CTA, 4 warps):
 //   thread 0   TMA producer: A_hi, A_lo (128 x 32 FP32) and B_hi, B_lo
@@ -22,7 +26,10 @@
 // Every mbarrier wait is bounded (2 s); on expiry the CTA records an error in
 // the context's flag word, frees its TMEM and returns.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cudaTypedefs.h>
+
+#include <cmath>
 
 #include "hs_internal.cuh"
 #include "hs_mixed.cuh"
@@ -55,14 +62,18 @@ struct TcArgs {
     int lo_base, inv;
     // persistent update with the npanels (1..kPanelGroup) consecutive panel columns
     // k + p, updating the trailing columns from first_col on.  Panel p keeps its FP32
-    // low parts from LO slot p nb and its BF16 split from P16 slot 2 p nb (hi of row r
+    // low parts from LO slot p nb and its 16-bit split from P16 slot 2 p nb (hi of row r
     // at 2 p nb + r - (k + p) - 1, lo nb slots further)
     int npanels;
     int first_col;
-    // TRSM with BF16 split products downstream: the epilogue writes L's BF16 hi / lo
-    // split (P16 slots 2 lo_base + r - k - 1 and nb further) instead of its TF32 low part
-    __nv_bfloat16* P16;
-    int bf16;
+    // TRSM with 16-bit split products downstream (split16 = HS_PRECISION_BF16X3 or
+    // HS_PRECISION_F16X3; 0: none): the epilogue writes L's hi / lo split (P16 slots
+    // 2 lo_base + r - k - 1 and nb further) instead of its TF32 low part.  The FP16
+    // split is of f16_scale L (a power of two); the update multiplies its FP32
+    // accumulator by f16_unscale = f16_scale^-2 (exact).
+    __nv_bfloat16* P16;  // 16-bit storage: BF16 or FP16 values
+    int split16;
+    float f16_scale, f16_unscale;
 };
 
 // CTA-uniform early exit once a diagonal POTRF has recorded a non-positive pivot:
@@ -229,7 +240,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const float x0 = sr[0], x1 = sr[1], x2 = sr[2], x3 = sr[3];
                     const size_t off = (size_t)(ti * 128 + warp * 32 + rr) * BSZ + j * 32 + c4;
                     *reinterpret_cast<float4*>(a.A32 + (size_t)blkA * bb + off) = make_float4(x0, x1, x2, x3);
-                    if (a.bf16) {
+                    if (a.split16 == HS_PRECISION_F16X3) {
+                        const float sc = a.f16_scale;
+                        const float y0 = x0 * sc, y1 = x1 * sc, y2 = x2 * sc, y3 = x3 * sc;
+                        const __half2 h01 = __floats2half2_rn(y0, y1), h23 = __floats2half2_rn(y2, y3);
+                        const float2 f01 = __half22float2(h01), f23 = __half22float2(h23);
+                        const __half2 l01 = __floats2half2_rn(y0 - f01.x, y1 - f01.y);
+                        const __half2 l23 = __floats2half2_rn(y2 - f23.x, y3 - f23.y);
+                        __half* ph =
+                            reinterpret_cast<__half*>(a.P16) + (size_t)(2 * a.lo_base + (r - a.k - 1)) * bb + off;
+                        __half2* h2 = reinterpret_cast<__half2*>(ph);
+                        __half2* l2 = reinterpret_cast<__half2*>(ph + (size_t)a.nb * bb);
+                        h2[0] = h01;
+                        h2[1] = h23;
+                        l2[0] = l01;
+                        l2[1] = l23;
+                    } else if (a.split16 == HS_PRECISION_BF16X3) {
                         const __nv_bfloat162 h01 = __floats2bfloat162_rn(x0, x1), h23 = __floats2bfloat162_rn(x2, x3);
                         const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
                         const __nv_bfloat162 l01 = __floats2bfloat162_rn(x0 - f01.x, x1 - f01.y);
@@ -292,8 +318,9 @@ constexpr int kPanelGroup = 4;
 constexpr uint64_t kStepWaitNs = 2000000000ull;
 
 // operand formats of the update: TF32 (FP32 storage, hi = the FP32 value as
-// read by the tensor core, lo = x - tf32(x)) or BF16 (hi = bf16(x), lo =
-// bf16(x - hi)); both give 128-byte operand rows per slab and 32-byte K steps
+// read by the tensor core, lo = x - tf32(x)), BF16 (hi = bf16(x), lo =
+// bf16(x - hi)) or FP16 of the scaled panel (hi = fp16(s x), lo = fp16(s x - hi));
+// all give 128-byte operand rows per slab and 32-byte K steps
 template <int PREC>
 struct UpdFmt;
 template <>
@@ -303,6 +330,10 @@ struct UpdFmt<HS_PRECISION_TF32X3> {
 template <>
 struct UpdFmt<HS_PRECISION_BF16X3> {
     static constexpr int kK = 2 * kUpdK, kKStep = 16, kFmt = kFmtBF16;
+};
+template <>
+struct UpdFmt<HS_PRECISION_F16X3> {
+    static constexpr int kK = 2 * kUpdK, kKStep = 16, kFmt = kFmtF16;
 };
 
 template <int BSZ>
@@ -423,7 +454,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                 // the epilogue's reduce-add finds its lines there
                 prefetch_l2(a.A32 + (size_t)block_id(r, c, a.nb) * BSZ * BSZ + (size_t)ti * 128 * BSZ,
                             128 * BSZ * 4);
-                const bool bf = PREC == HS_PRECISION_BF16X3;
+                const bool bf = PREC != HS_PRECISION_TF32X3;  // 16-bit split slots in P16
                 for (int kc = 0; kc < kSlabs; ++kc, ++g) {
                     const uint32_t s = g % SM::kStages, use = g / SM::kStages;
                     if (use > 0 && !mbar_wait_for(&empty[s], (use - 1) & 1, kStepWaitNs)) {
@@ -431,7 +462,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                         break;
                     }
                     // panel pi = column k + pi: TF32 hi = its FP32 block in A32, lo = its
-                    // LO slot; BF16 hi / lo = its split slots in P16
+                    // LO slot; BF16 / FP16 hi / lo = its split slots in P16
                     const int pi = kc / kSlabsP, kk = kc % kSlabsP;
                     const int colp = a.k + pi;
                     const int gA = r - colp - 1, gB = c - colp - 1;
@@ -480,7 +511,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                         const uint32_t off = ks * 32;  // one K step = 32 bytes along K
                         const uint64_t dAh = upd_desc(aHi + off), dAl = upd_desc(aLo + off);
                         const uint64_t dBh = upd_desc(bHi + off), dBl = upd_desc(bLo + off);
-                        if (PREC == HS_PRECISION_BF16X3) {
+                        if (PREC != HS_PRECISION_TF32X3) {
                             umma_f16(dcol, dAh, dBh, idesc, (kc | ks) != 0);
                             umma_f16(dcol, dAh, dBl, idesc, 1);
                             umma_f16(dcol, dAl, dBh, idesc, 1);
@@ -507,6 +538,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         const int half = (warp - 2) >> 2;  // 0: warps 2-5, 1: warps 6-9
         constexpr int kChunks = BSZ / 64;   // 32-column chunks per warp
         float4* stile = reinterpret_cast<float4*>(staging + (warp - 2) * 4096);
+        const float us = PREC == HS_PRECISION_F16X3 ? a.f16_unscale : 1.0f;  // exact power of two
         int it = 0;
         for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
             const int b = it & 1, u = it >> 1;
@@ -533,8 +565,8 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
 #pragma unroll
                 for (int e = 0; e < 8; ++e)
                     stile[lane * 8 + (e ^ (lane & 7))] =
-                        make_float4(-__uint_as_float(v[4 * e + 0]), -__uint_as_float(v[4 * e + 1]),
-                                    -__uint_as_float(v[4 * e + 2]), -__uint_as_float(v[4 * e + 3]));
+                        make_float4(-us * __uint_as_float(v[4 * e + 0]), -us * __uint_as_float(v[4 * e + 1]),
+                                    -us * __uint_as_float(v[4 * e + 2]), -us * __uint_as_float(v[4 * e + 3]));
                 fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) {
@@ -996,6 +1028,7 @@ hs_status make_map(CUtensorMap* m, void* base, int bsz, int64_t blocks, int box_
     cuuint64_t strides[2] = {(cuuint64_t)bsz * elem, (cuuint64_t)bsz * bsz * elem};
     cuuint32_t box[3] = {(cuuint32_t)box_k, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
+    // 2-byte maps are plain copies of the BF16 or FP16 split (no conversion on load)
     CUresult r = g_encode(m, elem == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base,
                           dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                           box_k * elem == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
@@ -1036,6 +1069,9 @@ hs_status tc_update_launch(hs_ctx ctx, const MixedWork& w, const TcArgs& a, int 
     if (precision == HS_PRECISION_BF16X3)
         tc_update_kernel<BSZ, HS_PRECISION_BF16X3>
             <<<grid, kUpdThreads, SM::kBytes, s>>>(w.mP128, w.mPB, w.mP128, w.mPB, w.mC32, a);
+    else if (precision == HS_PRECISION_F16X3)
+        tc_update_kernel<BSZ, HS_PRECISION_F16X3>
+            <<<grid, kUpdThreads, SM::kBytes, s>>>(w.mP128, w.mPB, w.mP128, w.mPB, w.mC32, a);
     else
         tc_update_kernel<BSZ, HS_PRECISION_TF32X3>
             <<<grid, kUpdThreads, SM::kBytes, s>>>(w.mU128, w.mUB, w.mV128, w.mVB, w.mC32, a);
@@ -1058,6 +1094,8 @@ hs_status tc_attrs() {
     HS_CUDA(cudaFuncSetAttribute(tc_update_kernel<BSZ, HS_PRECISION_TF32X3>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, UpdSmem<BSZ>::kBytes));
     HS_CUDA(cudaFuncSetAttribute(tc_update_kernel<BSZ, HS_PRECISION_BF16X3>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, UpdSmem<BSZ>::kBytes));
+    HS_CUDA(cudaFuncSetAttribute(tc_update_kernel<BSZ, HS_PRECISION_F16X3>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, UpdSmem<BSZ>::kBytes));
     HS_CUDA(cudaFuncSetAttribute(diag_chain_kernel<BSZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)ChainSmem<BSZ>::kBytes));
@@ -1082,7 +1120,7 @@ size_t mixed_workspace_bytes(int64_t N, int bsz) {
     bytes += (size_t)(kPanelGroup * nb + 2) * bb * 4;  // LO: a group's low parts + L_kk^-1 hi / lo
     bytes += (size_t)nb * bb * 8;        // Ldiag64
     bytes += (size_t)nb * bb * 8;        // Yinv
-    bytes += (size_t)2 * kPanelGroup * nb * bb * 2;  // BF16 split of a group's panels (hi / lo each)
+    bytes += (size_t)2 * kPanelGroup * nb * bb * 2;  // 16-bit split of a group's panels (hi / lo each)
     bytes += bb * 8;                     // S
     bytes += 1024;                       // error flags
     bytes += ((size_t)nb * 4 + 255) & ~size_t(255);  // sweep publication flags
@@ -1125,7 +1163,7 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
 int mixed_fro_grid(int64_t blocks) { return (int)(blocks < 1024 ? blocks : 1024); }
 
 hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift, int precision,
-                       double* fro_part) {
+                       double* fro_part, double maxdiag) {
     const int bsz = ctx->bsz, nb = ctx->nb;
     HS_REQUIRE(bsz == 128 || bsz == 256, "the mixed-precision factor supports matrixBlockSize 128 or 256");
     hs_status st = bsz == 256 ? tc_attrs<256>() : tc_attrs<128>();
@@ -1187,8 +1225,24 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
     base.err = w.err;
     base.abort_flag = ctx->d_info;
     base.inv = kPanelGroup * nb;
+    // FP16 split: scale s = 2^e, the largest e with s sqrt(maxdiag) <= 2^15.  Every
+    // |L_ij| <= sqrt(K_ii) <= sqrt(maxdiag), so s L stays below 2^15 (FP16 holds up to
+    // 65504), and entries small enough to reach FP16's subnormal range carry an absolute
+    // error below 2^-25 / s, far below the products that matter.  A matrix that is not
+    // positive definite can overflow it; its factor then fails a pivot check and is
+    // redone with 3xTF32 products.
+    base.f16_scale = base.f16_unscale = 1.0f;
+    if (precision == HS_PRECISION_F16X3) {
+        int e = 0;
+        if (maxdiag > 0.0 && std::isfinite(maxdiag)) {
+            e = (int)std::floor(std::log2(32768.0 / std::sqrt(maxdiag)));
+            e = e < -60 ? -60 : (e > 60 ? 60 : e);
+        }
+        base.f16_scale = std::ldexp(1.0f, e);
+        base.f16_unscale = std::ldexp(1.0f, -2 * e);
+    }
     // blocks k+1..nb-1 of column k: FP32 low parts into set `set`, TRSM-as-GEMM with
-    // L_kk^-T (writes L and its low part), and for BF16 the split of L into P16
+    // L_kk^-T (writes L and its low part), and for BF16 / FP16 the split of L into P16
     auto panel = [&](int k, int set) -> hs_status {
         const int64_t blockID = diag_id(k);
         float* dblk = w.A32 + (size_t)blockID * bb;
@@ -1201,8 +1255,8 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         a.blockID = blockID;
         a.k = k;
         a.lo_base = set * nb;
-        // BF16 products downstream: the TRSM writes L's BF16 split itself
-        a.bf16 = precision == HS_PRECISION_BF16X3 ? 1 : 0;
+        // 16-bit products downstream: the TRSM writes L's 16-bit split itself
+        a.split16 = (precision == HS_PRECISION_BF16X3 || precision == HS_PRECISION_F16X3) ? precision : 0;
         a.P16 = w.P16;
         prof_begin(ctx, s, HS_KERNEL_TRSM);
         hs_status r = bsz == 256 ? tc_launch<256>(ctx, MODE_TRSM, w, a, m, s) : tc_launch<128>(ctx, MODE_TRSM, w, a, m, s);

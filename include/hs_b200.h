@@ -225,7 +225,8 @@ hs_status hs_cg_solve(hs_ctx ctx, const double* A, const double* b, double* x, d
  * solve (src/gaussianProcess/GaussianProcess.cpp:20-40) and main.cpp:201-249:
  * X_host (N x d), y_host (N) -> RBF assembly -> factor + solve (algorithm 0),
  * CG (algorithm 1: epsilon, iMax as in hs_cg_solve) or the mixed-precision solve
- * (no reference counterpart: algorithm 2 with 3xTF32, 3 with BF16-split updates;
+ * (no reference counterpart: algorithm 2 with 3xTF32, 3 with BF16-split, 4 with
+ * FP16-split updates;
  * epsilon = backward-error target, iMax = refinement step limit;
  * report->factor_ms then covers factor and refinement) ->
  * x_host (N).  The device copies (X, the packed K, y, x) are kept by the context
@@ -246,15 +247,20 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
  * accumulation) and every diagonal-block POTRF in FP64.  HS_PRECISION_BF16X3
  * runs the trailing updates instead as BF16 split products (hi = bf16(x),
  * lo = bf16(x - hi), hi*hi + hi*lo + lo*hi on tcgen05 kind::f16, FP32
- * accumulation; ~2^-16 relative per product), the TRSM staying 3xTF32.  It then refines
+ * accumulation; ~2^-16 relative per product), the TRSM staying 3xTF32.
+ * HS_PRECISION_F16X3 runs them as FP16 split products of the panel scaled by a
+ * power of two s (hi = fp16(s x), lo = fp16(s x - hi): 22 significant bits, ~2^-22
+ * relative per product, at the BF16 rate; s = 2^e, the largest e with
+ * s sqrt(max_i K_ii) <= 2^15, is exact and is undone in the FP32 epilogue: every
+ * |L_ij| <= sqrt(K_ii), so the scaled panel stays inside the FP16 range).  It then refines
  * x <- x + (L L^T)^-1 (b - K x) with FP64 residuals until the backward error
  * ||b - K x|| / (||K||_F ||x||) <= tol.  When refinement stops contracting it
  * continues with conjugate gradients preconditioned by the FP32 factor.  b and x
  * are device vectors of hs_padded_vector_size doubles.  The workspace (FP32
  * factor: half the packed matrix) is kept by the context between calls.  When
  * the low-precision factor of K meets a non-positive pivot (K too ill-conditioned
- * for it; the factorization stops at that block), a BF16-split factor is redone
- * with 3xTF32 products, and then K + shift*I is factored with shift = 1e-6, 1e-5,
+ * for it; the factorization stops at that block), a BF16- or FP16-split factor is
+ * redone with 3xTF32 products, and then K + shift*I is factored with shift = 1e-6, 1e-5,
  * ... 1e-1 times the largest diagonal entry, the solve going straight to CG
  * preconditioned by that factor (report->shift, report->precision_used;
  * report->logdet is then the log-determinant of the shifted matrix).  Returns HS_ERR_REFINEMENT_STALLED
@@ -262,7 +268,8 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
 typedef enum hs_precision {
     HS_PRECISION_FP64 = 0,
     HS_PRECISION_TF32X3 = 1,
-    HS_PRECISION_BF16X3 = 2
+    HS_PRECISION_BF16X3 = 2,
+    HS_PRECISION_F16X3 = 3
 } hs_precision;
 typedef struct hs_mixed_report {
     int64_t refinement_steps;

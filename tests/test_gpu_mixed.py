@@ -12,13 +12,13 @@ import oracle_lib as ol
 pytestmark = pytest.mark.gpu
 
 
-def _system(hs, ctx, N, bsz, d, ell, sn2, seed=5):
+def _system(hs, ctx, N, bsz, d, ell, sn2, seed=5, sf2=1.0):
     rng = np.random.default_rng(seed)
     X = rng.random((N, d))
     y = np.sin(X.sum(axis=1)) + 0.1 * rng.standard_normal(N)
     ctx.set_problem(N, bsz)
     A = hs.SymmetricMatrix(N, bsz, device="cuda:0")
-    hs.MatrixGenerator.assemble(ctx, A.matrixData, X, ell, 1.0, sn2)
+    hs.MatrixGenerator.assemble(ctx, A.matrixData, X, ell, sf2, sn2)
     b = torch.zeros(hs.padded_size(N, bsz), dtype=torch.float64, device="cuda:0")
     b[:N] = torch.from_numpy(y)
     return A, b, X, y
@@ -151,9 +151,10 @@ def test_mixed_factor_breakdown_falls_back_to_shifted_preconditioner(hs, ctx):
         assert rep["factor_attempts"] == 1
 
 
-def test_mixed_bf16_breakdown_falls_back_to_tf32(hs, ctx):
-    """A BF16-split factor that breaks down is redone with 3xTF32 products before
-    any diagonal shift is tried; the solve still reaches the target."""
+@pytest.mark.parametrize("prec", ["bf16x3", "f16x3"])
+def test_mixed_split16_breakdown_falls_back_to_tf32(hs, ctx, prec):
+    """A BF16- or FP16-split factor that breaks down is redone with 3xTF32 products
+    before any diagonal shift is tried; the solve still reaches the target."""
     N, bsz, d = 1024, 128, 4
     rng = np.random.default_rng(12)
     base = rng.random((N // 2, d))
@@ -164,10 +165,10 @@ def test_mixed_bf16_breakdown_falls_back_to_tf32(hs, ctx):
     hs.MatrixGenerator.assemble(ctx, A.matrixData, X, 0.5, 1.0, 1e-7)
     b = torch.zeros(hs.padded_size(N, bsz), dtype=torch.float64, device="cuda:0")
     b[:N] = torch.from_numpy(y)
-    solver = hs.MixedPrecisionSolver(A, ctx, "bf16x3")
+    solver = hs.MixedPrecisionSolver(A, ctx, prec)
     x = solver.solve(b, tol=1e-14, max_steps=30)
     rep = solver.report
-    print("bf16 breakdown case:", rep)
+    print(f"{prec} breakdown case:", rep)
     if rep["factor_attempts"] > 1:
         assert rep["precision_used"] == hs.PRECISIONS["tf32x3"]
     Kd = A.to_dense()
@@ -193,3 +194,53 @@ def test_mixed_bf16_split_reaches_fp64_backward_error(hs, ctx, N, bsz, sn2):
     assert bwd <= 2e-14
     # a BF16-split factor: unrefined backward error well below plain BF16's ~1e-3
     assert rep["initial_backward_error"] <= 1e-4
+
+
+@pytest.mark.parametrize("N,bsz,sn2,sf2", [
+    (1000, 128, 1e-2, 1.0), (2048, 256, 1e-2, 1.0), (700, 256, 1e-1, 1.0), (1536, 256, 1e-3, 1.0),
+    (1000, 128, 1e4, 1e6), (1000, 128, 1e-8, 1e-6),
+])
+def test_mixed_f16_split_reaches_fp64_backward_error(hs, ctx, N, bsz, sn2, sf2):
+    """The FP16 split of the trailing update (the panel scaled by a power of two set
+    from the largest diagonal entry, 22 significant bits): refined to the FP64
+    backward-error target, with no more refinement work than the BF16 split on the
+    same system.  sf2 = 1e6 and 1e-6 move the scale far from 1 (2^5 and 2^25)."""
+    A, b, X, y = _system(hs, ctx, N, bsz, 8, 0.5, sn2, seed=31, sf2=sf2)
+    Kd = A.to_dense()
+    reps = {}
+    for prec in ("f16x3", "bf16x3"):
+        solver = hs.MixedPrecisionSolver(A, ctx, prec)
+        x = solver.solve(b, tol=1e-14, max_steps=30)
+        rep = solver.report
+        reps[prec] = rep
+        xg = x.cpu().numpy()[:N]
+        bwd = np.linalg.norm(y - Kd @ xg) / (np.linalg.norm(Kd, "fro") * np.linalg.norm(xg))
+        print(f"{prec} N={N} bsz={bsz} sn2={sn2} sf2={sf2}: attempts {rep['factor_attempts']} "
+              f"steps {rep['refinement_steps']} pcg {rep['pcg_iterations']} "
+              f"bwd0 {rep['initial_backward_error']:.2e} bwd {bwd:.2e}")
+        assert bwd <= 2e-14
+    f, g = reps["f16x3"], reps["bf16x3"]
+    assert f["factor_attempts"] == 1 and f["precision_used"] == hs.PRECISIONS["f16x3"] and f["shift"] == 0.0
+    assert f["initial_backward_error"] <= 1e-5
+    if g["factor_attempts"] == 1:
+        assert f["refinement_steps"] + f["pcg_iterations"] <= g["refinement_steps"] + g["pcg_iterations"]
+    sign, logdet_ref = np.linalg.slogdet(Kd)
+    assert sign > 0
+    assert abs(f["logdet"] - logdet_ref) <= 1e-4 * abs(logdet_ref) + 1e-3
+
+
+def test_gp_solve_host_mixed_f16(hs):
+    """hs_gp_solve_host, algorithm 4 (mixed, FP16 split): host X, y in, host x out."""
+    N, bsz, d = 900, 128, 8
+    rng = np.random.default_rng(22)
+    X = rng.random((N, d))
+    y = np.sin(X.sum(axis=1)) + 0.1 * rng.standard_normal(N)
+    with hs.Context(device=0) as c:
+        c.set_problem(N, bsz)
+        x, rep = hs.gp_solve_host(c, X, y, 0.5, 1.0, 1e-2, algorithm="mixed_f16x3", epsilon=1e-14, iMax=30)
+        A = hs.SymmetricMatrix(N, bsz, device="cuda:0")
+        hs.MatrixGenerator.assemble(c, A.matrixData, X, 0.5, 1.0, 1e-2)
+        Kd = A.to_dense()
+    bwd = np.linalg.norm(y - Kd @ x) / (np.linalg.norm(Kd, "fro") * np.linalg.norm(x))
+    assert bwd <= 2e-14
+    assert rep.iterations >= 1
