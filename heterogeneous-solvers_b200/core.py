@@ -418,7 +418,10 @@ class MixedPrecisionSolver:
 
     The factor runs in FP32 with the panel TRSM and SYRK/GEMM trailing updates
     on the tensor cores as split products ("tf32x3": three TF32 products per
-    FP32 product) and every diagonal-block POTRF in FP64; FP64 iterative
+    FP32 product; "bf16x3" / "f16x3": the trailing updates as three BF16, or
+    three FP16 products of the panel scaled by a power of two — 16 or 22
+    significant bits at twice the TF32 rate) and every diagonal-block POTRF in
+    FP64; FP64 iterative
     refinement then drives the backward error ||b - K x|| / (||K||_F ||x||)
     below ``tol``, continuing as CG preconditioned by the low-precision factor
     when refinement stalls.  K (packed, device) is left unchanged.
