@@ -16,14 +16,14 @@ struct MixedWork {
     double* Ld = nullptr;   // FP64 diagonal blocks of L (nb blocks; only the diagonal entries are written)
     double* Yinv = nullptr; // FP64 inverse diagonal blocks, Y_k = L_kk^-T (nb blocks)
     double* S = nullptr;    // FP64 scratch block (POTRF)
-    __nv_bfloat16* P16 = nullptr;  // BF16 split of a panel group: panel p hi blocks 2p nb.., lo (2p+1) nb..
+    __nv_bfloat16* P16 = nullptr;  // 16-bit (BF16 or FP16) split of a panel group: panel p hi blocks 2p nb.., lo (2p+1) nb..
     int* err = nullptr;     // [0] tensor-core tile timeout, [1] triangular-sweep timeout
     unsigned* flags = nullptr;  // per block row: epoch of the sweep that published it
     unsigned epoch = 0;         // last sweep launched (flags are cleared when it restarts at 0)
     float* Y32 = nullptr;       // FP32 copy of Yinv for the sweeps, in the P16 area once the factor is done
     CUtensorMap mA128, mAB, mL128, mLB;  // 128-byte swizzle, 32-wide K boxes (TRSM)
     CUtensorMap mU128, mUB, mV128, mVB;  // K boxes of 128 bytes over A32 / LO (TF32 update)
-    CUtensorMap mP128, mPB;              // K boxes of 128 bytes over P16 (BF16 update)
+    CUtensorMap mP128, mPB;              // K boxes of 128 bytes over P16 (BF16 / FP16 update)
     CUtensorMap mC32;                    // 32x32 FP32 boxes over A32 (TMA reduce of the update's C tiles)
 };
 
