@@ -16,13 +16,14 @@
 // ~2^-16) or FP16 of the panel scaled by a power of two s (hi = fp16(s a),
 // lo = fp16(s a - hi), ~2^-22), the accumulator being multiplied by s^-2.
 //
-// Kernel structure (one 128 x bsz output tile per CTA, 4 warps):
+// Panel TRSM kernel (one 128 x bsz output tile per CTA, 4 warps):
 //   thread 0   TMA producer: A_hi, A_lo (128 x 32 FP32) and B_hi, B_lo
 //              (bsz x 32 FP32) per K slab, 128-byte swizzle, 2-stage ring
 //   thread 32  MMA issuer: 3 x 4 tcgen05.mma (K = 8 each) per slab, commit to
 //              the stage's "empty" barrier and finally to "done"
 //   all warps  epilogue: TMEM -> registers (warp w owns lanes 32w..32w+31 =
-//              tile rows), C -= D (update) or L = D, L_lo = D - tf32(D) (TRSM)
+//              tile rows), L = D and L_lo = D - tf32(D) or L's 16-bit split
+// The trailing update is the persistent tc_update_kernel further down.
 // Every mbarrier wait is bounded (2 s); on expiry the CTA records an error in
 // the context's flag word, frees its TMEM and returns.
 #include <cuda_bf16.h>
@@ -44,16 +45,13 @@ constexpr int kTcThreads = 128;
 constexpr int kSlab = 32;               // K elements (FP32) per stage = 128 bytes
 constexpr uint64_t kWaitNs = 2000000000ull;
 
-enum { MODE_UPDATE = 0, MODE_TRSM = 1 };
+enum { MODE_TRSM = 1 };  // the tile kernel's one mode, the panel TRSM
 
 struct TcArgs {
     float* A32;        // packed FP32 working matrix
     float* LO;         // FP32 low parts of panel blocks and of L_kk^-T (slots below)
     int64_t blockID;   // id of the diagonal block of column k
     int k, nb;
-    int64_t gemmPairs, pairBase;  // MODE_UPDATE: GEMM pairs c < r, rows k+2..
-    int syrkStart;
-    int64_t totalPairs;
     int* err;          // error flag (timeouts)
     int part;          // persistent update: 0 columns first_col.., 1 column first_col only, 2 columns first_col+1..
     const long long* abort_flag;  // smallest failing pivot row so far (INT64_MAX: none)
@@ -99,8 +97,8 @@ struct TcSmem {
 
 template <int BSZ, int MODE>
 __global__ void __launch_bounds__(kTcThreads, 1)
-    tc_tile_kernel(const __grid_constant__ CUtensorMap mA128, const __grid_constant__ CUtensorMap mAB,
-                   const __grid_constant__ CUtensorMap mL128, const __grid_constant__ CUtensorMap mLB, TcArgs a) {
+    tc_tile_kernel(const __grid_constant__ CUtensorMap mA128, const __grid_constant__ CUtensorMap mL128,
+                   const __grid_constant__ CUtensorMap mLB, TcArgs a) {
     using SM = TcSmem<BSZ>;
     if (factor_aborted(a.abort_flag)) return;
     extern __shared__ uint8_t smem_raw[];
@@ -116,23 +114,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // ---- tile decode
     const int ti = (int)(blockIdx.x % SM::kTiles);
     const int64_t item = blockIdx.x / SM::kTiles;
-    int r, c;
-    if (MODE == MODE_TRSM) {
-        r = a.k + 1 + (int)item;
-        c = a.k;
-    } else if (item < a.gemmPairs) {
-        const int64_t t = item + a.pairBase;
-        const int u = tri_root(t);
-        r = a.k + 1 + (u + 1);
-        c = a.k + 1 + (int)(t - (int64_t)u * (u + 1) / 2);
-    } else {
-        r = c = a.syrkStart + (int)(item - a.gemmPairs);
-    }
+    static_assert(MODE == MODE_TRSM, "the tile kernel runs the panel TRSM only");
+    const int r = a.k + 1 + (int)item;  // block row of the panel (column k)
     // operand coordinates: (column, row, block) in the TMA maps
     const int blkA = (int)(a.blockID + (r - a.k));  // panel block of row r
     const int gA = a.lo_base + r - a.k - 1;         // its low-part slot
-    const int blkB = (MODE == MODE_TRSM) ? a.inv : (int)(a.blockID + (c - a.k));
-    const int gB = (MODE == MODE_TRSM) ? a.inv + 1 : a.lo_base + c - a.k - 1;
+    const int blkB = a.inv, gB = a.inv + 1;         // L_kk^-T hi / lo
 
     if (tid == 0) {
         for (int s = 0; s < SM::kStages; ++s) {
@@ -163,11 +150,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             mbar_arrive_expect_tx(&full[s], SM::kStage);
             tma_load_3d(st, &mA128, &full[s], kc * kSlab, ti * 128, blkA);
             tma_load_3d(st + SM::kABytes, &mL128, &full[s], kc * kSlab, ti * 128, gA);
-            if (MODE == MODE_TRSM) {
-                tma_load_3d(st + 2 * SM::kABytes, &mLB, &full[s], kc * kSlab, 0, blkB);
-            } else {
-                tma_load_3d(st + 2 * SM::kABytes, &mAB, &full[s], kc * kSlab, 0, blkB);
-            }
+            tma_load_3d(st + 2 * SM::kABytes, &mLB, &full[s], kc * kSlab, 0, blkB);
             tma_load_3d(st + 2 * SM::kABytes + SM::kBBytes, &mLB, &full[s], kc * kSlab, 0, gB);
         }
         if (!ok) atomicExch(a.err, 1);
@@ -206,75 +189,60 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (!done_ok) {
         if (lane == 0) atomicExch(a.err, 1);
     } else {
-        const int row = warp * 32 + lane;
-        float* outp = a.A32 + (size_t)block_id(r, c, a.nb) * bb + (size_t)(ti * 128 + row) * BSZ;  // MODE_UPDATE
 #pragma unroll 1
         for (int j = 0; j < BSZ / 32; ++j) {
             uint32_t v[32];
             tmem_ld_32x32b_x32(taddr + ((uint32_t)(warp * 32) << 16) + j * 32, v);
             tmem_ld_wait();
-            if (MODE == MODE_UPDATE) {
-                float4* o4 = reinterpret_cast<float4*>(outp + j * 32);
+            // staged through this warp's 32 x 33 shared tile (the operand ring is
+            // free once the MMAs are done), then written as whole 128-byte row
+            // segments: 8 lanes a row, 4 rows an instruction
+            float* stg = reinterpret_cast<float*>(smem) + warp * 32 * 33;
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    float4 cv = o4[q];
-                    cv.x -= __uint_as_float(v[4 * q + 0]);
-                    cv.y -= __uint_as_float(v[4 * q + 1]);
-                    cv.z -= __uint_as_float(v[4 * q + 2]);
-                    cv.w -= __uint_as_float(v[4 * q + 3]);
-                    o4[q] = cv;
-                }
-            } else {
-                // staged through this warp's 32 x 33 shared tile (the operand ring is
-                // free once the MMAs are done), then written as whole 128-byte row
-                // segments: 8 lanes a row, 4 rows an instruction
-                float* stg = reinterpret_cast<float*>(smem) + warp * 32 * 33;
-#pragma unroll
-                for (int q = 0; q < 32; ++q) stg[lane * 33 + q] = __uint_as_float(v[q]);
-                __syncwarp();
-                const int c4 = (lane & 7) * 4;
+            for (int q = 0; q < 32; ++q) stg[lane * 33 + q] = __uint_as_float(v[q]);
+            __syncwarp();
+            const int c4 = (lane & 7) * 4;
 #pragma unroll 2
-                for (int it = 0; it < 8; ++it) {
-                    const int rr = it * 4 + (lane >> 3);
-                    const float* sr = stg + rr * 33 + c4;
-                    const float x0 = sr[0], x1 = sr[1], x2 = sr[2], x3 = sr[3];
-                    const size_t off = (size_t)(ti * 128 + warp * 32 + rr) * BSZ + j * 32 + c4;
-                    *reinterpret_cast<float4*>(a.A32 + (size_t)blkA * bb + off) = make_float4(x0, x1, x2, x3);
-                    if (a.split16 == HS_PRECISION_F16X3) {
-                        const float sc = a.f16_scale;
-                        const float y0 = x0 * sc, y1 = x1 * sc, y2 = x2 * sc, y3 = x3 * sc;
-                        const __half2 h01 = __floats2half2_rn(y0, y1), h23 = __floats2half2_rn(y2, y3);
-                        const float2 f01 = __half22float2(h01), f23 = __half22float2(h23);
-                        const __half2 l01 = __floats2half2_rn(y0 - f01.x, y1 - f01.y);
-                        const __half2 l23 = __floats2half2_rn(y2 - f23.x, y3 - f23.y);
-                        __half* ph =
-                            reinterpret_cast<__half*>(a.P16) + (size_t)(2 * a.lo_base + (r - a.k - 1)) * bb + off;
-                        __half2* h2 = reinterpret_cast<__half2*>(ph);
-                        __half2* l2 = reinterpret_cast<__half2*>(ph + (size_t)a.nb * bb);
-                        h2[0] = h01;
-                        h2[1] = h23;
-                        l2[0] = l01;
-                        l2[1] = l23;
-                    } else if (a.split16 == HS_PRECISION_BF16X3) {
-                        const __nv_bfloat162 h01 = __floats2bfloat162_rn(x0, x1), h23 = __floats2bfloat162_rn(x2, x3);
-                        const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
-                        const __nv_bfloat162 l01 = __floats2bfloat162_rn(x0 - f01.x, x1 - f01.y);
-                        const __nv_bfloat162 l23 = __floats2bfloat162_rn(x2 - f23.x, x3 - f23.y);
-                        __nv_bfloat16* ph = a.P16 + (size_t)(2 * a.lo_base + (r - a.k - 1)) * bb + off;
-                        __nv_bfloat162* h2 = reinterpret_cast<__nv_bfloat162*>(ph);
-                        __nv_bfloat162* l2 = reinterpret_cast<__nv_bfloat162*>(ph + (size_t)a.nb * bb);
-                        h2[0] = h01;
-                        h2[1] = h23;
-                        l2[0] = l01;
-                        l2[1] = l23;
-                    } else {
-                        *reinterpret_cast<float4*>(a.LO + (size_t)gA * bb + off) =
-                            make_float4(x0 - tf32_trunc(x0), x1 - tf32_trunc(x1), x2 - tf32_trunc(x2),
-                                        x3 - tf32_trunc(x3));
-                    }
+            for (int it = 0; it < 8; ++it) {
+                const int rr = it * 4 + (lane >> 3);
+                const float* sr = stg + rr * 33 + c4;
+                const float x0 = sr[0], x1 = sr[1], x2 = sr[2], x3 = sr[3];
+                const size_t off = (size_t)(ti * 128 + warp * 32 + rr) * BSZ + j * 32 + c4;
+                *reinterpret_cast<float4*>(a.A32 + (size_t)blkA * bb + off) = make_float4(x0, x1, x2, x3);
+                if (a.split16 == HS_PRECISION_F16X3) {
+                    const float sc = a.f16_scale;
+                    const float y0 = x0 * sc, y1 = x1 * sc, y2 = x2 * sc, y3 = x3 * sc;
+                    const __half2 h01 = __floats2half2_rn(y0, y1), h23 = __floats2half2_rn(y2, y3);
+                    const float2 f01 = __half22float2(h01), f23 = __half22float2(h23);
+                    const __half2 l01 = __floats2half2_rn(y0 - f01.x, y1 - f01.y);
+                    const __half2 l23 = __floats2half2_rn(y2 - f23.x, y3 - f23.y);
+                    __half* ph =
+                        reinterpret_cast<__half*>(a.P16) + (size_t)(2 * a.lo_base + (r - a.k - 1)) * bb + off;
+                    __half2* h2 = reinterpret_cast<__half2*>(ph);
+                    __half2* l2 = reinterpret_cast<__half2*>(ph + (size_t)a.nb * bb);
+                    h2[0] = h01;
+                    h2[1] = h23;
+                    l2[0] = l01;
+                    l2[1] = l23;
+                } else if (a.split16 == HS_PRECISION_BF16X3) {
+                    const __nv_bfloat162 h01 = __floats2bfloat162_rn(x0, x1), h23 = __floats2bfloat162_rn(x2, x3);
+                    const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+                    const __nv_bfloat162 l01 = __floats2bfloat162_rn(x0 - f01.x, x1 - f01.y);
+                    const __nv_bfloat162 l23 = __floats2bfloat162_rn(x2 - f23.x, x3 - f23.y);
+                    __nv_bfloat16* ph = a.P16 + (size_t)(2 * a.lo_base + (r - a.k - 1)) * bb + off;
+                    __nv_bfloat162* h2 = reinterpret_cast<__nv_bfloat162*>(ph);
+                    __nv_bfloat162* l2 = reinterpret_cast<__nv_bfloat162*>(ph + (size_t)a.nb * bb);
+                    h2[0] = h01;
+                    h2[1] = h23;
+                    l2[0] = l01;
+                    l2[1] = l23;
+                } else {
+                    *reinterpret_cast<float4*>(a.LO + (size_t)gA * bb + off) =
+                        make_float4(x0 - tf32_trunc(x0), x1 - tf32_trunc(x1), x2 - tf32_trunc(x2),
+                                    x3 - tf32_trunc(x3));
                 }
-                __syncwarp();
             }
+            __syncwarp();
         }
     }
     tc_fence_before();
@@ -1040,19 +1008,15 @@ hs_status make_map(CUtensorMap* m, void* base, int bsz, int64_t blocks, int box_
     return HS_OK;
 }
 
+// panel TRSM of `items` blocks below the diagonal of column a.k
 template <int BSZ>
-hs_status tc_launch(hs_ctx ctx, int mode, const MixedWork& w, TcArgs a, int64_t items, cudaStream_t s) {
+hs_status tc_launch(hs_ctx ctx, const MixedWork& w, TcArgs a, int64_t items, cudaStream_t s) {
     using SM = TcSmem<BSZ>;
     const int64_t grid = items * SM::kTiles;
     if (grid <= 0) return HS_OK;
     HS_REQUIRE(grid < (1LL << 31), "too many tiles");
     ctx->launches += 1;
-    if (mode == MODE_TRSM)
-        tc_tile_kernel<BSZ, MODE_TRSM><<<(unsigned)grid, kTcThreads, SM::kBytes, s>>>(w.mA128, w.mAB, w.mL128,
-                                                                                     w.mLB, a);
-    else
-        tc_tile_kernel<BSZ, MODE_UPDATE><<<(unsigned)grid, kTcThreads, SM::kBytes, s>>>(w.mA128, w.mAB, w.mL128,
-                                                                                       w.mLB, a);
+    tc_tile_kernel<BSZ, MODE_TRSM><<<(unsigned)grid, kTcThreads, SM::kBytes, s>>>(w.mA128, w.mL128, w.mLB, a);
     HS_CHECK_LAUNCH("tc_tile_kernel");
     return HS_OK;
 }
@@ -1088,8 +1052,6 @@ hs_status tc_attrs() {
     const int slot = BSZ == 256 ? 1 : 0;
     if (dev < 64 && g_tc_attr[dev][slot]) return HS_OK;
     HS_CUDA(cudaFuncSetAttribute(tc_tile_kernel<BSZ, MODE_TRSM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 TcSmem<BSZ>::kBytes));
-    HS_CUDA(cudaFuncSetAttribute(tc_tile_kernel<BSZ, MODE_UPDATE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  TcSmem<BSZ>::kBytes));
     HS_CUDA(cudaFuncSetAttribute(tc_update_kernel<BSZ, HS_PRECISION_TF32X3>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, UpdSmem<BSZ>::kBytes));
@@ -1147,7 +1109,6 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
     w->err = reinterpret_cast<int*>(p);
     w->flags = reinterpret_cast<unsigned*>(p + 1024);
     hs_status st = make_map(&w->mA128, w->A32, bsz, (int64_t)T, 128);
-    if (st == HS_OK) st = make_map(&w->mAB, w->A32, bsz, (int64_t)T, bsz);
     if (st == HS_OK) st = make_map(&w->mL128, w->LO, bsz, kPanelGroup * nb + 2, 128);
     if (st == HS_OK) st = make_map(&w->mLB, w->LO, bsz, kPanelGroup * nb + 2, bsz);
     if (st == HS_OK) st = make_map(&w->mU128, w->A32, bsz, (int64_t)T, 128, kUpdK);
@@ -1259,7 +1220,7 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         a.split16 = (precision == HS_PRECISION_BF16X3 || precision == HS_PRECISION_F16X3) ? precision : 0;
         a.P16 = w.P16;
         prof_begin(ctx, s, HS_KERNEL_TRSM);
-        hs_status r = bsz == 256 ? tc_launch<256>(ctx, MODE_TRSM, w, a, m, s) : tc_launch<128>(ctx, MODE_TRSM, w, a, m, s);
+        hs_status r = bsz == 256 ? tc_launch<256>(ctx, w, a, m, s) : tc_launch<128>(ctx, w, a, m, s);
         if (r != HS_OK) return r;
         prof_end(ctx, s, HS_KERNEL_TRSM, (double)m * 2.0 * bsz * bb, 4.0 * m * bb * 4.0);
         return HS_OK;
