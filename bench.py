@@ -160,6 +160,18 @@ def cpu_reference_sample(n_sample, threads):
     return time.perf_counter() - t0, "port"
 
 
+def replicas_throughput(torch, dist, t_ms, steps, world, device):
+    """Whole-job solves/s of `world` independent replicas, each having timed
+    `steps` solves in t_ms: the slowest rank's time (max over ranks, every rank
+    gets it) and world * steps / that time.  `device` holds the reduction tensor
+    (a GPU for NCCL, the CPU for gloo)."""
+    t = torch.tensor([float(t_ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_max_ms = float(t.item())
+    return t_max_ms, world * steps / (t_max_ms * 1e-3)
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -460,14 +472,10 @@ def main():
     t_ms = e0.elapsed_time(e1)
     kernels = ("update", "potrf", "trsm", "assemble", "trsv", "colupd", "symv", "vector")
     prof = {k: ctx.read_profile(k) for k in kernels}
-    t_max = torch.tensor([t_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    t_max_ms = float(t_max.item())
+    t_max_ms, value = replicas_throughput(torch, dist, t_ms, args.steps, world, dev)
     if world > 1:
         dist.barrier()
     ms_per_step = t_max_ms / args.steps
-    value = world * args.steps / (t_max_ms * 1e-3)
     mixed_report = {f: getattr(mrep, f) for f, _ in hs._lib.MixedReport._fields_ if f != "reserved"}
     x_mixed = xd.clone()
     bwd_mixed = backward_error(x_mixed)
@@ -576,10 +584,8 @@ def main():
         for _ in range(args.steps):
             _, rep = hs.gp_solve_host(ctx, Xh, yh, cfg["lengthscale"], cfg["sf2"], cfg["sn2"], **kw)
         torch.cuda.synchronize()
-        t_e2e = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * args.steps / float(t_e2e.item()), "unit": "solves/s",
+        _, e2e_value = replicas_throughput(torch, dist, (time.perf_counter() - t0) * 1e3, args.steps, world, dev)
+        e2e = {"value": e2e_value, "unit": "solves/s",
                "h2d_bytes_per_step": int(X.nbytes + y.nbytes), "d2h_bytes_per_step": int(N * 8),
                "report_ms": {"assemble+h2d": rep.assemble_ms, "factor+refine": rep.factor_ms,
                              "total": rep.total_ms}}
