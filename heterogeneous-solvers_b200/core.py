@@ -751,6 +751,8 @@ def gp_solve_host(ctx, X, y, lengthscale=1.0, signal_variance=1.0, noise_varianc
     the refinement step limit).  X, y
     and ``out`` may be CPU torch tensors (pinned memory gives asynchronous
     copies) or numpy arrays."""
+    if algorithm not in _ALGORITHMS:
+        raise ValueError(f"algorithm must be one of {sorted(_ALGORITHMS)}")
 
     def host(a, shape=None):
         if isinstance(a, torch.Tensor):
