@@ -78,6 +78,7 @@ SIGNATURES = {
     "hs_ctx_destroy": [_P],
     "hs_ctx_set_stream": [_P, _P],
     "hs_ctx_release_buffers": [_P],
+    "hs_selftest_bounded_wait": [_P, _I64],
     "hs_ctx_set_problem": [_P, _I64, _I],
     "hs_sync": [_P],
     "hs_packed_matrix_size": [_I64, _I],

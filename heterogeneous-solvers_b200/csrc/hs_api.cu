@@ -357,6 +357,12 @@ hs_status hs_ctx_take_info(hs_ctx ctx, int64_t* info) {
     return HS_OK;
 }
 
+hs_status hs_selftest_bounded_wait(hs_ctx ctx, int64_t timeout_ns) {
+    HS_API_BEGIN("hs_selftest_bounded_wait");
+    HS_ARG(timeout_ns >= 1000000 && timeout_ns <= 2000000000LL, "timeout_ns must be in [1e6, 2e9]");
+    return launch_bounded_wait_selftest(ctx, timeout_ns);
+}
+
 // ---------------------------------------------------------------- operators
 hs_status hs_potrf_block(hs_ctx ctx, double* A, int blockID, int blockRow) {
     HS_API_BEGIN("hs_potrf_block");

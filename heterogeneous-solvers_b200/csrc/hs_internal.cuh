@@ -154,6 +154,7 @@ inline size_t block_elems(const hs_ctx ctx) { return (size_t)ctx->bsz * (size_t)
 // (implemented in the k_*.cu files; all stream-ordered on ctx->stream unless a
 // stream is passed)
 hs_status launch_potrf(hs_ctx ctx, double* A, int blockID, int blockRow, cudaStream_t s);
+hs_status launch_bounded_wait_selftest(hs_ctx ctx, int64_t timeout_ns);
 hs_status launch_trsm(hs_ctx ctx, double* A, int blockID, int blockRow, int blockStart, int blockCount,
                       cudaStream_t s);
 // SYRK over diag blocks [syrkStart, syrkStart+syrkCount) and GEMM over rows

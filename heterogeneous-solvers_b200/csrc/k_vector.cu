@@ -379,6 +379,21 @@ __device__ __forceinline__ uint64_t sweep_clock_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
+// Self-test of the bounded device-side wait every spin in the library uses: one
+// thread waits on *flag, which nothing sets, the way a sweep waits on a row's flag
+// (acquire loads against a deadline on the global timer), and records the expiry
+// in *err instead of waiting on.
+__global__ void bounded_wait_kernel(const unsigned* __restrict__ flag, unsigned long long timeout_ns,
+                                    int* __restrict__ err) {
+    const uint64_t deadline = sweep_clock_ns() + timeout_ns;
+    while (ld_acquire_u32(flag) == 0u) {
+        if (sweep_clock_ns() > deadline) {
+            atomicExch(err, 1);
+            return;
+        }
+    }
+}
+
 // hint: bring `bytes` (a multiple of 16) at p (16-byte aligned) into L2
 __device__ __forceinline__ void sweep_prefetch_l2(const void* p, uint32_t bytes) {
     const char* b = static_cast<const char*>(p);
@@ -730,6 +745,28 @@ hs_status launch_column_update(hs_ctx ctx, const double* A, double* b, int block
     HS_CHECK_LAUNCH("column_update");
     prof_end(ctx, s, HS_KERNEL_COLUPD, 2.0 * blockCount * (double)bsz * bsz,
              (double)blockCount * bsz * bsz * 8.0 + 24.0 * blockCount * bsz);
+    return HS_OK;
+}
+
+hs_status launch_bounded_wait_selftest(hs_ctx ctx, int64_t timeout_ns) {
+    hs_status st = ensure_scratch(ctx, kSmallScratch);
+    if (st != HS_OK) return st;
+    char* base = static_cast<char*>(ctx->scratch);
+    unsigned* flag = reinterpret_cast<unsigned*>(base);
+    int* err = reinterpret_cast<int*>(base + 256);
+    cudaStream_t s = ctx->stream;
+    HS_CUDA(cudaMemsetAsync(base, 0, 512, s));
+    ctx->launches += 1;
+    bounded_wait_kernel<<<1, 1, 0, s>>>(flag, (unsigned long long)timeout_ns, err);
+    HS_CHECK_LAUNCH("bounded_wait");
+    int e = 0;
+    HS_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HS_CUDA(cudaStreamSynchronize(s));
+    if (e) {
+        set_error("hs_selftest_bounded_wait: the device-side wait ran out and returned an error status "
+                  "(expected: nothing sets its flag)");
+        return HS_ERR_TIMEOUT;
+    }
     return HS_OK;
 }
 

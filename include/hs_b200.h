@@ -127,6 +127,12 @@ hs_status hs_potrf_block(hs_ctx ctx, double* A, int blockID, int blockRow);
  * the last call saw positive pivots, else the smallest failing global row.
  * Synchronises the stream. */
 hs_status hs_ctx_take_info(hs_ctx ctx, int64_t* info);
+/* Self-test of the failure path of every device-side wait in the library (no
+ * reference counterpart): one device thread waits on a flag that nothing sets, with
+ * the bounded wait the sweeps and tensor-core kernels use, for timeout_ns
+ * (1e6 .. 2e9).  Returns HS_ERR_TIMEOUT when the wait ran out (the expected
+ * outcome; the context stays usable), HS_OK if the flag was seen set. */
+hs_status hs_selftest_bounded_wait(hs_ctx ctx, int64_t timeout_ns);
 
 /* MatrixMatrixOperations::triangularSolve{,_optimizedGPU,_optimizedCPU}
  * (MatrixMatrixOperations.hpp:29,53,77; .cpp:5-144): B <- B L^-T for the blocks
