@@ -12,10 +12,12 @@ the steps against the oracle (CPU suite) and against the CUDA library (GPU
 suite).
 
 Usage (needs the reference checkout; the JSON it writes is committed):
-    python tests/golden/extract_reference_tests.py /root/reference
+    python tests/golden/extract_reference_tests.py <reference checkout>
+or with the checkout in the environment variable HS_REFERENCE_ROOT.
 """
 import json
 import math
+import os
 import re
 import sys
 from pathlib import Path
@@ -212,4 +214,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HS_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: extract_reference_tests.py <reference checkout> (or set HS_REFERENCE_ROOT)")
+    main(root)
