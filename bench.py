@@ -15,10 +15,10 @@ comparison at equal error), with both backward errors.
 Prints one JSON line on rank 0.  `value` is whole-job throughput in solves/s
 (N independent replicas under torchrun: the path does not shard).  `e2e` is
 the same metric through hs_gp_solve_host (the mixed algorithm of the headline's
-split variant) with pinned host buffers.  The
-reference arm (--impl reference) times the CPU restatement of the reference's
-CPU path (or its sources compiled through oracle/ref_build.py when present) on
-a bounded sample and extrapolates by N^3.
+split variant) with pinned host buffers.  The reference arm (--impl reference)
+times the CPU restatement of the reference's CPU path (RBF assembly, factor,
+solve) on a bounded sample and extrapolates it by an exponent fitted in the
+same run.
 """
 import argparse
 import json
@@ -61,7 +61,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=None, help="override N (smaller runs for profiling)")
-    ap.add_argument("--cg-iters", type=int, default=30, help="CG iterations timed for the matvec roofline")
+    ap.add_argument("--cg-iters", type=int, default=20000,
+                    help="iteration cap (iMax) of the CG solve to eps = 1e-10 on the benchmark system (0: skip)")
     ap.add_argument("--cpu-sample-n", type=int, default=8192)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -77,7 +78,9 @@ def parse_args():
     ap.add_argument("--fit", action="store_true",
                     help="hyperparameter fit: L-BFGS on the FP64 NLML + gradient (ARD RBF, d=8) at --fit-n, "
                          "--fit-steps iterations (one JSON line)")
-    ap.add_argument("--fit-n", type=int, default=65536)
+    ap.add_argument("--fit-n", type=int, default=65536,
+                    help="N of the L-BFGS configuration (--fit); the default run times one NLML + gradient of both "
+                         "forms there (0: skip)")
     ap.add_argument("--fit-steps", type=int, default=30)
     return ap.parse_args()
 
@@ -129,35 +132,91 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU baseline
-def cpu_reference_sample(n_sample, threads):
-    """Times the reference's CPU path (factor + solve) at N = n_sample with the
-    full configuration otherwise; returns (seconds, kind)."""
+def host_facts():
+    """CPU model, logical cores and RAM of this host (from /proc)."""
+    model, mem_gb = None, None
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+        for line in Path("/proc/meminfo").read_text().splitlines():
+            if line.startswith("MemTotal"):
+                mem_gb = int(line.split()[1]) / 1024 ** 2
+                break
+    except OSError:
+        pass
+    return {"cpu_model": model, "logical_cores": os.cpu_count(), "ram_gb": mem_gb}
+
+
+def _oracle(threads):
+    """The CPU restatement of the reference's CPU path (test infrastructure),
+    with OpenMP limited to `threads`."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    os.environ.setdefault("OMP_PROC_BIND", "close")
     sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib
+    return oracle_lib
+
+
+def cpu_solve_sample(n_sample, threads, workload=WORKLOAD):
+    """The reference's CPU path (init_gpu_perc=0) on one system of `workload`'s
+    configuration at N = n_sample: RBF assembly (MatrixGenerator.cpp:73-162),
+    blocked Cholesky factor (Cholesky.cpp:413-493, cpu_opt=2) and forward/back
+    solve (TriangularSystemSolver.cpp:15-105).  Returns seconds per phase."""
     import numpy as np
+    ol = _oracle(threads)
     hs = load_package()
     wl = __import__("hs_b200.workloads", fromlist=["CONFIGS"])
-    cfg = wl.CONFIGS[WORKLOAD]
+    cfg = wl.CONFIGS[workload]
     X, y = wl.gp_inputs(n_sample, cfg["d"], cfg["seed"])
-    ref_bin = ROOT / "oracle" / "_ref" / "ref_cholesky"
-    if ref_bin.exists():
-        # the reference's own sources (oracle/ref_build.py): prints the factor+solve seconds
-        inp = ROOT / "oracle" / "_ref" / "bench_inputs.bin"
-        np.concatenate([X.ravel(), y]).tofile(inp)
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close")
-        out = subprocess.run([str(ref_bin), str(inp), str(n_sample), str(cfg["d"]), str(cfg["bsz"]),
-                              repr(cfg["lengthscale"]), repr(cfg["sn2"])], capture_output=True, text=True, env=env,
-                             check=True)
-        return float(json.loads(out.stdout.strip().splitlines()[-1])["seconds"]), "reference"
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    import oracle_lib as ol
     bsz = cfg["bsz"]
-    K = ol.rbf_assemble(X, bsz, cfg["lengthscale"], cfg["sf2"], cfg["sn2"])
     b = np.zeros(hs.padded_size(n_sample, bsz))
     b[:n_sample] = y
     t0 = time.perf_counter()
+    K = ol.rbf_assemble(X, bsz, cfg["lengthscale"], cfg["sf2"], cfg["sn2"])
+    t1 = time.perf_counter()
     L = ol.cholesky(K, n_sample, bsz)
     ol.triangular_solve(L, b, n_sample, bsz)
-    return time.perf_counter() - t0, "port"
+    t2 = time.perf_counter()
+    return {"assemble_s": t1 - t0, "factor_solve_s": t2 - t1, "total_s": t2 - t0}
+
+
+def cpu_scaling_fit(threads, sizes=(4096, 8192, 16384)):
+    """Times cpu_solve_sample at each size once and fits t = c N^p by least
+    squares in log-log space; returns p and the samples."""
+    import numpy as np
+    samples = {n: cpu_solve_sample(n, threads) for n in sizes}
+    ns = np.array(sizes, dtype=float)
+    ts = np.array([samples[n]["total_s"] for n in sizes])
+    p = float(np.polyfit(np.log(ns), np.log(ts), 1)[0])
+    return p, {str(n): samples[n] for n in sizes}
+
+
+def cpu_c1_full(threads):
+    """The small configuration run in full on the CPU path: N=4096, d=8, l=0.5,
+    sn2=1e-2, bsz=128; assembly, factor + solve, and CG to eps=1e-10 with the
+    reference's CPU dot product (one chunk per core, VectorOperations.cpp:187-238)."""
+    import numpy as np
+    ol = _oracle(threads)
+    hs = load_package()
+    wl = __import__("hs_b200.workloads", fromlist=["CONFIGS"])
+    cfg = wl.CONFIGS["c1_n4096"]
+    N, bsz = cfg["N"], cfg["bsz"]
+    X, y = wl.gp_inputs(N, cfg["d"], cfg["seed"])
+    b = np.zeros(hs.padded_size(N, bsz))
+    b[:N] = y
+    t0 = time.perf_counter()
+    K = ol.rbf_assemble(X, bsz, cfg["lengthscale"], cfg["sf2"], cfg["sn2"])
+    t1 = time.perf_counter()
+    L = ol.cholesky(K, N, bsz)
+    x = ol.triangular_solve(L, b, N, bsz)
+    t2 = time.perf_counter()
+    x_cg, its, dn, d0 = ol.cg(K, b, N, bsz, cfg["eps"], 100000, chunks=threads)
+    t3 = time.perf_counter()
+    return {"workload": "c1_n4096: N=4096, d=8, l=0.5, sn2=1e-2, bsz=128", "assemble_s": t1 - t0,
+            "factor_solve_s": t2 - t1, "cg_s": t3 - t2, "cg_iterations": int(its), "cg_chunks": threads,
+            "cg_x_rel_diff_vs_factor": float(np.linalg.norm(x_cg - x) / np.linalg.norm(x))}
 
 
 def replicas_throughput(torch, dist, t_ms, steps, world, device):
@@ -173,28 +232,34 @@ def replicas_throughput(torch, dist, t_ms, steps, world, device):
 
 
 def run_reference_arm(args, rank, world):
+    """The reference's CPU path on this host's cores (rank 0 only): each step
+    assembles, factors and solves one system of the benchmark's configuration at
+    N = --cpu-sample-n, and is extrapolated to the full N by the exponent
+    fitted to samples at N = 4096, 8192, 16384 timed in the same run."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
     N = args.n or 131072
-    scale = (N / args.cpu_sample_n) ** 3
+    p, fit_samples = cpu_scaling_fit(threads)
+    scale = (N / args.cpu_sample_n) ** p
     for _ in range(args.warmup):
-        cpu_reference_sample(args.cpu_sample_n, threads)
-    times = []
-    kind = "port"
-    for _ in range(args.steps):
-        t, kind = cpu_reference_sample(args.cpu_sample_n, threads)
-        times.append(t * scale)
-    t_full = sum(times) / len(times)
+        cpu_solve_sample(args.cpu_sample_n, threads)
+    steps = [cpu_solve_sample(args.cpu_sample_n, threads) for _ in range(args.steps)]
+    t_sample = sum(s_["total_s"] for s_ in steps) / len(steps)
+    t_full = t_sample * scale
     value = 1.0 / t_full
-    sample = (f"FP64 factor+solve at N={args.cpu_sample_n} (same d, l, sn2, bsz), "
-              f"extrapolated by (N/{args.cpu_sample_n})^3 to N={N}")
+    sample = (f"RBF assembly + FP64 blocked Cholesky factor + forward/back solve at N={args.cpu_sample_n} "
+              f"(same d, l, sn2, bsz), {t_sample:.3f} s a step, extrapolated to N={N} by (N/{args.cpu_sample_n})^p "
+              f"with p = {p:.3f} fitted to N = 4096, 8192, 16384 in this run")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_full * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(bench_config(N), implementation="the reference's CPU path (init_gpu_perc=0): "
-                                                          "FP64 blocked Cholesky factor + forward/back solve"),
-            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind, "sample": sample},
+            "config": dict(bench_config(N), implementation="the reference's CPU path (init_gpu_perc=0): RBF "
+                                                          "assembly + FP64 blocked Cholesky factor + forward/back "
+                                                          "solve"),
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample,
+                             "host": host_facts(), "sample_seconds_per_step": t_sample, "fitted_exponent": p,
+                             "fit_samples": fit_samples, "c1_full": cpu_c1_full(threads)},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -223,11 +288,13 @@ def measure_gemm_peak(torch, device, dtype, tf32=False):
     return best
 
 
-def bench_lml(hs, torch, device, N, steps):
+def bench_lml(hs, torch, device, N, steps, precision="f16x3"):
     """NLML + gradient of an ARD RBF GP: X ~ U[0,1]^(N x 8), l_k ~ LogUniform[0.2, 2],
     sf2 = 1, sn2 = 1e-3, y drawn from the GP prior plus noise (a dense FP64
-    Cholesky of K through torch draws it; not timed).  Times hs_gp_nlml_grad
-    (assembly, FP64 factor, solve, reverse-mode Cholesky, gradient contraction)."""
+    Cholesky of K through torch draws it at N <= 32768, else y = sin(sum x) + noise;
+    not timed).  Times hs_gp_nlml_grad (assembly, FP64 factor, solve, reverse-mode
+    Cholesky, gradient contraction) and the same through the mixed-precision factor
+    (hs_gp_nlml_grad_mixed), with the mixed results' errors against the FP64 ones."""
     import numpy as np
     d, bsz = 8, 256
     rng = np.random.default_rng(4)
@@ -236,34 +303,53 @@ def bench_lml(hs, torch, device, N, steps):
     theta = np.concatenate([np.log(ell), [0.0, np.log(1e-3)]])
     dev = f"cuda:{device}"
     Xd = torch.from_numpy(X).to(dev)
-    Xs = Xd / torch.from_numpy(ell).to(dev)
-    K = torch.exp(-0.5 * torch.cdist(Xs, Xs).square()) + 1e-3 * torch.eye(N, dtype=torch.float64, device=dev)
-    z = torch.from_numpy(rng.standard_normal(N)).to(dev)
-    yd = torch.linalg.cholesky(K) @ z
-    del K, Xs
+    if N <= 32768:
+        Xs = Xd / torch.from_numpy(ell).to(dev)
+        K = torch.exp(-0.5 * torch.cdist(Xs, Xs).square()) + 1e-3 * torch.eye(N, dtype=torch.float64, device=dev)
+        z = torch.from_numpy(rng.standard_normal(N)).to(dev)
+        yd = torch.linalg.cholesky(K) @ z
+        del K, Xs
+        ydesc = "y ~ GP prior"
+    else:
+        yd = torch.from_numpy(np.sin(X.sum(axis=1)) + 0.1 * rng.standard_normal(N)).to(dev)
+        ydesc = "y = sin(sum x) + N(0, 0.1^2)"
     torch.cuda.empty_cache()
     c = hs.Context(device=device, N=N, matrixBlockSize=bsz)
-    hs.gp_nlml_grad(c, Xd, yd, theta)  # warm-up
-    torch.cuda.synchronize()
-    c.reset_profile()
-    c.set_profiling(True)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        nlml, grad, rep = hs.gp_nlml_grad(c, Xd, yd, theta)
-    t_ms = (time.perf_counter() - t0) * 1e3 / steps
-    c.set_profiling(False)
-    adj = c.read_profile("adjoint")
+    out = {"workload": f"GP NLML + gradient, ARD RBF, N={N}, d={d}, bsz={bsz}, sn2=1e-3, {ydesc}"}
+    for prec in (None, precision):
+        hs.gp_nlml_grad(c, Xd, yd, theta, precision=prec)  # warm-up (workspace, kernel loading)
+        torch.cuda.synchronize()
+        c.reset_profile()
+        c.set_profiling(prec is None)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            nlml, grad, rep = hs.gp_nlml_grad(c, Xd, yd, theta, precision=prec)
+        t_ms = (time.perf_counter() - t0) * 1e3 / steps
+        c.set_profiling(False)
+        row = {"ms_per_call": t_ms, "nlml": nlml, "grad": [float(v) for v in grad],
+               "phases_ms": {"assemble+factor(+refine)": rep["factor_ms"], "solve+adjoint": rep["adjoint_ms"],
+                             "gradient": rep["grad_ms"]}, "logdet": rep["logdet"], "data_fit": rep["data_fit"]}
+        if prec is None:
+            adj = c.read_profile("adjoint")
+            row["adjoint_dmma_tflops"] = adj["flops"] / (adj["ms"] * 1e-3) / 1e12 if adj["ms"] else None
+            row["useful_tflops_whole"] = (N ** 3 / 3 + 2 * N ** 3 / 3) / (t_ms * 1e-3) / 1e12
+            out["fp64"] = row
+        else:
+            row["mixed_report"] = rep["mixed"]
+            g64 = np.asarray(out["fp64"]["grad"])
+            row["grad_rel_err_vs_fp64"] = float(np.linalg.norm(grad - g64) / np.linalg.norm(g64))
+            row["grad_max_component_rel_err_vs_fp64"] = float(np.max(np.abs(grad - g64) / np.abs(g64)))
+            row["nlml_abs_diff_vs_fp64"] = abs(nlml - out["fp64"]["nlml"])
+            row["logdet_abs_diff_vs_fp64"] = abs(rep["logdet"] - out["fp64"]["logdet"])
+            row["data_fit_rel_diff_vs_fp64"] = abs(rep["data_fit"] - out["fp64"]["data_fit"]) / abs(
+                out["fp64"]["data_fit"])
+            row["speedup_vs_fp64"] = out["fp64"]["ms_per_call"] / t_ms
+            out[prec] = row
     c.close()
-    return {"workload": f"GP NLML + gradient, ARD RBF, N={N}, d={d}, bsz={bsz}, sn2=1e-3, y ~ GP prior",
-            "ms_per_call": t_ms, "nlml": nlml, "grad_norm": float(np.linalg.norm(grad)),
-            "phases_ms": {"assemble+factor": rep["factor_ms"], "solve+adjoint": rep["adjoint_ms"],
-                          "gradient": rep["grad_ms"]},
-            "adjoint_dmma_tflops": adj["flops"] / (adj["ms"] * 1e-3) / 1e12 if adj["ms"] else None,
-            "adjoint_launches_per_call": adj["launches"] / steps,
-            "useful_tflops_whole": (N ** 3 / 3 + 2 * N ** 3 / 3) / (t_ms * 1e-3) / 1e12}
+    return out
 
 
-def run_fit(hs, torch, device, N, steps):
+def run_fit(hs, torch, device, N, steps, precision=None):
     """Hyperparameter fit of an ARD RBF GP by L-BFGS (hs.fit_hyperparameters: scipy's
     L-BFGS-B over the library's FP64 NLML and analytic gradient): X ~ U[0,1]^(N x 8),
     y = sin(sum_k x_k) + N(0, 0.1^2), theta0 = [log l_k = 0, log sf2 = 0, log sn2 = log 1e-2],
@@ -277,12 +363,18 @@ def run_fit(hs, torch, device, N, steps):
     c = hs.Context(device=device, N=N, matrixBlockSize=bsz)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    res = hs.fit_hyperparameters(c, X, y, theta0, maxiter=steps)
+    res = hs.fit_hyperparameters(c, X, y, theta0, maxiter=steps, precision=precision)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
+    # both forms' gradients at the fitted theta, against the FP64 one
+    _, g64, _ = hs.gp_nlml_grad(c, X, y, res["theta"])
+    gm = g64 if precision is None else hs.gp_nlml_grad(c, X, y, res["theta"], precision=precision)[1]
     c.close()
     ev = np.asarray(res["eval_seconds"])
-    return {"workload": f"L-BFGS hyperparameter fit, ARD RBF, N={N}, d={d}, bsz={bsz}, FP64 NLML + gradient",
+    form = "FP64" if precision is None else f"mixed-precision ({precision} factor, FP64 refinement)"
+    return {"workload": f"L-BFGS hyperparameter fit, ARD RBF, N={N}, d={d}, bsz={bsz}, {form} NLML + gradient",
+            "grad_at_result_rel_err_vs_fp64": float(np.linalg.norm(gm - g64) / np.linalg.norm(g64)),
+            "seconds_per_step": wall / max(1, res["iterations"]),
             "max_iterations": steps, "iterations": res["iterations"], "evaluations": res["evaluations"],
             "fit_seconds": wall, "eval_seconds_median": float(np.median(ev)), "eval_seconds_max": float(ev.max()),
             "nlml_initial": res["nlml_trace"][0], "nlml_final": res["nlml"],
@@ -381,10 +473,16 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", device))
 
     if args.fit:
-        fit = run_fit(hs, torch, device, args.fit_n, args.fit_steps)
+        fits = {"fp64": run_fit(hs, torch, device, args.fit_n, args.fit_steps)}
+        fits[args.precision] = run_fit(hs, torch, device, args.fit_n, args.fit_steps, precision=args.precision)
+        m, f = fits[args.precision], fits["fp64"]
+        cmp = {"speedup_per_step": f["seconds_per_step"] / m["seconds_per_step"],
+               "speedup_whole_fit": f["fit_seconds"] / m["fit_seconds"],
+               "nlml_final_diff": m["nlml_final"] - f["nlml_final"],
+               "theta_final_max_abs_diff": float(max(abs(a - b) for a, b in zip(m["theta_final"], f["theta_final"])))}
         if rank == 0:
             print(json.dumps({"metric": METRIC, "mode": "hyperparameter fit", "n_gpus": world, "data": "synthetic",
-                              "fit": fit}), flush=True)
+                              "fit": fits, "mixed_vs_fp64": cmp}), flush=True)
         if world > 1:
             dist.destroy_process_group()
         return
@@ -524,27 +622,30 @@ def main():
         f1.record()
         torch.cuda.synchronize()
         ctx.set_profiling(False)
-        upd64 = ctx.read_profile("update")
+        prof64 = {k: ctx.read_profile(k) for k in ("update", "potrf", "trsm", "trsv", "colupd", "assemble")}
+        upd64 = prof64["update"]
         fp64_ms = f0.elapsed_time(f1)
         logdet64 = hs.cholesky_logdet(ctx, A)
         bwd64 = backward_error(x64)
+        dgemm = measure_gemm_peak(torch, device, torch.float64)
+        fac = (N ** 3 / 3) / (fp64_ms * 1e-3) / 1e12
+        upd_tf = upd64["flops"] / (upd64["ms"] * 1e-3) / 1e12 if upd64["ms"] else None
         fp64 = {"ms_per_step": fp64_ms, "solves_per_s": 1e3 / fp64_ms, "backward_error": bwd64,
-                "factor_tflops_whole": (N ** 3 / 3) / (fp64_ms * 1e-3) / 1e12,
-                "update_dmma_tflops": upd64["flops"] / (upd64["ms"] * 1e-3) / 1e12 if upd64["ms"] else None,
+                "factor_tflops_whole": fac, "update_dmma_tflops": upd_tf,
+                "dgemm_peak_tflops": dgemm,
+                "dgemm_peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul, FP64) measured in this run, best of 5",
+                "factor_frac_of_dgemm": fac / dgemm, "update_frac_of_dgemm": upd_tf / dgemm if upd_tf else None,
+                "phases_ms": {k: v["ms"] for k, v in prof64.items() if v["launches"]},
+                "phases_tflops": {k: v["flops"] / (v["ms"] * 1e-3) / 1e12 for k, v in prof64.items()
+                                  if v["launches"] and v["ms"] and k in ("update", "potrf", "trsm")},
                 "speedup_mixed_vs_fp64": fp64_ms / ms_per_step}
         fp64["mixed_x_rel_diff"] = float((torch.linalg.norm(x_mixed - x64) / torch.linalg.norm(x64)).item())
         if alt is not None:
             alt["speedup_vs_fp64"] = fp64_ms / alt["ms_per_step"]
         fp64["mixed_logdet_rel_diff"] = abs(mixed_report["logdet"] - logdet64) / abs(logdet64)
         fp64["logdet"] = logdet64
-        del x64
 
-    # ---------------- GP NLML + gradient (ARD, d = 8) at N = 16384
-    lml = None
-    if args.lml_n > 0:
-        lml = bench_lml(hs, torch, ctx.device, args.lml_n, args.lml_steps)
-
-    # ---------------- CG matvec roofline: a bounded number of CG iterations on K
+    # ---------------- CG on the same system to eps = 1e-10 (CG.cpp:38-163), against the FP64 solve
     cg_info = None
     if args.cg_iters > 0:
         assemble()
@@ -560,12 +661,21 @@ def main():
         torch.cuda.synchronize()
         ctx.set_profiling(False)
         symv = ctx.read_profile("symv")
-        cg_info = {"iterations": it.value, "ms_per_iteration": c0.elapsed_time(c1) / max(1, it.value),
-                   "rel_residual_sq": dn.value / d0.value if d0.value else None, "status": int(st),
-                   "matvec_ms": symv["ms"] / max(1, symv["launches"]),
+        cg_ms = c0.elapsed_time(c1)
+        r_cg = torch.empty_like(bd)
+        hs.MatrixVectorOperations.matrixVectorBlock(ctx, A, x_cg, r_cg, 0, 0, nb, nb, nb)
+        cg_info = {"epsilon": cfg["eps"], "iMax": args.cg_iters, "status": hs._lib.STATUS_NAMES.get(int(st), int(st)),
+                   "iterations": it.value, "ms": cg_ms, "ms_per_iteration": cg_ms / max(1, it.value),
+                   "rel_residual": (dn.value / d0.value) ** 0.5 if d0.value else None,
+                   "true_rel_residual": (torch.linalg.norm(r_cg - bd) / torch.linalg.norm(bd)).item(),
+                   "matvecs": symv["launches"], "matvec_ms": symv["ms"] / max(1, symv["launches"]),
                    "matvec_gbs": symv["bytes"] / (symv["ms"] * 1e-3) / 1e9 if symv["ms"] else None,
                    "matvec_frac_of_hbm": None}
-        del x_cg
+        if fp64 is not None:
+            cg_info["x_rel_diff_vs_fp64_solve"] = float((torch.linalg.norm(x_cg - x64) / torch.linalg.norm(x64)).item())
+        del x_cg, r_cg
+    if fp64 is not None:
+        del x64
 
     # ---------------- e2e through the host-buffer API (mixed precision, algorithm 2)
     e2e = None
@@ -589,6 +699,19 @@ def main():
                "h2d_bytes_per_step": int(X.nbytes + y.nbytes), "d2h_bytes_per_step": int(N * 8),
                "report_ms": {"assemble+h2d": rep.assemble_ms, "factor+refine": rep.factor_ms,
                              "total": rep.total_ms}}
+
+    # ---------------- GP NLML + gradient (ARD, d = 8): FP64 and mixed-precision forms, at
+    # N = --lml-n and at the L-BFGS configuration's N = --fit-n (the main system's
+    # buffers are released first)
+    lml = None
+    if args.lml_n > 0 or args.fit_n > 0:
+        lib.hs_ctx_release_buffers(ctx.handle)
+        torch.cuda.empty_cache()
+        lml = {}
+        if args.lml_n > 0:
+            lml[str(args.lml_n)] = bench_lml(hs, torch, ctx.device, args.lml_n, args.lml_steps)
+        if args.fit_n > 0 and args.fit_n != args.lml_n:
+            lml[str(args.fit_n)] = bench_lml(hs, torch, ctx.device, args.fit_n, 1)
 
     # ---------------- roofline of the dominant kernel (tensor-core trailing update)
     upd = prof["update"]
@@ -626,11 +749,14 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        t_s, kind = cpu_reference_sample(args.cpu_sample_n, threads)
-        t_full = t_s * (N / args.cpu_sample_n) ** 3
-        cpu = {"value": 1.0 / t_full, "unit": "solves/s", "cores": threads, "kind": kind,
-               "sample": f"FP64 factor+solve at N={args.cpu_sample_n}, extrapolated by N^3 to N={N}",
-               "sample_seconds": t_s}
+        p, fit_samples = cpu_scaling_fit(threads)
+        t_s = fit_samples[str(args.cpu_sample_n)]["total_s"] if str(args.cpu_sample_n) in fit_samples else \
+            cpu_solve_sample(args.cpu_sample_n, threads)["total_s"]
+        t_full = t_s * (N / args.cpu_sample_n) ** p
+        cpu = {"value": 1.0 / t_full, "unit": "solves/s", "cores": threads, "kind": "port",
+               "sample": f"RBF assembly + FP64 factor + solve at N={args.cpu_sample_n} ({t_s:.3f} s), extrapolated "
+                         f"to N={N} by (N/{args.cpu_sample_n})^p, p = {p:.3f} fitted to N = 4096, 8192, 16384",
+               "host": host_facts(), "fitted_exponent": p, "fit_samples": fit_samples}
 
     if rank == 0:
         phases = {k: {"launches": v["launches"], "ms_per_step": v["ms"] / args.steps,

@@ -114,6 +114,8 @@ SIGNATURES = {
     "hs_matrix_vector_gp": [_P, _P, _P, _P, _I64, _I64],
     "hs_gp_predict": [_P, _P, _P, _I64, _I, _P, _I, _D, _P, _P],
     "hs_gp_nlml_grad": [_P, _P, _P, _I, _P, _I, ctypes.POINTER(_D), _P, ctypes.POINTER(GpReport)],
+    "hs_gp_nlml_grad_mixed": [_P, _P, _P, _I, _P, _I, _I, _D, ctypes.POINTER(_D), _P, ctypes.POINTER(GpReport),
+                              ctypes.POINTER(MixedReport)],
 }
 _RESTYPES = {"hs_abi_version": _I, "hs_last_error": ctypes.c_char_p, "hs_status_string": ctypes.c_char_p,
              "hs_packed_matrix_size": _I64, "hs_padded_vector_size": _I64, "hs_ctx_launch_count": _I64}

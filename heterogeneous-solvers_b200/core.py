@@ -461,11 +461,15 @@ def cholesky_adjoint(ctx, L, Abar):
     return Abar
 
 
-def gp_nlml_grad(ctx, X, y, theta, n_ell=None):
+def gp_nlml_grad(ctx, X, y, theta, n_ell=None, precision=None, tol=1e-14):
     """GP negative log marginal likelihood and its gradient with respect to
     theta = [log l_1..log l_n_ell, log sf2, log sn2] (FP64 factor, reverse-mode
     Cholesky and an on-the-fly dK/dtheta contraction).  X (N x d) and y (N)
-    may be host or device float64 arrays; returns (nlml, grad ndarray, report)."""
+    may be host or device float64 arrays; returns (nlml, grad ndarray, report).
+    With ``precision`` ("tf32x3", "bf16x3" or "f16x3") the factor is the
+    mixed-precision one (hs_gp_nlml_grad_mixed): alpha refined in FP64 to the
+    backward error ``tol``; the report then also holds the solve's report under
+    "mixed"."""
     Xd = X if isinstance(X, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(X, dtype=np.float64))
     yd = y if isinstance(y, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(y, dtype=np.float64))
     Xd = _to_device(Xd.to(torch.float64), ctx).contiguous()
@@ -480,18 +484,29 @@ def gp_nlml_grad(ctx, X, y, theta, n_ell=None):
     nlml = ctypes.c_double()
     grad = np.zeros(n_ell + 2)
     rep = GpReport()
-    call("hs_gp_nlml_grad", ctx.handle, _dptr(Xd, ctx), _dptr(yd, ctx), int(Xd.shape[1]),
-         th.ctypes.data_as(ctypes.c_void_p), int(n_ell), ctypes.byref(nlml), grad.ctypes.data_as(ctypes.c_void_p),
-         ctypes.byref(rep))
-    return nlml.value, grad, {f: getattr(rep, f) for f, _ in GpReport._fields_}
+    if precision is None or precision == "fp64":
+        call("hs_gp_nlml_grad", ctx.handle, _dptr(Xd, ctx), _dptr(yd, ctx), int(Xd.shape[1]),
+             th.ctypes.data_as(ctypes.c_void_p), int(n_ell), ctypes.byref(nlml),
+             grad.ctypes.data_as(ctypes.c_void_p), ctypes.byref(rep))
+        return nlml.value, grad, {f: getattr(rep, f) for f, _ in GpReport._fields_}
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+    mrep = MixedReport()
+    call("hs_gp_nlml_grad_mixed", ctx.handle, _dptr(Xd, ctx), _dptr(yd, ctx), int(Xd.shape[1]),
+         th.ctypes.data_as(ctypes.c_void_p), int(n_ell), int(PRECISIONS[precision]), float(tol), ctypes.byref(nlml),
+         grad.ctypes.data_as(ctypes.c_void_p), ctypes.byref(rep), ctypes.byref(mrep))
+    out = {f: getattr(rep, f) for f, _ in GpReport._fields_}
+    out["mixed"] = {f: getattr(mrep, f) for f, _ in MixedReport._fields_ if f != "reserved"}
+    return nlml.value, grad, out
 
 
-def fit_hyperparameters(ctx, X, y, theta0, maxiter=30, n_ell=None, bounds=None):
+def fit_hyperparameters(ctx, X, y, theta0, maxiter=30, n_ell=None, bounds=None, precision=None, tol=1e-14):
     """Fit theta = [log l_1..log l_n_ell, log sf2, log sn2] by L-BFGS (scipy's
-    L-BFGS-B) on the NLML and its analytic gradient (hs_gp_nlml_grad).  X and y
-    are copied to the device once.  Returns a dict with theta, nlml, the
-    number of L-BFGS iterations and function evaluations, and the wall time of
-    every NLML + gradient evaluation."""
+    L-BFGS-B) on the NLML and its analytic gradient (hs_gp_nlml_grad, or the
+    mixed-precision form with ``precision``).  X and y are copied to the device
+    once.  Returns a dict with theta, nlml, the number of L-BFGS iterations and
+    function evaluations, and the wall time of every NLML + gradient
+    evaluation."""
     from scipy.optimize import minimize
 
     Xd = X if isinstance(X, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(X, dtype=np.float64))
@@ -504,7 +519,7 @@ def fit_hyperparameters(ctx, X, y, theta0, maxiter=30, n_ell=None, bounds=None):
 
     def fun(th):
         t0 = time.perf_counter()
-        v, g, _ = gp_nlml_grad(ctx, Xd, yd, th, n_ell)
+        v, g, _ = gp_nlml_grad(ctx, Xd, yd, th, n_ell, precision=precision, tol=tol)
         evals.append({"seconds": time.perf_counter() - t0, "nlml": v})
         return v, g
 

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "hs_gp.cuh"
+#include "hs_mixed.cuh"
 
 namespace hs {
 namespace {
@@ -53,6 +54,34 @@ __global__ void nlml_terms_kernel(const double* __restrict__ y, const double* __
         out[0] = s0;
         out[1] = s1;
     }
+}
+
+// FP64 packed copy of the mixed factor's off-diagonal FP32 blocks (diagonal blocks
+// skipped); one CTA a block, grid-stride over the blocks
+__global__ void offdiag_f32_to_f64_kernel(const float* __restrict__ A32, double* __restrict__ L, int nb, int bsz) {
+    const int64_t bb = (int64_t)bsz * bsz;
+    const int64_t T = (int64_t)nb * (nb + 1) / 2;
+    for (int64_t id = blockIdx.x; id < T; id += gridDim.x) {
+        int i, j;
+        block_coords(id, nb, &i, &j);
+        if (i == j) continue;
+        const float4* src = reinterpret_cast<const float4*>(A32 + id * bb);
+        double2* dst = reinterpret_cast<double2*>(L + id * bb);
+        for (int64_t e = threadIdx.x; e < bb / 4; e += blockDim.x) {
+            const float4 v = __ldcs(src + e);
+            __stcs(dst + 2 * e, make_double2(v.x, v.y));
+            __stcs(dst + 2 * e + 1, make_double2(v.z, v.w));
+        }
+    }
+}
+
+// X = Y^T (one bsz x bsz block)
+__global__ void transpose_kernel(const double* __restrict__ Y, double* __restrict__ X, int n) {
+    __shared__ double t[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) t[i][threadIdx.x] = Y[(size_t)(by + i) * n + bx + threadIdx.x];
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) X[(size_t)(bx + i) * n + by + threadIdx.x] = t[threadIdx.x][i];
 }
 
 __global__ void copy_pad_kernel(const double* __restrict__ y, double* __restrict__ b, int64_t N, int64_t n) {
@@ -211,8 +240,9 @@ hs_status hs_cholesky_adjoint(hs_ctx ctx, const double* L, double* Abar) {
     return HS_OK;
 }
 
-hs_status hs_gp_nlml_grad(hs_ctx ctx, const double* X, const double* y, int d, const double* theta, int n_ell,
-                          double* nlml, double* grad, hs_gp_report* report) {
+static hs_status gp_nlml_grad_impl(hs_ctx ctx, const double* X, const double* y, int d, const double* theta,
+                                   int n_ell, int precision, double tol, double* nlml, double* grad,
+                                   hs_gp_report* report, hs_mixed_report* mreport) {
     hs_status st = require_ctx(ctx, "hs_gp_nlml_grad");
     if (st != HS_OK) return st;
     if (!X || !y || !theta || !nlml) {
@@ -236,6 +266,7 @@ hs_status hs_gp_nlml_grad(hs_ctx ctx, const double* X, const double* y, int d, c
     const int nb = ctx->nb, bsz = ctx->bsz;
     const int64_t N = ctx->N, n = (int64_t)nb * bsz;
     const size_t packed = (size_t)total_blocks(nb) * bsz * bsz;
+    const size_t bb = (size_t)bsz * bsz;
     std::vector<double> ell(n_ell), inv_ell(d);
     for (int q = 0; q < n_ell; ++q) ell[q] = std::exp(theta[q]);
     for (int k = 0; k < d; ++k) inv_ell[k] = 1.0 / ell[n_ell == 1 ? 0 : k];
@@ -245,7 +276,7 @@ hs_status hs_gp_nlml_grad(hs_ctx ctx, const double* X, const double* y, int d, c
 
     // workspace: L, Abar (packed), adjoint work, alpha, Xs, inv_ell, partials, results
     const size_t adj = adjoint_work_bytes(nb, bsz);
-    const size_t bytes = 2 * packed * sizeof(double) + adj + (size_t)n * sizeof(double) +
+    const size_t bytes = 2 * packed * sizeof(double) + adj + (size_t)2 * n * sizeof(double) +
                          (size_t)N * d * sizeof(double) + 64 * sizeof(double) +
                          (size_t)parts * (dmax + 2) * sizeof(double) + 256 * sizeof(double);
     if ((st = ensure_gp(ctx, bytes)) != HS_OK) return st;  // kept by the context between calls
@@ -254,7 +285,8 @@ hs_status hs_gp_nlml_grad(hs_ctx ctx, const double* X, const double* y, int d, c
     AdjointWork w;
     adjoint_bind(Abar + packed, nb, bsz, &w);
     double* alpha = reinterpret_cast<double*>(reinterpret_cast<char*>(Abar + packed) + adj);
-    double* Xs = alpha + n;
+    double* yb = alpha + n;  // y zero-padded (right-hand side of the mixed solve)
+    double* Xs = yb + n;
     double* inv_ell_d = Xs + (size_t)N * d;
     double* part = inv_ell_d + 64;
     double* res = part + (size_t)parts * (dmax + 2);
@@ -269,24 +301,62 @@ hs_status hs_gp_nlml_grad(hs_ctx ctx, const double* X, const double* y, int d, c
     } eg{ev};
     for (auto& e : ev) HS_CUDA(cudaEventCreate(&e));
     HS_CUDA(cudaEventRecord(ev[0], s));
-    // K(theta) and its FP64 factor
+    // K(theta)
     st = launch_rbf_assemble(ctx, L, X, d, ell.data(), n_ell, sf2, sn2, s);
     if (st != HS_OK) return st;
-    ctx->launches += 1;
-    set_i64_dev(ctx->d_info, INT64_MAX, s);
-    if ((st = factor_driver(ctx, L)) != HS_OK) return st;
-    HS_CUDA(cudaEventRecord(ev[1], s));
-    int64_t info = -1;
-    if ((st = hs_ctx_take_info(ctx, &info)) != HS_OK) return st;
-    if (info >= 0) {
-        set_error("hs_gp_nlml_grad: K(theta) is not positive definite (row " + std::to_string(info) + ")");
-        return HS_ERR_NOT_SPD;
+    if (precision == 0) {
+        // its FP64 factor, alpha = K^-1 y
+        ctx->launches += 1;
+        set_i64_dev(ctx->d_info, INT64_MAX, s);
+        if ((st = factor_driver(ctx, L)) != HS_OK) return st;
+        HS_CUDA(cudaEventRecord(ev[1], s));
+        int64_t info = -1;
+        if ((st = hs_ctx_take_info(ctx, &info)) != HS_OK) return st;
+        if (info >= 0) {
+            set_error("hs_gp_nlml_grad: K(theta) is not positive definite (row " + std::to_string(info) + ")");
+            return HS_ERR_NOT_SPD;
+        }
+        ctx->launches += 1;
+        copy_pad_kernel<<<64, 256, 0, s>>>(y, alpha, N, n);
+        HS_CHECK_LAUNCH("copy y");
+        if ((st = solve_driver(ctx, L, alpha)) != HS_OK) return st;
+    } else {
+        // the mixed-precision factor, alpha = K^-1 y refined in FP64 against K to the
+        // backward error tol; then L (FP64, packed) <- the mixed factor: off-diagonal
+        // blocks widened from FP32, diagonal blocks L_kk = ((L_kk^-T)^T)^-1 from the
+        // FP64 inverses the factor keeps (K is no longer needed)
+        ctx->launches += 1;
+        copy_pad_kernel<<<64, 256, 0, s>>>(y, yb, N, n);
+        HS_CHECK_LAUNCH("copy y");
+        hs_mixed_report mr{};
+        st = mixed_solve_impl(ctx, L, yb, alpha, precision, tol, 30, &mr);
+        if (mreport) *mreport = mr;
+        if (st != HS_OK) return st;
+        if (mr.shift != 0.0) {
+            set_error("hs_gp_nlml_grad: the mixed-precision factor of K(theta) needed a diagonal shift; its adjoint "
+                      "would be that of K + shift I");
+            return HS_ERR_NOT_SPD;
+        }
+        MixedWork mw;
+        if ((st = mixed_bind(ctx, ctx->mixed, &mw)) != HS_OK) return st;
+        ctx->launches += 1;
+        offdiag_f32_to_f64_kernel<<<4 * ctx->num_sms, 256, 0, s>>>(mw.A32, L, nb, bsz);
+        HS_CHECK_LAUNCH("widen factor");
+        const dim3 tg(bsz / 32, bsz / 32), tb(32, 8);
+        for (int k = 0; k < nb; ++k) {
+            double* Dk = L + block_id(k, k, nb) * bb;
+            ctx->launches += 2;
+            transpose_kernel<<<tg, tb, 0, s>>>(mw.Yinv + (size_t)k * bb, w.W1, bsz);  // W1 = L_kk^-1
+            HS_CHECK_LAUNCH("transpose");
+            if ((st = launch_identity(ctx, w.W2, s)) != HS_OK) return st;
+            if ((st = launch_trsm_on(ctx, w.W1, bsz, w.W2, 1, s)) != HS_OK) return st;  // W2 = L_kk^T
+            transpose_kernel<<<tg, tb, 0, s>>>(w.W2, Dk, bsz);
+            HS_CHECK_LAUNCH("transpose");
+        }
+        HS_CUDA(cudaEventRecord(ev[1], s));
     }
-    // alpha = K^-1 y, the two NLML terms
-    ctx->launches += 2;
-    copy_pad_kernel<<<64, 256, 0, s>>>(y, alpha, N, n);
-    HS_CHECK_LAUNCH("copy y");
-    if ((st = solve_driver(ctx, L, alpha)) != HS_OK) return st;
+    // the two NLML terms
+    ctx->launches += 1;
     nlml_terms_kernel<<<1, 1024, 0, s>>>(y, alpha, L, bsz, nb, N, res);
     HS_CHECK_LAUNCH("nlml terms");
     // reverse sweep of sum_i log L_ii, then the gradient contraction
@@ -322,6 +392,26 @@ hs_status hs_gp_nlml_grad(hs_ctx ctx, const double* X, const double* y, int d, c
         report->logdet = 2.0 * h[1];
     }
     return HS_OK;
+}
+
+hs_status hs_gp_nlml_grad(hs_ctx ctx, const double* X, const double* y, int d, const double* theta, int n_ell,
+                          double* nlml, double* grad, hs_gp_report* report) {
+    return gp_nlml_grad_impl(ctx, X, y, d, theta, n_ell, 0, 0.0, nlml, grad, report, nullptr);
+}
+
+hs_status hs_gp_nlml_grad_mixed(hs_ctx ctx, const double* X, const double* y, int d, const double* theta, int n_ell,
+                                int precision, double tol, double* nlml, double* grad, hs_gp_report* report,
+                                hs_mixed_report* mixed_report) {
+    if (precision != HS_PRECISION_TF32X3 && precision != HS_PRECISION_BF16X3 && precision != HS_PRECISION_F16X3) {
+        set_error("hs_gp_nlml_grad_mixed: precision must be HS_PRECISION_TF32X3, HS_PRECISION_BF16X3 or "
+                  "HS_PRECISION_F16X3");
+        return HS_ERR_UNSUPPORTED;
+    }
+    if (!(tol > 0.0)) {
+        set_error("hs_gp_nlml_grad_mixed: tol must be > 0");
+        return HS_ERR_INVALID_ARG;
+    }
+    return gp_nlml_grad_impl(ctx, X, y, d, theta, n_ell, precision, tol, nlml, grad, report, mixed_report);
 }
 
 }  // extern "C"

@@ -347,6 +347,20 @@ typedef struct hs_gp_report {
 hs_status hs_gp_nlml_grad(hs_ctx ctx, const double* X, const double* y, int d, const double* theta, int n_ell,
                           double* nlml, double* grad, hs_gp_report* report);
 
+/* The same NLML and gradient through the mixed-precision factor (no reference
+ * counterpart): the factor of hs_mixed_solve with `precision` (HS_PRECISION_*),
+ * alpha = K^-1 y refined in FP64 to the backward error `tol`, log|K| from the
+ * factor's FP64 diagonal blocks, and the FP64 reverse sweep run on the mixed
+ * factor widened to FP64.  alpha (hence the data-fit term) has FP64 accuracy;
+ * log|K| and the trace term 1/2 tr(K^-1 dK/dtheta) carry the error of the
+ * low-precision factor (K~ = L~ L~^T = K + E gives log|K~| - log|K| =
+ * tr(K^-1 E) - 1/2 ||K^-1/2 E K^-1/2||_F^2 + ...).  The workspace holds K, the
+ * mixed factor and the adjoint: about 2.5x the packed K.  HS_ERR_NOT_SPD when the
+ * factor needed a diagonal shift.  mixed_report (nullable) gets the solve's report. */
+hs_status hs_gp_nlml_grad_mixed(hs_ctx ctx, const double* X, const double* y, int d, const double* theta, int n_ell,
+                                int precision, double tol, double* nlml, double* grad, hs_gp_report* report,
+                                hs_mixed_report* mixed_report);
+
 #ifdef __cplusplus
 }
 #endif

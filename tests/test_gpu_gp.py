@@ -149,3 +149,34 @@ def test_fit_hyperparameters_decreases_nlml(hs, ctx):
     nlml0 = g.nlml_value(X, y, theta0, d)
     assert out["nlml"] < nlml0 - 1.0
     assert abs(out["nlml"] - g.nlml_value(X, y, out["theta"], d)) <= 1e-9 * abs(out["nlml"])
+
+
+@pytest.mark.parametrize("prec", ["f16x3", "tf32x3"])
+@pytest.mark.parametrize("N,bsz", [(2048, 256), (1000, 128)])
+def test_mixed_nlml_grad_against_dense(hs, ctx, N, bsz, prec):
+    """The NLML and gradient through the mixed-precision factor: the data-fit term
+    1/2 y^T K^-1 y has FP64 accuracy (alpha is refined against the FP64 K); log|K|
+    and the gradient carry the low-precision factor's error, bounded here at the
+    sizes tested and reported by bench.py at N = 65536."""
+    d = 8
+    X, y, theta = _c4_problem(N, d, seed=40 + N)
+    ctx.set_problem(N, bsz)
+    nlml, grad, rep = hs.gp_nlml_grad(ctx, X, y, theta, precision=prec)
+    nlml_ref, grad_ref = g.nlml_dense(X, y, theta, d)
+    nlml64, grad64, rep64 = hs.gp_nlml_grad(ctx, X, y, theta)
+    ell = np.exp(theta[:d])
+    K, _, _ = g.rbf_dense(X, ell, 1.0, np.exp(theta[-1]))
+    fit_ref = 0.5 * y @ np.linalg.solve(K, y)
+    logdet_ref = np.linalg.slogdet(K)[1]
+    rel_fit = abs(rep["data_fit"] - fit_ref) / abs(fit_ref)
+    abs_logdet = abs(rep["logdet"] - logdet_ref)
+    rel_grad = np.max(np.abs(grad - grad_ref) / np.abs(grad_ref))
+    rel_grad_norm = np.linalg.norm(grad - grad_ref) / np.linalg.norm(grad_ref)
+    print(f"{prec} N={N}: data fit rel {rel_fit:.2e}, log|K| abs {abs_logdet:.2e} (FP64 form "
+          f"{abs(rep64['logdet'] - logdet_ref):.2e}), nlml abs {abs(nlml - nlml_ref):.2e}, grad rel max "
+          f"{rel_grad:.2e} normwise {rel_grad_norm:.2e} (FP64 form "
+          f"{np.max(np.abs(grad64 - grad_ref) / np.abs(grad_ref)):.2e}); {rep['mixed']}")
+    assert rep["mixed"]["backward_error"] <= 1e-14
+    assert rel_fit <= 1e-10
+    assert abs_logdet <= 1e-3 * N * 1e-3
+    assert rel_grad_norm <= 1e-3
