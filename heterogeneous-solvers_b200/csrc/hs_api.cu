@@ -38,6 +38,7 @@ hs_status ensure_scratch(hs_ctx ctx, size_t bytes) {
     if (want < 1024 * 1024) want = 1024 * 1024;
     HS_CUDA(cudaStreamSynchronize(ctx->stream));
     if (ctx->side) HS_CUDA(cudaStreamSynchronize(ctx->side));
+    if (ctx->side_hi) HS_CUDA(cudaStreamSynchronize(ctx->side_hi));
     if (ctx->scratch) HS_CUDA(cudaFree(ctx->scratch));
     ctx->scratch = nullptr;
     ctx->scratch_bytes = 0;
@@ -213,6 +214,11 @@ hs_status hs_ctx_create(int device, void* stream, hs_ctx* out) {
     ctx->num_sms = prop.multiProcessorCount;
     ctx->stream = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
     HS_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    {
+        int least = 0, greatest = 0;
+        HS_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        HS_CUDA(cudaStreamCreateWithPriority(&ctx->side_hi, cudaStreamNonBlocking, greatest));
+    }
     HS_CUDA(cudaEventCreateWithFlags(&ctx->ev_a, cudaEventDisableTiming));
     HS_CUDA(cudaEventCreateWithFlags(&ctx->ev_b, cudaEventDisableTiming));
     HS_CUDA(cudaMalloc(&ctx->d_info, sizeof(long long)));
@@ -231,6 +237,10 @@ hs_status hs_ctx_destroy(hs_ctx ctx) {
     if (ctx->side) {
         cudaStreamSynchronize(ctx->side);
         cudaStreamDestroy(ctx->side);
+    }
+    if (ctx->side_hi) {
+        cudaStreamSynchronize(ctx->side_hi);
+        cudaStreamDestroy(ctx->side_hi);
     }
     if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
     if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
@@ -258,6 +268,7 @@ hs_status hs_ctx_release_buffers(hs_ctx ctx) {
     HS_CUDA(cudaSetDevice(ctx->device));
     HS_CUDA(cudaStreamSynchronize(ctx->stream));
     if (ctx->side) HS_CUDA(cudaStreamSynchronize(ctx->side));
+    if (ctx->side_hi) HS_CUDA(cudaStreamSynchronize(ctx->side_hi));
     if (ctx->scratch) HS_CUDA(cudaFree(ctx->scratch));
     if (ctx->work) HS_CUDA(cudaFree(ctx->work));
     if (ctx->mixed) HS_CUDA(cudaFree(ctx->mixed));

@@ -42,6 +42,9 @@ struct hs_ctx_s {
     double* h_pinned = nullptr;
     // second stream + events used by the drivers for lookahead
     cudaStream_t side = nullptr;
+    // high-priority stream of the FP64 factor's lookahead (its diagonal-block work
+    // takes SMs ahead of the trailing update's CTAs)
+    cudaStream_t side_hi = nullptr;
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
 
     // > 0: matvec, dot and vector updates follow the reference CPU path's exact
@@ -162,6 +165,16 @@ hs_status launch_trsm(hs_ctx ctx, double* A, int blockID, int blockRow, int bloc
 // in one launch (either count may be zero)
 hs_status launch_update(hs_ctx ctx, double* A, int blockID, int blockRow, int syrkStart, int syrkCount,
                         int gemmStart, int gemmCount, cudaStream_t s);
+// the same update restricted to the trailing block columns [colStart, colEnd)
+// (SYRK on their diagonal blocks, GEMM below them)
+hs_status launch_update_cols(hs_ctx ctx, double* A, int blockID, int blockRow, int colStart, int colEnd,
+                             cudaStream_t s);
+// X = L^-1 (row major) of one lower-triangular bsz x bsz block; Y is a block of scratch
+hs_status launch_diag_inverse(hs_ctx ctx, const double* Lkk, double* Y, double* X, cudaStream_t s);
+// B <- B X^T in place for blockCount consecutive blocks from firstBlock (bsz 128 or 256):
+// the panel TRSM on the FP64 tensor pipe, given X = L_kk^-1
+hs_status launch_trsm_dmma(hs_ctx ctx, double* A, int64_t firstBlock, int blockCount, const double* X,
+                           cudaStream_t s);
 hs_status launch_symv(hs_ctx ctx, const double* A, const double* b, double* result, int bi0, int bj0, int nbi,
                       int nbj, int reset, double* dot_with /*nullable: also dot(result, dot_with) */,
                       double* dot_out, cudaStream_t s);

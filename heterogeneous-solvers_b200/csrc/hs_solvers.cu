@@ -85,22 +85,59 @@ int grid_for(int64_t n, int num_sms) {
 
 hs_status factor_driver(hs_ctx ctx, double* A) {
     // Cholesky.cpp:446-471 with the GPU owning every block row: per block
-    // column k, POTRF(k), TRSM on rows k+1.., then one launch for the SYRK on
-    // diagonal blocks k+1.. and the GEMM on rows k+2...
-    const int nb = ctx->nb;
+    // column k, POTRF(k), TRSM on rows k+1.., then the SYRK on diagonal blocks
+    // k+1.. and the GEMM on rows k+2...
+    const int nb = ctx->nb, bsz = ctx->bsz;
     const int64_t T = total_blocks(nb);
     cudaStream_t s = ctx->stream;
-    for (int k = 0; k < nb; ++k) {
-        const int right = nb - k;
-        const int blockID = (int)(T - (int64_t)right * (right + 1) / 2);
-        hs_status st = launch_potrf(ctx, A, blockID, k, s);
-        if (st != HS_OK) return st;
+    auto diag_id = [&](int k) { return (int)(T - (int64_t)(nb - k) * (nb - k + 1) / 2); };
+    if ((bsz != 128 && bsz != 256) || !ctx->side_hi) {
+        for (int k = 0; k < nb; ++k) {
+            const int blockID = diag_id(k);
+            hs_status st = launch_potrf(ctx, A, blockID, k, s);
+            if (st != HS_OK) return st;
+            const int cnt = nb - (k + 1);
+            if (cnt > 0) {
+                st = launch_trsm(ctx, A, blockID, k, k + 1, cnt, s);
+                if (st != HS_OK) return st;
+                st = launch_update(ctx, A, blockID, k, k + 1, cnt, k + 2, cnt - 1, s);
+                if (st != HS_OK) return st;
+            }
+        }
+        return HS_OK;
+    }
+    // Tensor-core form with lookahead.  The panel TRSM is a product with
+    // X = L_kk^-1.  Per column k the trailing update runs in two launches: column
+    // k+1 first; then, while the rest of the update runs, POTRF(k+1), X and the
+    // TRSM of column k+1 run on the high-priority side stream.  Every block sees
+    // the same operations in the same order as without lookahead.
+    const size_t bb = (size_t)bsz * bsz;
+    hs_status st = ensure_scratch(ctx, kSmallScratch + 2 * bb * sizeof(double));
+    if (st != HS_OK) return st;
+    double* Y = reinterpret_cast<double*>(static_cast<char*>(ctx->scratch) + kSmallScratch);
+    double* X = Y + bb;
+    auto diag = [&](int k, cudaStream_t q) -> hs_status {
+        const int blockID = diag_id(k);
+        hs_status s2 = launch_potrf(ctx, A, blockID, k, q);
+        if (s2 != HS_OK) return s2;
         const int cnt = nb - (k + 1);
-        if (cnt > 0) {
-            st = launch_trsm(ctx, A, blockID, k, k + 1, cnt, s);
-            if (st != HS_OK) return st;
-            st = launch_update(ctx, A, blockID, k, k + 1, cnt, k + 2, cnt - 1, s);
-            if (st != HS_OK) return st;
+        if (cnt <= 0) return HS_OK;
+        if ((s2 = launch_diag_inverse(ctx, A + (size_t)blockID * bb, Y, X, q)) != HS_OK) return s2;
+        return launch_trsm_dmma(ctx, A, (int64_t)blockID + 1, cnt, X, q);
+    };
+    if ((st = diag(0, s)) != HS_OK) return st;
+    for (int k = 0; k + 1 < nb; ++k) {
+        const int blockID = diag_id(k);
+        if ((st = launch_update_cols(ctx, A, blockID, k, k + 1, k + 2, s)) != HS_OK) return st;
+        if (k + 2 < nb) {
+            HS_CUDA(cudaEventRecord(ctx->ev_a, s));
+            HS_CUDA(cudaStreamWaitEvent(ctx->side_hi, ctx->ev_a, 0));
+            if ((st = diag(k + 1, ctx->side_hi)) != HS_OK) return st;
+            HS_CUDA(cudaEventRecord(ctx->ev_b, ctx->side_hi));
+            if ((st = launch_update_cols(ctx, A, blockID, k, k + 2, nb, s)) != HS_OK) return st;
+            HS_CUDA(cudaStreamWaitEvent(s, ctx->ev_b, 0));
+        } else if ((st = diag(k + 1, s)) != HS_OK) {
+            return st;
         }
     }
     return HS_OK;

@@ -266,47 +266,215 @@ __device__ __forceinline__ void dmma_tile(double* __restrict__ C, int64_t ldc, c
         }
 }
 
-// One launch for the whole trailing update of block column blockRow: GEMM
-// pairs (r, c), r in [gemmStart, gemmStart+gemmCount), blockRow < c < r,
-// followed by SYRK diagonal blocks j in [syrkStart, syrkStart+syrkCount).
-// CTA = one 128x128 tile of one output block.
+// ------------------------------------------------------ templated DMMA tiles
+// A CTA computes a TM x TN output tile with (TM/WM) x (TN/WN) warps of WM x WN
+// (m8n8k4 sub-tiles), K streamed in 16-wide slabs through an ST-stage cp.async
+// ring with rows padded to SPAD doubles (row stride 40 banks: the eight rows a
+// fragment load touches fall in distinct bank groups).
+template <int TM, int TN, int WM, int WN, int ST>
+struct DTile {
+    static constexpr int kWarpsN = TN / WN;
+    static constexpr int kThreads = 32 * (TM / WM) * (TN / WN);
+    static constexpr int kMi = WM / 8, kNi = WN / 8;
+    static constexpr int kSmem = ST * (TM + TN) * SPAD * (int)sizeof(double);
+    static constexpr int kChunks = (TM + TN) * (BK / 2);  // 16-byte copies a stage
+    static_assert(kChunks % kThreads == 0, "copies must split evenly over the threads");
+    static_assert((TM * (BK / 2)) % 32 == 0, "A and B copies must not share a warp");
+};
+
+// PRODUCT = false: C (TM x TN, ldc) <- C - A (TM x K, lda) B (TN x K, ldb)^T,
+//   accumulated from -C in k order; with `lower`, entry (r, c) is written only
+//   if c + shift <= r (a tile that crosses the diagonal of a diagonal block).
+// PRODUCT = true: C <- A B^T with B lower triangular by rows (B[c][k] = 0 for
+//   k > c): a warp skips the K slabs past its last column.  C may be A itself:
+//   every load of A completes before the first store.
+template <int TM, int TN, int WM, int WN, int ST, bool PRODUCT>
+__device__ __forceinline__ void dmma_tile_t(double* C, int64_t ldc, const double* Ag, int64_t lda,
+                                            const double* __restrict__ Bg, int64_t ldb, int K, bool lower, int shift,
+                                            double* smem) {
+    using D = DTile<TM, TN, WM, WN, ST>;
+    double* As = smem;                   // [ST][TM][SPAD]
+    double* Bs = smem + ST * TM * SPAD;  // [ST][TN][SPAD]
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int wm = warp / D::kWarpsN, wn = warp % D::kWarpsN;
+    const int g = lane >> 2, t = lane & 3;
+
+    double acc[D::kMi][D::kNi][2];
+#pragma unroll
+    for (int mi = 0; mi < D::kMi; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < D::kNi; ++ni) {
+            if (PRODUCT) {
+                acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+            } else {
+                const int r = wm * WM + mi * 8 + g;
+                const int c = wn * WN + ni * 8 + 2 * t;
+                const double2 v = *reinterpret_cast<const double2*>(C + (size_t)r * ldc + c);
+                acc[mi][ni][0] = -v.x;
+                acc[mi][ni][1] = -v.y;
+            }
+        }
+
+    const int ktiles = K / BK;
+    // PRODUCT: rows wn*WN .. wn*WN+WN-1 of B vanish past column wn*WN+WN-1
+    const int kt_warp = PRODUCT ? min(ktiles, (wn * WN + WN + BK - 1) / BK) : ktiles;
+    auto load_stage = [&](int stage, int kt) {
+        const int kc = kt * BK;
+#pragma unroll
+        for (int q = 0; q < D::kChunks / D::kThreads; ++q) {
+            const int e = tid + D::kThreads * q;
+            const int row = e >> 3, ch = e & 7;
+            if (row < TM)
+                cp_async16(As + (stage * TM + row) * SPAD + ch * 2, Ag + (size_t)row * lda + kc + ch * 2);
+            else
+                cp_async16(Bs + (stage * TN + row - TM) * SPAD + ch * 2, Bg + (size_t)(row - TM) * ldb + kc + ch * 2);
+        }
+    };
+#pragma unroll
+    for (int s = 0; s < ST - 1; ++s) {
+        if (s < ktiles) load_stage(s, s);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < ktiles; ++kt) {
+        cp_async_wait<ST - 2>();
+        __syncthreads();
+        {
+            const int nk = kt + ST - 1;
+            if (nk < ktiles) load_stage(nk % ST, nk);
+            cp_async_commit();
+        }
+        if (kt < kt_warp) {
+            const double* as = As + (kt % ST) * TM * SPAD + (wm * WM + g) * SPAD + t;
+            const double* bs = Bs + (kt % ST) * TN * SPAD + (wn * WN + g) * SPAD + t;
+#pragma unroll
+            for (int kk = 0; kk < BK / 4; ++kk) {
+                double a[D::kMi], b[D::kNi];
+#pragma unroll
+                for (int mi = 0; mi < D::kMi; ++mi) a[mi] = as[mi * 8 * SPAD + kk * 4];
+#pragma unroll
+                for (int ni = 0; ni < D::kNi; ++ni) b[ni] = bs[ni * 8 * SPAD + kk * 4];
+#pragma unroll
+                for (int mi = 0; mi < D::kMi; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < D::kNi; ++ni) dmma884(acc[mi][ni], a[mi], b[ni]);
+            }
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();  // every load of A has landed before C (possibly A) is written
+#pragma unroll
+    for (int mi = 0; mi < D::kMi; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < D::kNi; ++ni) {
+            const int r = wm * WM + mi * 8 + g;
+            const int c = wn * WN + ni * 8 + 2 * t;
+            const double v0 = PRODUCT ? acc[mi][ni][0] : -acc[mi][ni][0];
+            const double v1 = PRODUCT ? acc[mi][ni][1] : -acc[mi][ni][1];
+            double* p = C + (size_t)r * ldc + c;
+            if (!lower || c + 1 + shift <= r) {
+                *reinterpret_cast<double2*>(p) = make_double2(v0, v1);
+            } else if (c + shift <= r) {
+                p[0] = v0;
+            }
+        }
+}
+
+// Trailing update, two CTAs an SM: 128 x 64 tiles, 8 warps of 32 x 32, 3 stages.
+// Each CTA's C preload and store overlap the other CTA's tensor work.
+constexpr int kUTM = 128, kUTN = 64, kUWM = 32, kUWN = 32, kUST = 3;
+using UTile = DTile<kUTM, kUTN, kUWM, kUWN, kUST>;
+
+// Work list of a trailing update.  Column mode (the factor driver): the pairs
+// (r, c) of the columns c in [colStart, colEnd), c <= r < nb, column by column.
+// Row mode (the operator entry points, MatrixMatrixOperations.cpp:146-906): GEMM
+// pairs (r, c), r in [gemmStart, gemmStart+gemmCount), blockRow < c < r, then
+// SYRK diagonal blocks j in [syrkStart, syrkStart+syrkCount).
 struct UpdateArgs {
     double* A;
-    int64_t blockID;
+    int64_t blockID;  // diagonal block of column blockRow (the panel's column)
     int blockRow, nb, bsz;
-    int64_t gemmPairs;   // number of GEMM pairs
-    int64_t pairBase;    // triangular offset of gemmStart
+    int rowMode;
+    int colStart, colEnd;            // column mode
+    int64_t gemmPairs, pairBase;     // row mode
     int syrkStart;
-    int tilesPerSide;
-    int64_t totalPairs;  // gemmPairs + SYRK blocks
+    int tilesM, tilesN;
+    int64_t totalPairs;
 };
 
 __device__ __forceinline__ void decode_pair(const UpdateArgs& a, int64_t pair, int* r, int* c) {
-    if (pair < a.gemmPairs) {
-        const int64_t tt = pair + a.pairBase;
-        const int u = tri_root(tt);
-        *r = a.blockRow + 1 + (u + 1);
-        *c = a.blockRow + 1 + (int)(tt - (int64_t)u * (u + 1) / 2);
-    } else {
-        *r = *c = a.syrkStart + (int)(pair - a.gemmPairs);
+    if (a.rowMode) {
+        if (pair < a.gemmPairs) {
+            const int64_t tt = pair + a.pairBase;
+            const int u = tri_root(tt);
+            *r = a.blockRow + 1 + (u + 1);
+            *c = a.blockRow + 1 + (int)(tt - (int64_t)u * (u + 1) / 2);
+        } else {
+            *r = *c = a.syrkStart + (int)(pair - a.gemmPairs);
+        }
+        return;
     }
+    // column c holds nb - c pairs: the largest c with offset(c) <= pair
+    auto offset = [&](int cc) -> int64_t {
+        return (int64_t)(cc - a.colStart) * a.nb - ((int64_t)cc * (cc - 1) - (int64_t)a.colStart * (a.colStart - 1)) / 2;
+    };
+    int lo = a.colStart, hi = a.colEnd - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (offset(mid) <= pair) lo = mid; else hi = mid - 1;
+    }
+    *c = lo;
+    *r = lo + (int)(pair - offset(lo));
 }
 
-__global__ void __launch_bounds__(256, 1) update_dmma_kernel(UpdateArgs a) {
+__global__ void __launch_bounds__(UTile::kThreads, 2) update_dmma_kernel(UpdateArgs a) {
     extern __shared__ __align__(16) double smem[];
-    const int tps = a.tilesPerSide;
-    const int64_t idx = blockIdx.x;
-    const int tile = (int)(idx % (tps * tps));
-    const int64_t pair = idx / (tps * tps);
+    const int tpb = a.tilesM * a.tilesN;
+    const int64_t pair = blockIdx.x / tpb;
+    const int tile = (int)(blockIdx.x % tpb);
     int r, c;
     decode_pair(a, pair, &r, &c);
-    const int ti = tile / tps, tj = tile % tps;
-    if (r == c && tj > ti) return;
+    const int ti = tile / a.tilesN, tj = tile % a.tilesN;
+    const int shift = tj * kUTN - ti * kUTM;  // tile column offset minus row offset inside the block
+    const bool diag = r == c;
+    if (diag && shift > kUTM - 1) return;      // entirely above the diagonal
+    const bool lower = diag && shift + kUTN - 1 > 0;
     const size_t bb = (size_t)a.bsz * a.bsz;
-    double* C = a.A + (size_t)block_id(r, c, a.nb) * bb + (size_t)ti * BM * a.bsz + (size_t)tj * BN;
-    const double* Ag = a.A + (size_t)(a.blockID + (r - a.blockRow)) * bb + (size_t)ti * BM * a.bsz;
-    const double* Bg = a.A + (size_t)(a.blockID + (c - a.blockRow)) * bb + (size_t)tj * BN * a.bsz;
-    dmma_tile(C, a.bsz, Ag, a.bsz, Bg, a.bsz, a.bsz, r == c && ti == tj, smem);
+    double* C = a.A + (size_t)block_id(r, c, a.nb) * bb + (size_t)ti * kUTM * a.bsz + (size_t)tj * kUTN;
+    const double* Ag = a.A + (size_t)(a.blockID + (r - a.blockRow)) * bb + (size_t)ti * kUTM * a.bsz;
+    const double* Bg = a.A + (size_t)(a.blockID + (c - a.blockRow)) * bb + (size_t)tj * kUTN * a.bsz;
+    dmma_tile_t<kUTM, kUTN, kUWM, kUWN, kUST, false>(C, a.bsz, Ag, a.bsz, Bg, a.bsz, a.bsz, lower, shift, smem);
+}
+
+// Panel TRSM as a tensor-core product: B <- B X^T with X = L_kk^-1 (row major,
+// lower triangular), in place; one CTA per 64 rows of a panel block.
+template <int BSZ>
+struct TrsmTile {
+    using T = DTile<64, BSZ, 32, BSZ / 4, 3>;
+};
+
+template <int BSZ>
+__global__ void __launch_bounds__(256, 1) trsm_dmma_kernel(double* A, int64_t firstBlock, const double* __restrict__ X) {
+    extern __shared__ __align__(16) double smem[];
+    constexpr int kSlabs = BSZ / 64;
+    const int64_t item = blockIdx.x / kSlabs;
+    const int slab = blockIdx.x % kSlabs;
+    double* B = A + (size_t)(firstBlock + item) * BSZ * BSZ + (size_t)slab * 64 * BSZ;
+    dmma_tile_t<64, BSZ, 32, BSZ / 4, 3, true>(B, BSZ, B, BSZ, X, BSZ, BSZ, false, 0, smem);
+}
+
+__global__ void identity_block_kernel(double* __restrict__ Y, int n) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * n; e += gridDim.x * blockDim.x)
+        Y[e] = (e / n == e % n) ? 1.0 : 0.0;
+}
+
+// X = Y^T for one n x n block (32 x 32 tiles through shared memory)
+__global__ void transpose_block_kernel(const double* __restrict__ Y, double* __restrict__ X, int n) {
+    __shared__ double tile[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) tile[i][threadIdx.x] = Y[(size_t)(by + i) * n + bx + threadIdx.x];
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) X[(size_t)(bx + i) * n + by + threadIdx.x] = tile[threadIdx.x][i];
 }
 
 // single-tile form used inside the blocked POTRF of a 256 block
@@ -348,7 +516,11 @@ hs_status set_attrs() {
     int dev = 0;
     HS_CUDA(cudaGetDevice(&dev));
     if (dev >= 0 && dev < 64 && attrs_done[dev]) return HS_OK;
-    HS_CUDA(cudaFuncSetAttribute(update_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
+    HS_CUDA(cudaFuncSetAttribute(update_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, UTile::kSmem));
+    HS_CUDA(cudaFuncSetAttribute(trsm_dmma_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TrsmTile<128>::T::kSmem));
+    HS_CUDA(cudaFuncSetAttribute(trsm_dmma_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TrsmTile<256>::T::kSmem));
     HS_CUDA(cudaFuncSetAttribute(tile_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
     HS_CUDA(cudaFuncSetAttribute(trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem(256)));
     HS_CUDA(cudaFuncSetAttribute(potrf_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -425,6 +597,42 @@ hs_status launch_potrf(hs_ctx ctx, double* A, int blockID, int blockRow, cudaStr
     return st;
 }
 
+hs_status launch_diag_inverse(hs_ctx ctx, const double* Lkk, double* Y, double* X, cudaStream_t s) {
+    // Y = I L^-T by the substitution kernel, X = Y^T = L^-1 (row major, lower triangular:
+    // every entry above the diagonal of Y comes out exactly zero)
+    const int n = ctx->bsz;
+    ctx->launches += 1;
+    identity_block_kernel<<<64, 256, 0, s>>>(Y, n);
+    HS_CHECK_LAUNCH("identity");
+    hs_status st = launch_trsm_on(ctx, Lkk, n, Y, 1, s);
+    if (st != HS_OK) return st;
+    ctx->launches += 1;
+    transpose_block_kernel<<<dim3(n / 32, n / 32), dim3(32, 8), 0, s>>>(Y, X, n);
+    HS_CHECK_LAUNCH("transpose");
+    return HS_OK;
+}
+
+hs_status launch_trsm_dmma(hs_ctx ctx, double* A, int64_t firstBlock, int blockCount, const double* X,
+                           cudaStream_t s) {
+    if (blockCount <= 0) return HS_OK;
+    hs_status st = set_attrs();
+    if (st != HS_OK) return st;
+    const int bsz = ctx->bsz;
+    HS_REQUIRE(bsz == 128 || bsz == 256, "the tensor-core TRSM needs matrixBlockSize 128 or 256");
+    const double n = bsz;
+    prof_begin(ctx, s, HS_KERNEL_TRSM);
+    ctx->launches += 1;
+    const unsigned grid = (unsigned)((int64_t)blockCount * (bsz / 64));
+    if (bsz == 256)
+        trsm_dmma_kernel<256><<<grid, 256, TrsmTile<256>::T::kSmem, s>>>(A, firstBlock, X);
+    else
+        trsm_dmma_kernel<128><<<grid, 256, TrsmTile<128>::T::kSmem, s>>>(A, firstBlock, X);
+    HS_CHECK_LAUNCH("trsm_dmma");
+    // algorithmic work: the triangular solve's n^3 flops a block
+    prof_end(ctx, s, HS_KERNEL_TRSM, blockCount * n * n * n, (2.0 * blockCount + 1.0) * n * n * 8.0);
+    return HS_OK;
+}
+
 hs_status launch_trsm(hs_ctx ctx, double* A, int blockID, int blockRow, int blockStart, int blockCount,
                       cudaStream_t s) {
     if (blockCount <= 0) return HS_OK;
@@ -433,6 +641,16 @@ hs_status launch_trsm(hs_ctx ctx, double* A, int blockID, int blockRow, int bloc
     const int bsz = ctx->bsz;
     HS_REQUIRE(bsz <= 256, "TRSM supports matrixBlockSize up to 256");
     const size_t bb = (size_t)bsz * bsz;
+    if (bsz == 128 || bsz == 256) {
+        // on the FP64 tensor pipe: X = L_kk^-1 once, then B <- B X^T block by block
+        st = ensure_scratch(ctx, kSmallScratch + 2 * bb * sizeof(double));
+        if (st != HS_OK) return st;
+        double* Y = reinterpret_cast<double*>(static_cast<char*>(ctx->scratch) + kSmallScratch);
+        double* X = Y + bb;
+        st = launch_diag_inverse(ctx, A + (size_t)blockID * bb, Y, X, s);
+        if (st != HS_OK) return st;
+        return launch_trsm_dmma(ctx, A, (int64_t)blockID + (blockStart - blockRow), blockCount, X, s);
+    }
     TrsmArgs ta{A + (size_t)blockID * bb, bsz, bsz, A, bsz, (int64_t)blockID + (blockStart - blockRow),
                 (bsz + kTrsmRows - 1) / kTrsmRows, bsz, (int64_t)bb};
     const double n = bsz;
@@ -449,6 +667,35 @@ hs_status launch_trsm_on(hs_ctx ctx, const double* L, int n, double* B, int item
     return launch_trsm_args(ctx, ta, items, s);
 }
 
+namespace {
+
+// launches the update of `a` (totalPairs set) with its algorithmic flops / bytes
+hs_status run_update(hs_ctx ctx, UpdateArgs& a, double flops, double bytes, cudaStream_t s) {
+    if (a.totalPairs <= 0) return HS_OK;
+    const bool dmma = ctx->bsz % kUTM == 0;
+    a.tilesM = dmma ? ctx->bsz / kUTM : 1;
+    a.tilesN = dmma ? ctx->bsz / kUTN : 1;
+    const int64_t grid = a.totalPairs * a.tilesM * a.tilesN;
+    HS_REQUIRE(grid < (1LL << 31), "trailing update too large for one launch");
+    prof_begin(ctx, s, HS_KERNEL_UPDATE);
+    ctx->launches += 1;
+    if (dmma) {
+        update_dmma_kernel<<<(unsigned)grid, UTile::kThreads, UTile::kSmem, s>>>(a);
+        HS_CHECK_LAUNCH("update_dmma");
+    } else {
+        const int64_t bb = (int64_t)ctx->bsz * ctx->bsz;
+        const int64_t total = a.totalPairs;
+        dim3 g((unsigned)((bb + 255) / 256), (unsigned)(total < 65535 ? total : 65535),
+               (unsigned)((total + 65534) / 65535));
+        update_scalar_kernel<<<g, 256, 0, s>>>(a);
+        HS_CHECK_LAUNCH("update_scalar");
+    }
+    prof_end(ctx, s, HS_KERNEL_UPDATE, flops, bytes);
+    return HS_OK;
+}
+
+}  // namespace
+
 hs_status launch_update(hs_ctx ctx, double* A, int blockID, int blockRow, int syrkStart, int syrkCount,
                         int gemmStart, int gemmCount, cudaStream_t s) {
     hs_status st = set_attrs();
@@ -459,6 +706,7 @@ hs_status launch_update(hs_ctx ctx, double* A, int blockID, int blockRow, int sy
     a.blockRow = blockRow;
     a.nb = ctx->nb;
     a.bsz = ctx->bsz;
+    a.rowMode = 1;
     int64_t pairs = 0;
     if (gemmCount > 0) {
         // rows r' = r - blockRow - 1 in [g0, g0 + gemmCount) own r' pairs each
@@ -469,36 +717,40 @@ hs_status launch_update(hs_ctx ctx, double* A, int blockID, int blockRow, int sy
     }
     a.gemmPairs = pairs;
     a.syrkStart = syrkStart;
-    const int64_t total = pairs + (syrkCount > 0 ? syrkCount : 0);
-    if (total <= 0) return HS_OK;
-    a.totalPairs = total;
+    const int64_t syrkN = syrkCount > 0 ? syrkCount : 0;
+    a.totalPairs = pairs + syrkN;
     // algorithmic work: 2 bsz^3 per GEMM pair, bsz^2 (bsz + 1) per SYRK block;
     // bytes: read + write of every output block plus the panel column once
     const double n = ctx->bsz;
-    const int64_t syrkN = syrkCount > 0 ? syrkCount : 0;
     const double flops = (double)pairs * 2.0 * n * n * n + (double)syrkN * n * n * (n + 1.0);
     const int64_t panel = (gemmCount > 0 ? gemmCount + 1 : 0) > syrkN ? (gemmCount + 1) : syrkN;
     const double bytes = ((double)pairs * 2.0 + (double)syrkN * 2.0 + (double)panel) * n * n * 8.0;
-    if (ctx->bsz % BM == 0) {
-        a.tilesPerSide = ctx->bsz / BM;
-        const int64_t grid = total * a.tilesPerSide * a.tilesPerSide;
-        HS_REQUIRE(grid < (1LL << 31), "trailing update too large for one launch");
-        prof_begin(ctx, s, HS_KERNEL_UPDATE);
-        ctx->launches += 1;
-        update_dmma_kernel<<<(unsigned)grid, 256, kTileSmem, s>>>(a);
-        HS_CHECK_LAUNCH("update_dmma");
-        prof_end(ctx, s, HS_KERNEL_UPDATE, flops, bytes);
-    } else {
-        const int64_t bb = (int64_t)ctx->bsz * ctx->bsz;
-        dim3 grid((unsigned)((bb + 255) / 256), (unsigned)(total < 65535 ? total : 65535),
-                  (unsigned)((total + 65534) / 65535));
-        prof_begin(ctx, s, HS_KERNEL_UPDATE);
-        ctx->launches += 1;
-        update_scalar_kernel<<<grid, 256, 0, s>>>(a);
-        HS_CHECK_LAUNCH("update_scalar");
-        prof_end(ctx, s, HS_KERNEL_UPDATE, flops, bytes);
-    }
-    return HS_OK;
+    return run_update(ctx, a, flops, bytes, s);
+}
+
+hs_status launch_update_cols(hs_ctx ctx, double* A, int blockID, int blockRow, int colStart, int colEnd,
+                             cudaStream_t s) {
+    hs_status st = set_attrs();
+    if (st != HS_OK) return st;
+    const int nb = ctx->nb;
+    HS_REQUIRE(blockRow < colStart && colStart <= colEnd && colEnd <= nb, "columns outside the trailing matrix");
+    UpdateArgs a{};
+    a.A = A;
+    a.blockID = blockID;
+    a.blockRow = blockRow;
+    a.nb = nb;
+    a.bsz = ctx->bsz;
+    a.rowMode = 0;
+    a.colStart = colStart;
+    a.colEnd = colEnd;
+    int64_t pairs = 0;
+    for (int c = colStart; c < colEnd; ++c) pairs += nb - c;
+    a.totalPairs = pairs;
+    const double n = ctx->bsz;
+    const int64_t syrkN = colEnd - colStart;
+    const double flops = (double)(pairs - syrkN) * 2.0 * n * n * n + (double)syrkN * n * n * (n + 1.0);
+    const double bytes = ((double)pairs * 2.0 + (double)(nb - colStart)) * n * n * 8.0;
+    return run_update(ctx, a, flops, bytes, s);
 }
 
 }  // namespace hs

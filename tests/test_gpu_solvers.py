@@ -46,7 +46,8 @@ def test_rbf_assembly_matches_oracle(hs, ctx, N, bsz, d, ell):
     assert np.max(np.abs(A - ref)) <= 1e-14  # FMA contraction and exp may differ from the host by a few ulp
 
 
-@pytest.mark.parametrize("N,bsz", [(1000, 128), (1024, 256), (700, 256), (600, 256), (130, 20), (47, 6)])
+@pytest.mark.parametrize("N,bsz", [(1000, 128), (1024, 256), (700, 256), (600, 256), (130, 20), (47, 6),
+                                   (2900, 128), (3000, 256)])
 def test_cholesky_factor_matches_oracle(hs, ctx, N, bsz):
     X, _ = _problem(N, 8)
     A = _assemble_gpu(hs, ctx, X, bsz, 0.5, 1.0, 1e-2)
@@ -66,6 +67,42 @@ def test_cholesky_factor_matches_oracle(hs, ctx, N, bsz):
     K = ol.packed_to_dense(ol.rbf_assemble(X, bsz, 0.5, 1.0, 1e-2), N, bsz)
     Ld = ol.packed_to_dense(L, N, bsz, lower_only=True)
     assert np.linalg.norm(Ld - np.linalg.cholesky(K)) / np.linalg.norm(Ld) <= 1e-12
+
+
+@pytest.mark.parametrize("N,bsz,k", [(1000, 128, 0), (1000, 128, 3), (1500, 256, 0), (1500, 256, 2), (700, 256, 1)])
+def test_panel_trsm_on_tensor_cores_matches_oracle(hs, ctx, N, bsz, k):
+    """hs_trsm_panel for matrixBlockSize 128 / 256 runs as a product with L_kk^-1 on
+    the FP64 tensor pipe: the panel of column k (after POTRF) against the
+    reference's substitution (MatrixMatrixOperations.cpp:109-144) on the oracle."""
+    X, _ = _problem(N, 8)
+    K = ol.rbf_assemble(X, bsz, 0.5, 1.0, 1e-2)
+    nb = -(-N // bsz)
+    # factor columns 0..k-1 on the oracle, POTRF column k: the state TRSM(k) sees
+    ref = K.copy()
+    lib = ol.lib()
+    T = nb * (nb + 1) // 2
+    for j in range(k + 1):
+        bid = T - (nb - j) * (nb - j + 1) // 2
+        lib.or_potrf_block(ol.ptr(ref), N, bsz, bid, j)
+        if j < k:
+            cnt = nb - j - 1
+            lib.or_trsm_panel(ol.ptr(ref), bsz, bid, j, j + 1, cnt)
+            lib.or_syrk_diag(ol.ptr(ref), bsz, bid, j, j + 1, cnt, nb)
+            if cnt > 1:
+                lib.or_gemm_trailing(ol.ptr(ref), bsz, bid, j, j + 2, cnt - 1, nb)
+    bid = T - (nb - k) * (nb - k + 1) // 2
+    ctx.set_problem(N, bsz)
+    A = torch.from_numpy(ref).cuda()
+    cnt = nb - k - 1
+    hs.MatrixMatrixOperations.triangularSolve(ctx, A, bid, k, k + 1, cnt)
+    lib.or_trsm_panel(ol.ptr(ref), bsz, bid, k, k + 1, cnt)
+    got = A.cpu().numpy()
+    panel = slice((bid + 1) * bsz * bsz, (bid + 1 + cnt) * bsz * bsz)
+    rel = np.linalg.norm(got[panel] - ref[panel]) / np.linalg.norm(ref[panel])
+    assert rel <= 1e-12, rel
+    keep = np.ones(got.size, dtype=bool)
+    keep[panel] = False
+    assert np.array_equal(got[keep], ref[keep])
 
 
 @pytest.mark.parametrize("N,bsz", [(1000, 128), (700, 256), (130, 20)])
