@@ -221,7 +221,7 @@ hs_status hs_ctx_create(int device, void* stream, hs_ctx* out) {
     }
     HS_CUDA(cudaEventCreateWithFlags(&ctx->ev_a, cudaEventDisableTiming));
     HS_CUDA(cudaEventCreateWithFlags(&ctx->ev_b, cudaEventDisableTiming));
-    HS_CUDA(cudaMalloc(&ctx->d_info, sizeof(long long)));
+    HS_CUDA(cudaMalloc(&ctx->d_info, 2 * sizeof(long long)));
     HS_CUDA(cudaMallocHost(&ctx->h_pinned, 64 * sizeof(double)));
     set_i64_kernel<<<1, 1, 0, ctx->stream>>>(ctx->d_info, INT64_MAX);
     HS_CUDA(cudaGetLastError());

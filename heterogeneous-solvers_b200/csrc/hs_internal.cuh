@@ -36,7 +36,9 @@ struct hs_ctx_s {
     void* hostws = nullptr;
     size_t hostws_bytes = 0;
 
-    // device word holding the smallest failing pivot row (INT64_MAX = none)
+    // device words: [0] the smallest failing pivot row (INT64_MAX = none); [1] the
+    // bit pattern of the most negative failing pivot of the mixed factor's FP64
+    // diagonal blocks (LLONG_MIN, the pattern of -0.0 = none recorded)
     long long* d_info = nullptr;
     // pinned host staging for scalars read back by the solver drivers
     double* h_pinned = nullptr;

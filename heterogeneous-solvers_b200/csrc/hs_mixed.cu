@@ -7,7 +7,10 @@
 // packed K and the FP64 matvec; the triangular solves apply the FP32 factor
 // with FP64 arithmetic (FP32 off-diagonal blocks, FP64 inverses of the
 // diagonal blocks), one fused launch per block column and direction.
+#include <algorithm>
 #include <chrono>
+#include <climits>
+#include <cstring>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -209,8 +212,9 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
     };
     if (prec == HS_PRECISION_F16X3 && (st = read_maxdiag()) != HS_OK) return st;
     for (int attempt = 1;; ++attempt) {
-        ctx->launches += 1;
+        ctx->launches += 2;
         set_i64_dev(ctx->d_info, INT64_MAX, s);
+        set_i64_dev(ctx->d_info + 1, LLONG_MIN, s);
         // the first attempt's conversion to FP32 also sums ||K||_F^2
         st = mixed_factor(ctx, K, w, s, shift, prec, attempt == 1 ? part : nullptr, have_maxdiag ? h[9] + shift : 0.0);
         if (st != HS_OK) return st;
@@ -218,14 +222,24 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
         if (ctx->side) HS_CUDA(cudaStreamSynchronize(ctx->side));
         st = mixed_check_error(ctx, w);
         if (st != HS_OK) return st;
+        long long piv_bits = LLONG_MIN;
+        HS_CUDA(cudaMemcpyAsync(&piv_bits, ctx->d_info + 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
         int64_t info = -1;
-        st = hs_ctx_take_info(ctx, &info);
+        st = hs_ctx_take_info(ctx, &info);  // synchronises the stream
         if (st != HS_OK) return st;
         R.factor_attempts = attempt;
         R.precision_used = prec;
         R.shift = shift;
         if (info < 0) break;
-        if (prec == HS_PRECISION_BF16X3 || prec == HS_PRECISION_F16X3) {  // the more accurate split products first
+        // the failing pivot (NaN when the scaled FP16 panel overflowed: no value)
+        double piv = 0.0;
+        std::memcpy(&piv, &piv_bits, sizeof(piv));
+        const bool have_piv = piv_bits != LLONG_MIN && std::isfinite(piv) && piv < 0.0;
+        // the BF16 split (16 significant bits) is redone with 3xTF32 products, which
+        // hold ~2^-21; so is a FP16 split that failed without a finite pivot (an
+        // overflow of the scaled panel).  A FP16 split (~2^-22) that met a negative
+        // pivot is past what any FP32 factor holds: straight to the shift.
+        if (prec == HS_PRECISION_BF16X3 || (prec == HS_PRECISION_F16X3 && !have_piv)) {
             prec = HS_PRECISION_TF32X3;
             continue;
         }
@@ -234,12 +248,14 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
                       std::to_string(info) + " even with a diagonal shift of " + std::to_string(shift));
             return HS_ERR_NOT_SPD;
         }
-        if (shift == 0.0) {
-            if (!have_maxdiag && (st = read_maxdiag()) != HS_OK) return st;
-            shift = 1e-6 * h[9];
-        } else {
-            shift *= 10.0;  // 1e-6 .. 1e-1 x the largest diagonal entry
-        }
+        if (!have_maxdiag && (st = read_maxdiag()) != HS_OK) return st;
+        // a pivot -p < 0 means the rounding of the factor moved a Schur complement by
+        // more than p (the exact one is positive); rows further down collect more
+        // rounding, so the next shift covers 30 p on top of the shift so far, at least
+        // 10x that shift (or 1e-6 x the largest diagonal entry), at most 0.05x
+        const double floor_shift = shift > 0.0 ? 10.0 * shift : 1e-6 * h[9];
+        shift = have_piv ? std::max(floor_shift, shift + 30.0 * -piv) : floor_shift;
+        shift = std::min(shift, 0.05 * h[9]);
     }
     // the sweeps read the inverse diagonal blocks in FP32 (their rounding is far below
     // the factor's own error), from the 16-bit panel area the factor no longer needs

@@ -107,6 +107,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     uint64_t* empty = full + SM::kStages;
     uint64_t* done = empty + SM::kStages;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+    __shared__ int s_fail;  // a wait of the producer or the MMA issuer ran out
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const size_t bb = (size_t)BSZ * BSZ;
@@ -128,6 +129,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         mbar_init(done, 1);
         fence_barrier_init();
+        s_fail = 0;
     }
     if (warp == 0) {
         tmem_alloc(tslot, BSZ);
@@ -143,6 +145,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
     if (tid == 0) {
         // ---- producer
+        int issued = 0;
         for (int kc = 0; kc < kSlabs && ok; ++kc) {
             const int s = kc % SM::kStages, use = kc / SM::kStages;
             if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, deadline)) { ok = false; break; }
@@ -152,8 +155,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             tma_load_3d(st + SM::kABytes, &mL128, &full[s], kc * kSlab, ti * 128, gA);
             tma_load_3d(st + 2 * SM::kABytes, &mLB, &full[s], kc * kSlab, 0, blkB);
             tma_load_3d(st + 2 * SM::kABytes + SM::kBBytes, &mLB, &full[s], kc * kSlab, 0, gB);
+            ++issued;
         }
-        if (!ok) atomicExch(a.err, 1);
+        if (!ok) {
+            s_fail = 1;
+            atomicExch(a.err, 1);
+        }
+        // no load may still be writing into shared memory when the CTA leaves: wait
+        // (bounded) for the phase each stage was last armed with (a completed phase
+        // passes at once)
+        for (int kc = issued > SM::kStages ? issued - SM::kStages : 0; kc < issued; ++kc)
+            if (!mbar_wait_for(&full[kc % SM::kStages], (kc / SM::kStages) & 1, kWaitNs)) atomicExch(a.err, 1);
     } else if (tid == 32) {
         // ---- MMA issuer
         constexpr uint32_t idesc = umma_idesc(kFmtTF32, kFmtTF32, 128, BSZ);
@@ -175,18 +187,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
             umma_commit(&empty[s]);
         }
-        if (ok) umma_commit(done);
-        else atomicExch(a.err, 1);
+        if (!ok) {
+            s_fail = 1;
+            atomicExch(a.err, 1);
+        }
+        // "done" arrives once every MMA this thread issued has completed, also after a
+        // wait ran out: TMEM is released only after that
+        umma_commit(done);
     }
-    __syncwarp();
+    __syncthreads();  // the roles have issued all their work; s_fail is final
 
     // ---- epilogue: all 4 warps, thread = tile row
     int wok = 0;
-    if (lane == 0) wok = mbar_wait(done, 0, deadline) ? 1 : 0;
+    if (lane == 0) wok = mbar_wait_for(done, 0, kWaitNs) ? 1 : 0;
     const bool done_ok = __shfl_sync(0xffffffffu, wok, 0) != 0;
     __syncwarp();
     tc_fence_after();
-    if (!done_ok) {
+    if (!done_ok || s_fail) {
         if (lane == 0) atomicExch(a.err, 1);
     } else {
 #pragma unroll 1
@@ -366,7 +383,8 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     uint64_t* empty = full + SM::kStages;
     uint64_t* tfull = empty + SM::kStages;
     uint64_t* tempty = tfull + 2;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(tempty + 2);
+    uint64_t* drained = tempty + 2;  // every MMA of the issuer has completed
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(drained + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m = a.nb - a.first_col;
@@ -384,6 +402,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             mbar_init(&tfull[b], 1);
             mbar_init(&tempty[b], 8);
         }
+        mbar_init(drained, 1);
         fence_barrier_init();
     }
     if (warp == 0) {
@@ -449,6 +468,11 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                 }
             }
             if (!ok) atomicExch(a.err, 1);
+            // no load may still be writing into shared memory when the CTA leaves: wait
+            // (bounded) for the phase each stage was last armed with (slabs g - kStages ..
+            // g - 1; a completed phase passes at once)
+            for (uint32_t h = g > (uint32_t)SM::kStages ? g - SM::kStages : 0; h < g; ++h)
+                if (!mbar_wait_for(&full[h % SM::kStages], (h / SM::kStages) & 1, kStepWaitNs)) atomicExch(a.err, 1);
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -495,6 +519,10 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                 umma_commit(&tfull[b]);
             }
             if (!ok) atomicExch(a.err, 1);
+            // TMEM is released only after every MMA issued here has completed, also
+            // after a wait ran out
+            umma_commit(drained);
+            if (!mbar_wait_for(drained, 0, kStepWaitNs)) atomicExch(a.err, 1);
         }
     } else {
         // ---- epilogue warps 2..9: lane quarter q = warp % 4 holds tile rows 32q..32q+31;
@@ -700,7 +728,13 @@ __device__ __forceinline__ void chain_diag(double* __restrict__ D, double* __res
     double piv = __shfl_sync(0xffffffffu, x[0], 0);
 #pragma unroll
     for (int k = 0; k < 32; ++k) {
-        if (lane == 0 && d0 + k < valid && !(piv > 0.0)) atomicMin(info, row_base + d0 + k);
+        if (lane == 0 && d0 + k < valid && !(piv > 0.0)) {
+            atomicMin(info, row_base + d0 + k);
+            // info[1]: the most negative failing pivot (bit pattern of a negative double;
+            // a larger signed pattern is a larger magnitude); NaN and zero pivots are not
+            // recorded
+            if (piv < 0.0) atomicMax(info + 1, __double_as_longlong(piv));
+        }
         const double ri = rsqrt(piv);
         const double lk = lane == k ? piv * ri : (lane > k ? x[k] * ri : 0.0);  // L[lane][k]
         const double zk = z[k] * ri;                                            // X[k][lane]
