@@ -62,7 +62,7 @@ struct AdjointWork {
     double* partial;  // split-chain partial blocks
     int64_t partial_blocks;
 };
-constexpr int64_t kAdjointPartialBlocks = 128;
+constexpr int64_t kAdjointPartialBlocks = 512;
 size_t adjoint_work_bytes(int nb, int bsz);
 void adjoint_bind(void* base, int nb, int bsz, AdjointWork* w);
 // Abar (packed lower blocks, holding Lbar on entry) <- adjoint of the lower

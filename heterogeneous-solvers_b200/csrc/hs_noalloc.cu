@@ -21,9 +21,15 @@
 //  * Nothing in the array needs to start at zero: every partial slot the
 //    second kernel reads is written by the first kernel of the same call, so
 //    the contents a previous call left behind are never used.
-//  * The array's device address is looked up once per device, by the first
-//    call made on that device, with that device current; make that first call
-//    before any stream capture begins.
+//  * The array's device address is looked up once per device (and again after
+//    the device's primary context was reset, e.g. by cudaDeviceReset), by the
+//    first call made there, with that device current; make that first call
+//    before any stream capture begins.  Devices 0..63 are supported.
+//  * In reference-order mode (hs_ctx_set_reference_order) the call runs the
+//    reference-order kernel of hs_symv_block, which needs no scratch at all: the
+//    two entry points give the same bits in either mode.
+#include <cudaTypedefs.h>
+
 #include <mutex>
 
 #include "hs_internal.cuh"
@@ -35,23 +41,46 @@ static __device__ __align__(256) double g_symv_noalloc_scratch[HS_SYMV_NOALLOC_M
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
-double* g_scratch_addr[kMaxDevices] = {};
+struct ScratchAddr {
+    CUcontext owner = nullptr;  // the context the address belongs to
+    double* ptr = nullptr;
+};
+ScratchAddr g_scratch_addr[kMaxDevices];
+PFN_cuCtxGetCurrent_v4000 g_ctx_current = nullptr;
 
-// set-up, once per device, with `device` current: the host-side symbol is only
-// a stand-in, the kernels need the array's device address
+// set-up, once per device context, with `device` current: the host-side symbol is
+// only a stand-in, the kernels need the array's device address
 hs_status scratch_address(int device, double** out) {
     if (device < 0 || device >= kMaxDevices) {
-        hs::set_error("hs_symv_block_noalloc: device index out of range");
+        hs::set_error("hs_symv_block_noalloc: device index out of range (devices 0..63 are supported)");
         return HS_ERR_INVALID_ARG;
     }
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[device]) {
+    if (!g_ctx_current) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        const cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess) return hs::cuda_fail(e, "cudaGetDriverEntryPoint(cuCtxGetCurrent)");
+        if (q != cudaDriverEntryPointSuccess || !fn) {
+            hs::set_error("hs_symv_block_noalloc: cuCtxGetCurrent is not available from the driver");
+            return HS_ERR_UNSUPPORTED;
+        }
+        g_ctx_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(fn);
+    }
+    CUcontext cur = nullptr;
+    if (g_ctx_current(&cur) != CUDA_SUCCESS || !cur) {
+        hs::set_error("hs_symv_block_noalloc: no current CUDA context");
+        return HS_ERR_CUDA;
+    }
+    ScratchAddr& a = g_scratch_addr[device];
+    if (!a.ptr || a.owner != cur) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_symv_noalloc_scratch);
         if (e != cudaSuccess) return hs::cuda_fail(e, "cudaGetSymbolAddress(g_symv_noalloc_scratch)");
-        g_scratch_addr[device] = static_cast<double*>(p);
+        a.ptr = static_cast<double*>(p);
+        a.owner = cur;
     }
-    *out = g_scratch_addr[device];
+    *out = a.ptr;
     return HS_OK;
 }
 
@@ -75,6 +104,9 @@ extern "C" hs_status hs_symv_block_noalloc(hs_ctx ctx, const double* A, const do
         hs::set_error("hs_symv_block_noalloc: blocks out of range");
         return HS_ERR_INVALID_ARG;
     }
+    if (ctx->ref_chunks > 0)  // the reference-order kernel of hs_symv_block uses no scratch
+        return hs::launch_symv_refseq(ctx, A, b, result, blockStart_i, blockStart_j, blockCount_i, blockCount_j,
+                                      reset, ctx->stream);
     const long long need = (long long)blockCount_i * blockCount_j * ctx->bsz;
     if (need > (long long)HS_SYMV_NOALLOC_MAX_DOUBLES) {
         hs::set_error("hs_symv_block_noalloc: this rectangle needs " + std::to_string(need) +

@@ -276,12 +276,25 @@ __global__ void sym_tril_half_kernel(const double* __restrict__ G, double* __res
     }
 }
 
+// Split count of a chain over `base_ctas` output tiles (one CTA an SM): the s that
+// minimises the time model waves(base s) x ceil(chain / s) chain steps, plus the
+// fixed-order reduction of the s partial blocks of each item (~0.1 chain step a
+// partial tile an SM), so that the last wave is not left mostly empty.
 int pick_splits(int64_t base_ctas, int64_t chain, int items, int64_t partial_blocks, int sms) {
-    int64_t s = (2LL * sms + base_ctas - 1) / base_ctas;
-    if (s > chain) s = chain;
-    if (s < 1) s = 1;
-    while (s > 1 && s * items > partial_blocks) --s;
-    return (int)s;
+    int64_t best = 1;
+    double best_cost = 1e300;
+    const int64_t smax = chain < 64 ? chain : 64;
+    for (int64_t s = 1; s <= smax; ++s) {
+        if (s > 1 && s * items > partial_blocks) break;
+        const int64_t waves = (base_ctas * s + sms - 1) / sms;
+        const double cost = (double)waves * (double)((chain + s - 1) / s) +
+                            (s > 1 ? 0.1 * (double)(base_ctas * s) / sms : 0.0);
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best = s;
+        }
+    }
+    return (int)best;
 }
 
 bool g_chain_attr[64] = {};

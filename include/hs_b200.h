@@ -170,8 +170,11 @@ hs_status hs_symv_block(hs_ctx ctx, const double* A, const double* b, double* re
  * (blockCount_i * blockCount_j * matrixBlockSize doubles) is rejected with
  * HS_ERR_INVALID_ARG.  All calls on a device share the array, so calls whose
  * kernels can overlap on that device race on it: order them on one stream.  The
- * first call on each device looks up the array's device address (with that device
- * current); make that first call before any stream capture starts. */
+ * first call on each device (and the first after a reset of its context) looks up
+ * the array's device address, with that device current; make that first call
+ * before any stream capture starts.  Devices 0..63.  In reference-order mode
+ * (hs_ctx_set_reference_order) it runs hs_symv_block's reference-order kernel,
+ * which uses no scratch: the two entry points give the same bits in both modes. */
 #define HS_SYMV_NOALLOC_MAX_DOUBLES (2 * 1024 * 1024)
 hs_status hs_symv_block_noalloc(hs_ctx ctx, const double* A, const double* b, double* result, int blockStart_i,
                                 int blockStart_j, int blockCount_i, int blockCount_j, int blockCountXY, int reset);

@@ -66,3 +66,66 @@ def test_noalloc_matvec_rejects_rectangles_beyond_its_scratch(hs, ctx):
     st = lib.hs_symv_block_noalloc(ctx.handle, _p(dummy), _p(dummy), _p(dummy), 0, 0, nb, nb, nb, 1)
     assert st == 1  # HS_ERR_INVALID_ARG, nothing launched
     assert "static scratch holds" in lib.hs_last_error().decode()
+
+
+def test_noalloc_matvec_allocates_nothing_on_a_fresh_context(hs, ctx):
+    """On a context that has never run the allocating matvec, only the no-alloc
+    entry point is called: the product matches the dense one and the device's free
+    memory does not move.  The rectangle is the largest the static scratch takes
+    (nb * nb * bsz == HS_SYMV_NOALLOC_MAX_DOUBLES: N = 16384, bsz = 128)."""
+    N, bsz = 16384, 128
+    rng = np.random.default_rng(8)
+    X = rng.random((N, 4))
+    lib = hs._lib.load()
+    with hs.Context(device=0) as warm:  # kernels loaded once per process, outside the measurement
+        warm.set_problem(256, 128)
+        z = torch.zeros(hs.packed_size(256, 128), dtype=torch.float64, device="cuda")
+        v = torch.zeros(256, dtype=torch.float64, device="cuda")
+        w = torch.zeros(256, dtype=torch.float64, device="cuda")
+        hs._lib.check(lib.hs_symv_block_noalloc(warm.handle, _p(z), _p(v), _p(w), 0, 0, 2, 2, 2, 1))
+        warm.sync()
+    K = torch.empty(hs.packed_size(N, bsz), dtype=torch.float64, device="cuda")
+    b = torch.from_numpy(rng.standard_normal(N)).cuda()
+    out = torch.full((N,), np.nan, dtype=torch.float64, device="cuda")
+    with hs.Context(device=0) as fresh:
+        fresh.set_problem(N, bsz)
+        hs.MatrixGenerator.assemble(fresh, K, X, 0.5, 1.0, 1e-2)
+        nb = fresh.blockCountXY
+        assert nb * nb * bsz == MAX_DOUBLES
+        fresh.sync()
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        for _ in range(2):
+            hs._lib.check(lib.hs_symv_block_noalloc(fresh.handle, _p(K), _p(b), _p(out), 0, 0, nb, nb, nb, 1))
+        fresh.sync()
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 == free0, (free0, free1)
+        # one block row more than the scratch holds is rejected before any launch
+        fresh.set_problem(N + bsz, bsz)
+        nb1 = fresh.blockCountXY
+        assert nb1 * nb * bsz > MAX_DOUBLES
+        st = lib.hs_symv_block_noalloc(fresh.handle, _p(K), _p(b), _p(out), 0, 0, nb1, nb, nb1, 1)
+        assert st == 1
+    Kd = ol.packed_to_dense(K.cpu().numpy(), N, bsz)
+    dense = Kd @ b.cpu().numpy()
+    assert np.allclose(out.cpu().numpy(), dense, rtol=1e-12, atol=1e-12)
+
+
+def test_noalloc_matvec_in_reference_order_mode_is_bitwise_equal(hs, ctx):
+    """In reference-order mode both entry points run the reference-order kernel."""
+    N, bsz = 700, 128
+    rng = np.random.default_rng(9)
+    X = rng.random((N, 8))
+    K = torch.from_numpy(ol.rbf_assemble(X, bsz, 0.5, 1.0, 1e-2)).cuda()
+    ctx.set_problem(N, bsz)
+    nb = ctx.blockCountXY
+    n = nb * bsz
+    b = torch.from_numpy(rng.standard_normal(n)).cuda()
+    ctx.set_reference_order(8)
+    try:
+        for _ in range(2):
+            ref, new = _matvec_both(hs, ctx, K, b, (0, 0, nb, nb), 1, torch.zeros(n, dtype=torch.float64,
+                                                                                  device="cuda"))
+            assert np.array_equal(ref, new)
+    finally:
+        ctx.set_reference_order(0)
