@@ -24,13 +24,18 @@
 namespace hs {
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4;
-constexpr int SPAD = 20;   // row pitch (doubles) of K-contiguous operand rows
-constexpr int LDT = 136;   // row pitch (doubles) of M/N-contiguous operand rows
-constexpr int kStageA = BM * SPAD;  // >= BK * LDT
-constexpr int kStage = 2 * kStageA;
-constexpr int kChainSmem = STAGES * kStage * (int)sizeof(double);  // 160 KB
-static_assert(BK * LDT <= kStageA, "stage layout");
+// 128 x 64 output tiles, 8 warps of 32 x 32, 3-stage ring: 128 registers and 90 KB of
+// shared memory, two CTAs an SM (one CTA's prologue / epilogue beside the other's MMAs)
+constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3;
+constexpr int WM = 32, WN = 32, kWarpsN = BN / WN;
+constexpr int SPAD = 20;        // row pitch (doubles) of K-contiguous operand rows
+constexpr int LDTA = BM + 8;    // row pitch (doubles) of M-contiguous A rows
+constexpr int LDTB = BN + 8;    // row pitch (doubles) of N-contiguous B rows
+constexpr int kStageA = BM * SPAD;  // >= BK * LDTA
+constexpr int kStageB = BN * SPAD;  // >= BK * LDTB
+constexpr int kStage = kStageA + kStageB;
+constexpr int kChainSmem = STAGES * kStage * (int)sizeof(double);  // 90 KB
+static_assert(BK * LDTA <= kStageA && BK * LDTB <= kStageB, "stage layout");
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -76,31 +81,31 @@ __device__ __forceinline__ Elem chain_elem(const ChainArgs& a, int item, int64_t
     return e;
 }
 
-// One CTA = one 128 x 128 tile of one output block, accumulating the chain
-// elements [q0, q1) of its item; 8 warps of 64 x 32, K streamed in 16-wide
-// slabs through a 4-stage cp.async ring.  Operands that enter transposed are
+// One CTA = one 128 x 64 tile of one output block, accumulating the chain
+// elements [q0, q1) of its item; 8 warps of 32 x 32, K streamed in 16-wide
+// slabs through a 3-stage cp.async ring.  Operands that enter transposed are
 // staged with the M (or N) index contiguous, the others with K contiguous.
-__global__ void __launch_bounds__(256, 1) chain_dmma_kernel(ChainArgs a) {
+__global__ void __launch_bounds__(256, 2) chain_dmma_kernel(ChainArgs a) {
     extern __shared__ __align__(16) double smem[];
-    const int tps = a.bsz / BM;
+    const int tpm = a.bsz / BM, tpn = a.bsz / BN;
     const int64_t idx = blockIdx.x;
     const int split = (int)(idx % a.splits);
     const int64_t rest = idx / a.splits;
-    const int tile = (int)(rest % (tps * tps));
-    const int item = (int)(rest / (tps * tps));
-    const int ti = tile / tps, tj = tile % tps;
+    const int tile = (int)(rest % (tpm * tpn));
+    const int item = (int)(rest / (tpm * tpn));
+    const int ti = tile / tpn, tj = tile % tpn;
     const int64_t q0 = a.chain * split / a.splits, q1 = a.chain * (split + 1) / a.splits;
     const int spb = a.bsz / BK;  // slabs per chain element
     const int64_t nk = (q1 - q0) * spb;
     const int bsz = a.bsz;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int wm = warp >> 2, wn = warp & 3;
+    const int wm = warp / kWarpsN, wn = warp % kWarpsN;
     const int g = lane >> 2, t = lane & 3;
 
-    double acc[8][4][2];
+    double acc[4][4][2];
 #pragma unroll
-    for (int mi = 0; mi < 8; ++mi)
+    for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
 
@@ -110,19 +115,23 @@ __global__ void __launch_bounds__(256, 1) chain_dmma_kernel(ChainArgs a) {
         double* As = smem + stage * kStage;
         double* Bs = As + kStageA;
 #pragma unroll
-        for (int qq = 0; qq < 4; ++qq) {
+        for (int qq = 0; qq < 4; ++qq) {  // A: 1024 16-byte copies
             const int x = tid + 256 * qq;
             if (!e.ta) {  // A_op[m][k] = A[ti*128+m][kc+k]: rows m, K contiguous
                 const int row = x >> 3, ch = x & 7;
                 cp_async16(As + row * SPAD + ch * 2, e.A + (size_t)(ti * BM + row) * bsz + kc + ch * 2);
             } else {      // A_op[m][k] = A[kc+k][ti*128+m]: rows k, M contiguous
                 const int row = x >> 6, ch = x & 63;
-                cp_async16(As + row * LDT + ch * 2, e.A + (size_t)(kc + row) * bsz + ti * BM + ch * 2);
+                cp_async16(As + row * LDTA + ch * 2, e.A + (size_t)(kc + row) * bsz + ti * BM + ch * 2);
             }
-            if (!e.tb) {  // B_op[k][n] = B[kc+k][tj*128+n]: rows k, N contiguous
-                const int row = x >> 6, ch = x & 63;
-                cp_async16(Bs + row * LDT + ch * 2, e.B + (size_t)(kc + row) * bsz + tj * BN + ch * 2);
-            } else {      // B_op[k][n] = B[tj*128+n][kc+k]: rows n, K contiguous
+        }
+#pragma unroll
+        for (int qq = 0; qq < 2; ++qq) {  // B: 512 16-byte copies
+            const int x = tid + 256 * qq;
+            if (!e.tb) {  // B_op[k][n] = B[kc+k][tj*64+n]: rows k, N contiguous
+                const int row = x >> 5, ch = x & 31;
+                cp_async16(Bs + row * LDTB + ch * 2, e.B + (size_t)(kc + row) * bsz + tj * BN + ch * 2);
+            } else {      // B_op[k][n] = B[tj*64+n][kc+k]: rows n, K contiguous
                 const int row = x >> 3, ch = x & 7;
                 cp_async16(Bs + row * SPAD + ch * 2, e.B + (size_t)(tj * BN + row) * bsz + kc + ch * 2);
             }
@@ -146,23 +155,23 @@ __global__ void __launch_bounds__(256, 1) chain_dmma_kernel(ChainArgs a) {
         const double* Bs = As + kStageA;
 #pragma unroll
         for (int kk = 0; kk < BK / 4; ++kk) {
-            double av[8], bv[4];
+            double av[4], bv[4];
             if (!e.ta) {
 #pragma unroll
-                for (int mi = 0; mi < 8; ++mi) av[mi] = As[(wm * 64 + mi * 8 + g) * SPAD + kk * 4 + t];
+                for (int mi = 0; mi < 4; ++mi) av[mi] = As[(wm * WM + mi * 8 + g) * SPAD + kk * 4 + t];
             } else {
 #pragma unroll
-                for (int mi = 0; mi < 8; ++mi) av[mi] = As[(kk * 4 + t) * LDT + wm * 64 + mi * 8 + g];
+                for (int mi = 0; mi < 4; ++mi) av[mi] = As[(kk * 4 + t) * LDTA + wm * WM + mi * 8 + g];
             }
             if (!e.tb) {
 #pragma unroll
-                for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(kk * 4 + t) * LDT + wn * 32 + ni * 8 + g];
+                for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(kk * 4 + t) * LDTB + wn * WN + ni * 8 + g];
             } else {
 #pragma unroll
-                for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(wn * 32 + ni * 8 + g) * SPAD + kk * 4 + t];
+                for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(wn * WN + ni * 8 + g) * SPAD + kk * 4 + t];
             }
 #pragma unroll
-            for (int mi = 0; mi < 8; ++mi)
+            for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
                 for (int ni = 0; ni < 4; ++ni) dmma884(acc[mi][ni], av[mi], bv[ni]);
         }
@@ -183,11 +192,11 @@ __global__ void __launch_bounds__(256, 1) chain_dmma_kernel(ChainArgs a) {
     }
     const double alpha = a.alpha;
 #pragma unroll
-    for (int mi = 0; mi < 8; ++mi)
+    for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni) {
-            const int r = ti * BM + wm * 64 + mi * 8 + g;
-            const int c = tj * BN + wn * 32 + ni * 8 + 2 * t;
+            const int r = ti * BM + wm * WM + mi * 8 + g;
+            const int c = tj * BN + wn * WN + ni * 8 + 2 * t;
             double* p = C + (size_t)r * bsz + c;
             const double v0 = alpha * acc[mi][ni][0], v1 = alpha * acc[mi][ni][1];
             if (epi == EPI_STORE) {
@@ -276,10 +285,10 @@ __global__ void sym_tril_half_kernel(const double* __restrict__ G, double* __res
     }
 }
 
-// Split count of a chain over `base_ctas` output tiles (one CTA an SM): the s that
+// Split count of a chain over `base_ctas` output tiles (`sms` = CTAs resident at once): the s that
 // minimises the time model waves(base s) x ceil(chain / s) chain steps, plus the
 // fixed-order reduction of the s partial blocks of each item (~0.1 chain step a
-// partial tile an SM), so that the last wave is not left mostly empty.
+// partial tile a CTA slot), so that the last wave is not left mostly empty.
 int pick_splits(int64_t base_ctas, int64_t chain, int items, int64_t partial_blocks, int sms) {
     int64_t best = 1;
     double best_cost = 1e300;
@@ -315,9 +324,8 @@ hs_status launch_chain(hs_ctx ctx, ChainArgs a, double* partial, int64_t partial
     if (st != HS_OK) return st;
     HS_REQUIRE(a.bsz == 128 || a.bsz == 256, "the tensor-core adjoint supports matrixBlockSize 128 or 256");
     if (a.items <= 0 || a.chain <= 0) return HS_OK;
-    const int tps = a.bsz / BM;
-    const int64_t base = (int64_t)a.items * tps * tps;
-    a.splits = (partial && a.allow_split) ? pick_splits(base, a.chain, a.items, partial_blocks, ctx->num_sms) : 1;
+    const int64_t base = (int64_t)a.items * (a.bsz / BM) * (a.bsz / BN);
+    a.splits = (partial && a.allow_split) ? pick_splits(base, a.chain, a.items, partial_blocks, 2 * ctx->num_sms) : 1;
     a.partial = partial;
     const int64_t grid = base * a.splits;
     HS_REQUIRE(grid < (1LL << 31), "too many tiles");

@@ -214,12 +214,14 @@ def test_config1_parity_with_oracle(hs, ctx):
     rhs = hs.RightHandSide(N, bsz)
     rhs.rightHandSideData.copy_(torch.from_numpy(b))
     cg = hs.CG(Ah, rhs, ctx).solveHeterogeneous(epsilon=cfg["eps"], iMax=100000)
-    its = [ol.cg(K, b, N, bsz, cfg["eps"], 100000, chunks=c)[1] for c in (1, 8, 64, 224)]
-    # ~900 iterations: the reference's own count moves by ~1% with its core count
-    # (924..931 over 1..224 chunks); the fused tree-reduced path must stay within 2%
-    slack = max(1, int(0.02 * max(its)))
-    assert min(its) - slack <= cg.iterations <= max(its) + slack, (cg.iterations, its)
-    assert np.linalg.norm(cg.x.numpy() - x_cg_ref) / np.linalg.norm(x_cg_ref) <= 1e-8
+    its = [ol.cg(K, b, N, bsz, cfg["eps"], 100000, chunks=c)[1] for c in CHUNK_COUNTS]
+    # ~920 iterations: the reference's own count moves with its core count (915..931
+    # over 1..224 chunks, VectorOperations.cpp:197-218); the fused tree-reduced path
+    # lands inside that spread (917 measured), checked to +-1
+    print(f"C1 CG: fast path {cg.iterations} iterations, oracle {dict(zip(CHUNK_COUNTS, its))}")
+    assert min(its) - 1 <= cg.iterations <= max(its) + 1, (cg.iterations, its)
+    # x of two CG runs to eps = 1e-10 in different summation orders (measured 1.9e-12)
+    assert np.linalg.norm(cg.x.numpy() - x_cg_ref) / np.linalg.norm(x_cg_ref) <= 1e-11
     # reference order: the oracle's iterates exactly
     cg8 = _cg_gpu(hs, ctx, K, b, N, bsz, cfg["eps"], 100000, chunks=8)
     assert cg8.iterations == it_ref and np.array_equal(cg8.x.numpy(), x_cg_ref)
