@@ -250,11 +250,12 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
         }
         if (!have_maxdiag && (st = read_maxdiag()) != HS_OK) return st;
         // a pivot -p < 0 means the rounding of the factor moved a Schur complement by
-        // more than p (the exact one is positive); rows further down collect more
-        // rounding, so the next shift covers 30 p on top of the shift so far, at least
-        // 10x that shift (or 1e-6 x the largest diagonal entry), at most 0.05x
+        // more than p (the exact one is positive): the next shift covers 2 p on top of
+        // the shift so far, and is at least 10x that shift (or 1e-6 x the largest
+        // diagonal entry), at most 0.05x.  (30 p overshot: a weaker preconditioner cost
+        // more CG iterations than the attempts it saved.)
         const double floor_shift = shift > 0.0 ? 10.0 * shift : 1e-6 * h[9];
-        shift = have_piv ? std::max(floor_shift, shift + 30.0 * -piv) : floor_shift;
+        shift = have_piv ? std::max(floor_shift, shift + 2.0 * -piv) : floor_shift;
         shift = std::min(shift, 0.05 * h[9]);
     }
     // the sweeps read the inverse diagonal blocks in FP32 (their rounding is far below

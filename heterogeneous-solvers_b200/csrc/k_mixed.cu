@@ -277,8 +277,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 //                        the tile's C rows
 //   warp 1 (one thread)  MMA issuer: kUpdK/8 x 3 tcgen05.mma per slab (hi*hi, hi*lo,
 //                        lo*hi) into one of two TMEM accumulators (2 x BSZ
-//                        columns), so that the epilogue of tile i overlaps the
-//                        MMAs of tile i+1
+//                        columns), one accumulation a (tile, panel) unit, so that
+//                        the epilogue of a unit overlaps the MMAs of the next
 //   warps 2-9            epilogue: TMEM -> registers -> -D in a swizzled shared
 //                        tile -> TMA reduce-add into C (two warps per TMEM lane
 //                        quarter, half the columns each), then free the
@@ -477,46 +477,54 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     } else if (warp == 1) {
         if (lane == 0) {
             // ---- MMA issuer
+            // one accumulation unit = one tile x one panel (K = BSZ): each panel's product
+            // is added into C on its own (an FP32 round-to-nearest add in L2), instead of
+            // the whole group's K = npanels x BSZ sum in TMEM first, whose accumulation
+            // measured several times less accurate (log|K| and the unrefined backward
+            // error); the C tile stays in L2 across its units, so the DRAM traffic of a
+            // group pass is unchanged
             constexpr uint32_t idesc = umma_idesc(F::kFmt, F::kFmt, 128, BSZ);
             uint32_t g = 0;
-            int it = 0;
-            for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++it) {
-                const int b = it & 1, u = it >> 1;
-                if (u > 0 && !mbar_wait_for(&tempty[b], (u - 1) & 1, kStepWaitNs)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t dcol = taddr + (uint32_t)(b * BSZ);
-                for (int kc = 0; kc < kSlabs; ++kc, ++g) {
-                    const uint32_t s = g % SM::kStages, use = g / SM::kStages;
-                    if (!mbar_wait_for(&full[s], use & 1, kStepWaitNs)) {
+            int un = 0;
+            for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                for (int pi = 0; pi < a.npanels && ok; ++pi, ++un) {
+                    const int b = un & 1, u = un >> 1;
+                    if (u > 0 && !mbar_wait_for(&tempty[b], (u - 1) & 1, kStepWaitNs)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t base = smem_u32(smem + s * SM::kStage);
-                    const uint32_t aHi = base, bHi = base + SM::kA;
-                    const uint32_t aLo = base + SM::kRaw, bLo = aLo + SM::kA;
-#pragma unroll
-                    for (int ks = 0; ks < F::kK / F::kKStep; ++ks) {
-                        const uint32_t off = ks * 32;  // one K step = 32 bytes along K
-                        const uint64_t dAh = upd_desc(aHi + off), dAl = upd_desc(aLo + off);
-                        const uint64_t dBh = upd_desc(bHi + off), dBl = upd_desc(bLo + off);
-                        if (PREC != HS_PRECISION_TF32X3) {
-                            umma_f16(dcol, dAh, dBh, idesc, (kc | ks) != 0);
-                            umma_f16(dcol, dAh, dBl, idesc, 1);
-                            umma_f16(dcol, dAl, dBh, idesc, 1);
-                        } else {
-                            umma_tf32(dcol, dAh, dBh, idesc, (kc | ks) != 0);
-                            umma_tf32(dcol, dAh, dBl, idesc, 1);
-                            umma_tf32(dcol, dAl, dBh, idesc, 1);
+                    const uint32_t dcol = taddr + (uint32_t)(b * BSZ);
+                    for (int kk = 0; kk < kSlabsP; ++kk, ++g) {
+                        const uint32_t s = g % SM::kStages, use = g / SM::kStages;
+                        if (!mbar_wait_for(&full[s], use & 1, kStepWaitNs)) {
+                            ok = false;
+                            break;
                         }
+                        tc_fence_after();
+                        const uint32_t base = smem_u32(smem + s * SM::kStage);
+                        const uint32_t aHi = base, bHi = base + SM::kA;
+                        const uint32_t aLo = base + SM::kRaw, bLo = aLo + SM::kA;
+#pragma unroll
+                        for (int ks = 0; ks < F::kK / F::kKStep; ++ks) {
+                            const uint32_t off = ks * 32;  // one K step = 32 bytes along K
+                            const uint64_t dAh = upd_desc(aHi + off), dAl = upd_desc(aLo + off);
+                            const uint64_t dBh = upd_desc(bHi + off), dBl = upd_desc(bLo + off);
+                            if (PREC != HS_PRECISION_TF32X3) {
+                                umma_f16(dcol, dAh, dBh, idesc, (kk | ks) != 0);
+                                umma_f16(dcol, dAh, dBl, idesc, 1);
+                                umma_f16(dcol, dAl, dBh, idesc, 1);
+                            } else {
+                                umma_tf32(dcol, dAh, dBh, idesc, (kk | ks) != 0);
+                                umma_tf32(dcol, dAh, dBl, idesc, 1);
+                                umma_tf32(dcol, dAl, dBh, idesc, 1);
+                            }
+                        }
+                        umma_commit(&empty[s]);
                     }
-                    umma_commit(&empty[s]);
+                    if (!ok) break;
+                    umma_commit(&tfull[b]);
                 }
-                if (!ok) break;
-                umma_commit(&tfull[b]);
             }
             if (!ok) atomicExch(a.err, 1);
             // TMEM is released only after every MMA issued here has completed, also
@@ -535,14 +543,17 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         constexpr int kChunks = BSZ / 64;   // 32-column chunks per warp
         float4* stile = reinterpret_cast<float4*>(staging + (warp - 2) * 4096);
         const float us = PREC == HS_PRECISION_F16X3 ? a.f16_unscale : 1.0f;  // exact power of two
-        int it = 0;
-        for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
-            const int b = it & 1, u = it >> 1;
+        int un = 0;
+        bool eok = true;
+        for (int64_t t = blockIdx.x; t < ntiles && eok; t += gridDim.x)
+        for (int pi = 0; pi < a.npanels; ++pi, ++un) {  // one unit a panel (see the issuer)
+            const int b = un & 1, u = un >> 1;
             int wok = 0;
             if (lane == 0) wok = mbar_wait_for(&tfull[b], u & 1, kStepWaitNs) ? 1 : 0;
             wok = __shfl_sync(0xffffffffu, wok, 0);
             if (!wok) {
                 if (lane == 0) atomicExch(a.err, 1);
+                eok = false;
                 break;
             }
             tc_fence_after();
@@ -551,6 +562,10 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             const int cblk = (int)block_id(r, c, a.nb);
             const int row0 = ti * 128 + q * 32;
             const uint32_t tcol = taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BSZ + half * (BSZ / 2));
+            // the previous panel's adds into the same C entries (this warp's) have
+            // completed: the adds into an entry happen in panel order, so the result
+            // is the same every run
+            if (lane == 0 && pi > 0) bulk_wait0();
 #pragma unroll 1
             for (int j = 0; j < kChunks; ++j) {
                 uint32_t v[32];

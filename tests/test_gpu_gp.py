@@ -177,7 +177,8 @@ def test_mixed_nlml_grad_against_dense(hs, ctx, N, bsz, prec):
           f"{rel_grad:.2e} normwise {rel_grad_norm:.2e} (FP64 form "
           f"{np.max(np.abs(grad64 - grad_ref) / np.abs(grad_ref)):.2e}); {rep['mixed']}")
     assert rep["mixed"]["backward_error"] <= 1e-14
-    assert rel_fit <= 1e-10
+    # alpha to ~cond(K) x 1e-14 (cond ~6e5 here; measured 8e-12 / 2.3e-10)
+    assert rel_fit <= 1e-8
     # the low-precision factor's share (measured: log|K| 2.8 nats and gradient 1.5e-2
     # normwise for the FP16 split at N = 2048, against 9e-12 and 1e-10 for the FP64 form)
     assert abs_logdet <= 2e-3 * N
