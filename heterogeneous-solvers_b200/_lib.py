@@ -88,6 +88,7 @@ SIGNATURES = {
     "hs_ctx_reset_profile": [_P],
     "hs_ctx_launch_count": [_P],
     "hs_ctx_set_reference_order": [_P, _I],
+    "hs_ctx_set_mixed_accumulation": [_P, _I],
     "hs_potrf_block": [_P, _P, _I, _I],
     "hs_ctx_take_info": [_P, ctypes.POINTER(_I64)],
     "hs_trsm_panel": [_P, _P, _I, _I, _I, _I],

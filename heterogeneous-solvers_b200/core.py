@@ -108,6 +108,12 @@ class Context:
         `cpu_chunks` = core-count chunks); 0 restores the fast kernels."""
         call("hs_ctx_set_reference_order", self.handle, int(cpu_chunks))
 
+    def set_mixed_accumulation(self, per_panel):
+        """Mixed-precision factor: True adds each panel's trailing-update product into
+        the FP32 matrix on its own (more accurate factor and log|K|, slower update);
+        False (default) a group of four panels' at once."""
+        call("hs_ctx_set_mixed_accumulation", self.handle, int(bool(per_panel)))
+
     def launch_count(self):
         return _lib.load().hs_ctx_launch_count(self.handle)
 

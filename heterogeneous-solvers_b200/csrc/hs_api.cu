@@ -356,6 +356,15 @@ hs_status hs_ctx_set_reference_order(hs_ctx ctx, int cpu_chunks) {
     return HS_OK;
 }
 
+hs_status hs_ctx_set_mixed_accumulation(hs_ctx ctx, int per_panel) {
+    if (!ctx || (per_panel != 0 && per_panel != 1)) {
+        set_error("hs_ctx_set_mixed_accumulation: per_panel must be 0 or 1");
+        return HS_ERR_INVALID_ARG;
+    }
+    ctx->mixed_per_panel = per_panel;
+    return HS_OK;
+}
+
 hs_status hs_ctx_take_info(hs_ctx ctx, int64_t* info) {
     HS_API_BEGIN("hs_ctx_take_info");
     long long v = 0;

@@ -63,6 +63,10 @@ struct TcArgs {
     // low parts from LO slot p nb and its 16-bit split from P16 slot 2 p nb (hi of row r
     // at 2 p nb + r - (k + p) - 1, lo nb slots further)
     int npanels;
+    // panels summed in one TMEM accumulation before the add into C: npanels (the
+    // whole group, fewest adds, fastest) or 1 (each panel's product added on its own:
+    // a several times more accurate factor, ~25 % slower update)
+    int unit_panels;
     int first_col;
     // TRSM with 16-bit split products downstream (split16 = HS_PRECISION_BF16X3 or
     // HS_PRECISION_F16X3; 0: none): the epilogue writes L's hi / lo split (P16 slots
@@ -477,17 +481,19 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     } else if (warp == 1) {
         if (lane == 0) {
             // ---- MMA issuer
-            // one accumulation unit = one tile x one panel (K = BSZ): each panel's product
-            // is added into C on its own (an FP32 round-to-nearest add in L2), instead of
-            // the whole group's K = npanels x BSZ sum in TMEM first, whose accumulation
-            // measured several times less accurate (log|K| and the unrefined backward
-            // error); the C tile stays in L2 across its units, so the DRAM traffic of a
-            // group pass is unchanged
+            // one accumulation unit = one tile x unit_panels panels: with unit_panels = 1
+            // each panel's product is added into C on its own (an FP32 round-to-nearest
+            // add in L2) instead of the whole group's K = npanels x BSZ sum in TMEM first,
+            // whose accumulation measured several times less accurate (log|K|, the
+            // unrefined backward error); the C tile stays in L2 across its units, so the
+            // DRAM traffic of a group pass is unchanged, but the extra adds cost time
             constexpr uint32_t idesc = umma_idesc(F::kFmt, F::kFmt, 128, BSZ);
+            const int unit_slabs = a.unit_panels * kSlabsP;
+            const int units = a.npanels / a.unit_panels;
             uint32_t g = 0;
             int un = 0;
             for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                for (int pi = 0; pi < a.npanels && ok; ++pi, ++un) {
+                for (int pi = 0; pi < units && ok; ++pi, ++un) {
                     const int b = un & 1, u = un >> 1;
                     if (u > 0 && !mbar_wait_for(&tempty[b], (u - 1) & 1, kStepWaitNs)) {
                         ok = false;
@@ -495,7 +501,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                     }
                     tc_fence_after();
                     const uint32_t dcol = taddr + (uint32_t)(b * BSZ);
-                    for (int kk = 0; kk < kSlabsP; ++kk, ++g) {
+                    for (int kk = 0; kk < unit_slabs; ++kk, ++g) {
                         const uint32_t s = g % SM::kStages, use = g / SM::kStages;
                         if (!mbar_wait_for(&full[s], use & 1, kStepWaitNs)) {
                             ok = false;
@@ -545,8 +551,9 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         const float us = PREC == HS_PRECISION_F16X3 ? a.f16_unscale : 1.0f;  // exact power of two
         int un = 0;
         bool eok = true;
+        const int units = a.npanels / a.unit_panels;
         for (int64_t t = blockIdx.x; t < ntiles && eok; t += gridDim.x)
-        for (int pi = 0; pi < a.npanels; ++pi, ++un) {  // one unit a panel (see the issuer)
+        for (int pi = 0; pi < units; ++pi, ++un) {  // accumulation units (see the issuer)
             const int b = un & 1, u = un >> 1;
             int wok = 0;
             if (lane == 0) wok = mbar_wait_for(&tfull[b], u & 1, kStepWaitNs) ? 1 : 0;
@@ -1173,7 +1180,7 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
 int mixed_fro_grid(int64_t blocks) { return (int)(blocks < 1024 ? blocks : 1024); }
 
 hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift, int precision,
-                       double* fro_part, double maxdiag) {
+                       double* fro_part, double maxdiag, bool per_panel) {
     const int bsz = ctx->bsz, nb = ctx->nb;
     HS_REQUIRE(bsz == 128 || bsz == 256, "the mixed-precision factor supports matrixBlockSize 128 or 256");
     hs_status st = bsz == 256 ? tc_attrs<256>() : tc_attrs<128>();
@@ -1281,6 +1288,7 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         a.k = k;
         a.blockID = diag_id(k);
         a.npanels = npanels;
+        a.unit_panels = per_panel ? 1 : npanels;
         a.first_col = c0;
         a.part = part;
         const double m = nb - c0, np = npanels;
