@@ -108,11 +108,11 @@ class Context:
         `cpu_chunks` = core-count chunks); 0 restores the fast kernels."""
         call("hs_ctx_set_reference_order", self.handle, int(cpu_chunks))
 
-    def set_mixed_accumulation(self, per_panel):
-        """Mixed-precision factor: True adds each panel's trailing-update product into
-        the FP32 matrix on its own (more accurate factor and log|K|, slower update);
-        False (default) a group of four panels' at once."""
-        call("hs_ctx_set_mixed_accumulation", self.handle, int(bool(per_panel)))
+    def set_mixed_accumulation(self, panels):
+        """Mixed-precision factor: the trailing-update products of `panels` (1, 2 or 4)
+        panels are summed in the tensor cores' accumulator before each add into the
+        FP32 matrix; fewer is the more accurate factor and log|K|, more adds."""
+        call("hs_ctx_set_mixed_accumulation", self.handle, int(panels))
 
     def launch_count(self):
         return _lib.load().hs_ctx_launch_count(self.handle)

@@ -356,12 +356,12 @@ hs_status hs_ctx_set_reference_order(hs_ctx ctx, int cpu_chunks) {
     return HS_OK;
 }
 
-hs_status hs_ctx_set_mixed_accumulation(hs_ctx ctx, int per_panel) {
-    if (!ctx || (per_panel != 0 && per_panel != 1)) {
-        set_error("hs_ctx_set_mixed_accumulation: per_panel must be 0 or 1");
+hs_status hs_ctx_set_mixed_accumulation(hs_ctx ctx, int panels) {
+    if (!ctx || (panels != 1 && panels != 2 && panels != 4)) {
+        set_error("hs_ctx_set_mixed_accumulation: panels must be 1, 2 or 4");
         return HS_ERR_INVALID_ARG;
     }
-    ctx->mixed_per_panel = per_panel;
+    ctx->mixed_acc_panels = panels;
     return HS_OK;
 }
 

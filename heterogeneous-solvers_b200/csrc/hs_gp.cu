@@ -329,7 +329,7 @@ static hs_status gp_nlml_grad_impl(hs_ctx ctx, const double* X, const double* y,
         copy_pad_kernel<<<64, 256, 0, s>>>(y, yb, N, n);
         HS_CHECK_LAUNCH("copy y");
         hs_mixed_report mr{};
-        // per-panel accumulation: log|K| and the trace term come from the factor itself
+        // one panel an accumulation: log|K| and the trace term come from the factor itself
         st = mixed_solve_impl(ctx, L, yb, alpha, precision, tol, 30, &mr, 1);
         if (mreport) *mreport = mr;
         if (st != HS_OK) return st;

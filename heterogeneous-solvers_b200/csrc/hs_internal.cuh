@@ -53,9 +53,10 @@ struct hs_ctx_s {
     // accumulation order (separate multiply and add, dot products in this many
     // sequential chunks) so that CG reproduces it bit for bit
     int ref_chunks = 0;
-    // mixed factor: 1 = add each panel's trailing-update product into the FP32 matrix on
-    // its own (hs_ctx_set_mixed_accumulation); 0 = a panel group's at once (default)
-    int mixed_per_panel = 0;
+    // mixed factor: panels (1, 2 or 4) whose trailing-update products are summed in the
+    // tensor cores' accumulator before one add into the FP32 matrix
+    // (hs_ctx_set_mixed_accumulation)
+    int mixed_acc_panels = 4;
 
     // kernels launched through this context (all launch sites count)
     int64_t launches = 0;

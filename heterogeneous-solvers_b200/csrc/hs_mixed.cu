@@ -155,7 +155,7 @@ struct Events {
 }  // namespace
 
 hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,
-                           int max_steps, hs_mixed_report* out, int per_panel) {
+                           int max_steps, hs_mixed_report* out, int acc_panels) {
     if (precision != HS_PRECISION_TF32X3 && precision != HS_PRECISION_BF16X3 && precision != HS_PRECISION_F16X3) {
         set_error("hs_mixed_solve: precision must be HS_PRECISION_TF32X3, HS_PRECISION_BF16X3 or HS_PRECISION_F16X3");
         return HS_ERR_UNSUPPORTED;
@@ -217,7 +217,7 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
         set_i64_dev(ctx->d_info + 1, LLONG_MIN, s);
         // the first attempt's conversion to FP32 also sums ||K||_F^2
         st = mixed_factor(ctx, K, w, s, shift, prec, attempt == 1 ? part : nullptr, have_maxdiag ? h[9] + shift : 0.0,
-                          per_panel < 0 ? ctx->mixed_per_panel != 0 : per_panel != 0);
+                          acc_panels > 0 ? acc_panels : ctx->mixed_acc_panels);
         if (st != HS_OK) return st;
         HS_CUDA(cudaStreamSynchronize(s));
         if (ctx->side) HS_CUDA(cudaStreamSynchronize(ctx->side));

@@ -34,19 +34,20 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w);
 // as mixed_fro_grid(blocks) CTA partials
 // maxdiag: the largest diagonal entry of the matrix factored (with its shift); it sets
 // the power-of-two scale of the FP16 split and is not read by the other precisions
-// per_panel: each panel's trailing-update product is added into the FP32 matrix on its
-// own instead of a whole panel group's (more accurate factor, slower update)
+// acc_panels: panels (1, 2 or 4, the panel group) whose trailing-update products are
+// summed in the tensor cores' accumulator before one add into the FP32 matrix (fewer:
+// more accurate factor, more adds)
 hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift = 0.0,
                        int precision = HS_PRECISION_TF32X3, double* fro_part = nullptr, double maxdiag = 0.0,
-                       bool per_panel = false);
+                       int acc_panels = 4);
 int mixed_fro_grid(int64_t blocks);
 hs_status mixed_check_error(hs_ctx ctx, const MixedWork& w);
 // b <- (L L^T)^-1 b with the mixed factor (tmp: intermediate)
 hs_status mixed_apply(hs_ctx ctx, MixedWork& w, double* b, double* tmp, cudaStream_t s);
 // the mixed-precision solve behind hs_mixed_solve (workspace kept by the context)
-// (per_panel < 0: the context's setting, hs_ctx_set_mixed_accumulation)
+// (acc_panels <= 0: the context's setting, hs_ctx_set_mixed_accumulation)
 hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double* x, int precision, double tol,
-                           int max_steps, hs_mixed_report* out, int per_panel = -1);
+                           int max_steps, hs_mixed_report* out, int acc_panels = 0);
 
 // TRSM of `items` bsz x bsz FP64 blocks stored contiguously at B against the
 // lower triangle L (bsz x bsz): B <- B L^-T

@@ -63,9 +63,9 @@ struct TcArgs {
     // low parts from LO slot p nb and its 16-bit split from P16 slot 2 p nb (hi of row r
     // at 2 p nb + r - (k + p) - 1, lo nb slots further)
     int npanels;
-    // panels summed in one TMEM accumulation before the add into C: npanels (the
-    // whole group, fewest adds, fastest) or 1 (each panel's product added on its own:
-    // a several times more accurate factor, ~25 % slower update)
+    // panels summed in one TMEM accumulation before the add into C (1, 2 or
+    // kPanelGroup; the last unit of a tile takes what is left of its npanels): fewer
+    // panels a unit is a more accurate factor, more adds into C
     int unit_panels;
     int first_col;
     // TRSM with 16-bit split products downstream (split16 = HS_PRECISION_BF16X3 or
@@ -488,12 +488,11 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             // unrefined backward error); the C tile stays in L2 across its units, so the
             // DRAM traffic of a group pass is unchanged, but the extra adds cost time
             constexpr uint32_t idesc = umma_idesc(F::kFmt, F::kFmt, 128, BSZ);
-            const int unit_slabs = a.unit_panels * kSlabsP;
-            const int units = a.npanels / a.unit_panels;
             uint32_t g = 0;
             int un = 0;
             for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                for (int pi = 0; pi < units && ok; ++pi, ++un) {
+                for (int p0 = 0; p0 < a.npanels && ok; p0 += a.unit_panels, ++un) {
+                    const int unit_slabs = min(a.unit_panels, a.npanels - p0) * kSlabsP;
                     const int b = un & 1, u = un >> 1;
                     if (u > 0 && !mbar_wait_for(&tempty[b], (u - 1) & 1, kStepWaitNs)) {
                         ok = false;
@@ -551,7 +550,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         const float us = PREC == HS_PRECISION_F16X3 ? a.f16_unscale : 1.0f;  // exact power of two
         int un = 0;
         bool eok = true;
-        const int units = a.npanels / a.unit_panels;
+        const int units = (a.npanels + a.unit_panels - 1) / a.unit_panels;
         for (int64_t t = blockIdx.x; t < ntiles && eok; t += gridDim.x)
         for (int pi = 0; pi < units; ++pi, ++un) {  // accumulation units (see the issuer)
             const int b = un & 1, u = un >> 1;
@@ -1180,7 +1179,8 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
 int mixed_fro_grid(int64_t blocks) { return (int)(blocks < 1024 ? blocks : 1024); }
 
 hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t s, double shift, int precision,
-                       double* fro_part, double maxdiag, bool per_panel) {
+                       double* fro_part, double maxdiag, int acc_panels) {
+    if (acc_panels != 1 && acc_panels != 2 && acc_panels != kPanelGroup) acc_panels = kPanelGroup;
     const int bsz = ctx->bsz, nb = ctx->nb;
     HS_REQUIRE(bsz == 128 || bsz == 256, "the mixed-precision factor supports matrixBlockSize 128 or 256");
     hs_status st = bsz == 256 ? tc_attrs<256>() : tc_attrs<128>();
@@ -1288,7 +1288,7 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         a.k = k;
         a.blockID = diag_id(k);
         a.npanels = npanels;
-        a.unit_panels = per_panel ? 1 : npanels;
+        a.unit_panels = acc_panels < npanels ? acc_panels : npanels;
         a.first_col = c0;
         a.part = part;
         const double m = nb - c0, np = npanels;

@@ -116,13 +116,13 @@ int64_t hs_ctx_launch_count(hs_ctx ctx);
  * far slower than the default (0: fused, tree-reduced kernels). */
 hs_status hs_ctx_set_reference_order(hs_ctx ctx, int cpu_chunks);
 
-/* Mixed-precision factor (no reference counterpart): per_panel = 1 adds each panel's
- * trailing-update product into the FP32 working matrix on its own; 0 (the default)
- * sums a group of four panels in the tensor cores' accumulator first.  Per panel is
- * the more accurate factor (log|K| error ~4x smaller, fewer refinement steps) and a
- * ~25 % slower update; hs_mixed_solve's x reaches its target either way.
- * hs_gp_nlml_grad_mixed always adds per panel. */
-hs_status hs_ctx_set_mixed_accumulation(hs_ctx ctx, int per_panel);
+/* Mixed-precision factor (no reference counterpart): `panels` (1, 2 or 4) trailing-update
+ * panel products are summed in the tensor cores' FP32 accumulator before each
+ * round-to-nearest add into the FP32 working matrix.  Fewer panels an add is the more
+ * accurate factor (one panel: log|K| error ~4-7x smaller than four, fewer refinement
+ * steps) and more adds into C (one panel: a ~25 % slower update); hs_mixed_solve's x
+ * reaches its target either way.  hs_gp_nlml_grad_mixed always uses one panel. */
+hs_status hs_ctx_set_mixed_accumulation(hs_ctx ctx, int panels);
 
 /* ------------------------------------------------------------------ operators */
 /* MatrixOperations::cholesky / cholesky_GPU / cholesky_optimizedGPU
