@@ -476,6 +476,8 @@ def gp_nlml_grad(ctx, X, y, theta, n_ell=None, precision=None, tol=1e-14):
     mixed-precision one (hs_gp_nlml_grad_mixed): alpha refined in FP64 to the
     backward error ``tol``; the report then also holds the solve's report under
     "mixed"."""
+    if precision is not None and precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
     Xd = X if isinstance(X, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(X, dtype=np.float64))
     yd = y if isinstance(y, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(y, dtype=np.float64))
     Xd = _to_device(Xd.to(torch.float64), ctx).contiguous()
@@ -495,8 +497,6 @@ def gp_nlml_grad(ctx, X, y, theta, n_ell=None, precision=None, tol=1e-14):
              th.ctypes.data_as(ctypes.c_void_p), int(n_ell), ctypes.byref(nlml),
              grad.ctypes.data_as(ctypes.c_void_p), ctypes.byref(rep))
         return nlml.value, grad, {f: getattr(rep, f) for f, _ in GpReport._fields_}
-    if precision not in PRECISIONS:
-        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
     mrep = MixedReport()
     call("hs_gp_nlml_grad_mixed", ctx.handle, _dptr(Xd, ctx), _dptr(yd, ctx), int(Xd.shape[1]),
          th.ctypes.data_as(ctypes.c_void_p), int(n_ell), int(PRECISIONS[precision]), float(tol), ctypes.byref(nlml),
