@@ -150,20 +150,24 @@ __global__ void __launch_bounds__(256, 2) chain_dmma_kernel(ChainArgs a) {
             if (nx < nk) load_stage((int)(nx % STAGES), nx);
             cp_async_commit();
         }
-        const Elem e = chain_elem(a, item, q0 + kt / spb);
+        // operand orientation of this slab's chain element (its pointers are only
+        // needed by the loads): CHAIN_SYMM takes Abar_cr^T from c = r on (q >= r - k)
+        const int64_t q = q0 + kt / spb;
+        const int eta = a.mode == CHAIN_SYMM ? (q >= item + 1) : a.ta;
+        const int etb = a.mode == CHAIN_SYMM ? 0 : a.tb;
         const double* As = smem + (int)(kt % STAGES) * kStage;
         const double* Bs = As + kStageA;
 #pragma unroll
         for (int kk = 0; kk < BK / 4; ++kk) {
             double av[4], bv[4];
-            if (!e.ta) {
+            if (!eta) {
 #pragma unroll
                 for (int mi = 0; mi < 4; ++mi) av[mi] = As[(wm * WM + mi * 8 + g) * SPAD + kk * 4 + t];
             } else {
 #pragma unroll
                 for (int mi = 0; mi < 4; ++mi) av[mi] = As[(kk * 4 + t) * LDTA + wm * WM + mi * 8 + g];
             }
-            if (!e.tb) {
+            if (!etb) {
 #pragma unroll
                 for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(kk * 4 + t) * LDTB + wn * WN + ni * 8 + g];
             } else {
