@@ -91,6 +91,17 @@ hs_status ensure_hostws(hs_ctx ctx, size_t bytes) {
     return HS_OK;
 }
 
+hs_status ensure_solvews(hs_ctx ctx, size_t bytes) {
+    if (ctx->solvews_bytes >= bytes) return HS_OK;
+    HS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->solvews) HS_CUDA(cudaFree(ctx->solvews));
+    ctx->solvews = nullptr;
+    ctx->solvews_bytes = 0;
+    HS_CUDA(cudaMalloc(&ctx->solvews, bytes));
+    ctx->solvews_bytes = bytes;
+    return HS_OK;
+}
+
 __global__ void set_i64_kernel(long long* p, long long v) { *p = v; }
 
 void set_i64_dev(long long* p, long long v, cudaStream_t s) { set_i64_kernel<<<1, 1, 0, s>>>(p, v); }
@@ -254,6 +265,7 @@ hs_status hs_ctx_destroy(hs_ctx ctx) {
     if (ctx->mixed) cudaFree(ctx->mixed);
     if (ctx->gpws) cudaFree(ctx->gpws);
     if (ctx->hostws) cudaFree(ctx->hostws);
+    if (ctx->solvews) cudaFree(ctx->solvews);
     if (ctx->d_info) cudaFree(ctx->d_info);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     delete ctx;
@@ -274,8 +286,10 @@ hs_status hs_ctx_release_buffers(hs_ctx ctx) {
     if (ctx->mixed) HS_CUDA(cudaFree(ctx->mixed));
     if (ctx->gpws) HS_CUDA(cudaFree(ctx->gpws));
     if (ctx->hostws) HS_CUDA(cudaFree(ctx->hostws));
-    ctx->scratch = ctx->work = ctx->mixed = ctx->gpws = ctx->hostws = nullptr;
+    if (ctx->solvews) HS_CUDA(cudaFree(ctx->solvews));
+    ctx->scratch = ctx->work = ctx->mixed = ctx->gpws = ctx->hostws = ctx->solvews = nullptr;
     ctx->scratch_bytes = ctx->work_bytes = ctx->mixed_bytes = ctx->gpws_bytes = ctx->hostws_bytes = 0;
+    ctx->solvews_bytes = 0;
     return HS_OK;
 }
 

@@ -35,6 +35,10 @@ struct hs_ctx_s {
     // grow-only device copies of the host-buffer GP solve (X, K, y, x)
     void* hostws = nullptr;
     size_t hostws_bytes = 0;
+    // grow-only workspace of the FP64 triangular solve (inverse diagonal blocks,
+    // intermediate vector, sweep flags)
+    void* solvews = nullptr;
+    size_t solvews_bytes = 0;
 
     // device words: [0] the smallest failing pivot row (INT64_MAX = none); [1] the
     // bit pattern of the most negative failing pivot of the mixed factor's FP64
@@ -111,6 +115,7 @@ hs_status ensure_work(hs_ctx ctx, size_t bytes);
 hs_status ensure_mixed(hs_ctx ctx, size_t bytes);
 hs_status ensure_gp(hs_ctx ctx, size_t bytes);
 hs_status ensure_hostws(hs_ctx ctx, size_t bytes);
+hs_status ensure_solvews(hs_ctx ctx, size_t bytes);
 
 // scratch layout: [0, 32 KB) reduction partials, [32 KB, 48 KB) solver scalars,
 // [56 KB, 64 KB) small constants; matvec partial blocks start at 64 KB
@@ -175,6 +180,13 @@ hs_status launch_update(hs_ctx ctx, double* A, int blockID, int blockRow, int sy
 // (SYRK on their diagonal blocks, GEMM below them)
 hs_status launch_update_cols(hs_ctx ctx, double* A, int blockID, int blockRow, int colStart, int colEnd,
                              cudaStream_t s);
+// Y_k = L_kk^-T for all nb diagonal blocks of the packed factor L (Y: nb consecutive
+// blocks; pad: one block of scratch for a last block with padding rows)
+hs_status launch_diag_inverses(hs_ctx ctx, const double* L, double* Y, double* pad, cudaStream_t s);
+// a whole forward (L^-1 in) or backward (L^-T in) sweep over the FP64 packed factor in
+// one cooperative launch, given Y_k = L_kk^-T (k_vector.cu)
+hs_status launch_sweep_whole_f64(hs_ctx ctx, const double* L, const double* Y, const double* in, double* out,
+                                 int forward, unsigned epoch, unsigned* flags, int* err, cudaStream_t s);
 // X = L^-1 (row major) of one lower-triangular bsz x bsz block; Y is a block of scratch
 hs_status launch_diag_inverse(hs_ctx ctx, const double* Lkk, double* Y, double* X, cudaStream_t s);
 // B <- B X^T in place for blockCount consecutive blocks from firstBlock (bsz 128 or 256):

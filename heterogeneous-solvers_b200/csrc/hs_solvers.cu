@@ -148,6 +148,35 @@ hs_status solve_driver(hs_ctx ctx, const double* L, double* b) {
     const int nb = ctx->nb;
     const int64_t T = total_blocks(nb);
     cudaStream_t s = ctx->stream;
+    if ((ctx->bsz == 128 || ctx->bsz == 256) && nb > 1) {
+        // both sweeps as single cooperative launches over the FP64 factor (each row
+        // reduced by one CTA in column order), with the diagonal solves as products with
+        // Y_k = L_kk^-T formed for all blocks in one batched launch first; the reference's
+        // 2 nb dependent launches a sweep are latency-bound
+        const size_t bb = (size_t)ctx->bsz * ctx->bsz;
+        const int64_t n = (int64_t)nb * ctx->bsz;
+        const size_t ybytes = ((size_t)nb * bb + bb + (size_t)n) * sizeof(double);
+        hs_status st = ensure_solvews(ctx, ybytes + 256 + (((size_t)nb * sizeof(unsigned) + 255) & ~size_t(255)));
+        if (st != HS_OK) return st;
+        double* Y = static_cast<double*>(ctx->solvews);
+        double* pad = Y + (size_t)nb * bb;
+        double* tmp = pad + bb;
+        int* err = reinterpret_cast<int*>(static_cast<char*>(ctx->solvews) + ybytes);
+        unsigned* flags = reinterpret_cast<unsigned*>(static_cast<char*>(ctx->solvews) + ybytes + 256);
+        if ((st = launch_diag_inverses(ctx, L, Y, pad, s)) != HS_OK) return st;
+        HS_CUDA(cudaMemsetAsync(flags, 0, (size_t)nb * sizeof(unsigned), s));
+        HS_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+        if ((st = launch_sweep_whole_f64(ctx, L, Y, b, tmp, 1, 1u, flags, err, s)) != HS_OK) return st;
+        if ((st = launch_sweep_whole_f64(ctx, L, Y, tmp, b, 0, 2u, flags, err, s)) != HS_OK) return st;
+        int h_err = 0;
+        HS_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        HS_CUDA(cudaStreamSynchronize(s));
+        if (h_err != 0) {
+            set_error("hs_cholesky_solve: a bounded wait of the triangular sweep ran out");
+            return HS_ERR_TIMEOUT;
+        }
+        return HS_OK;
+    }
     for (int j = 0; j < nb; ++j) {
         const int right = nb - j;
         const int blockID = (int)(T - (int64_t)right * (right + 1) / 2);

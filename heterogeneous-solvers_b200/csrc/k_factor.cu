@@ -110,6 +110,8 @@ struct TrsmArgs {
     int slabs;         // slabs per B item
     int rows_last;     // rows in each item (bsz or sub-block rows)
     int64_t block_elems;  // panel mode: stride between B blocks (elements); 0: single item at A
+    int l_diag_nb;        // > 0: item q solves against its own triangle, the diagonal block q of the
+                          // packed matrix at L with this many block columns (L = its base)
 };
 
 __global__ void __launch_bounds__(256) trsm_kernel(TrsmArgs a) {
@@ -121,6 +123,7 @@ __global__ void __launch_bounds__(256) trsm_kernel(TrsmArgs a) {
     double* Lp = Tc + kTrsmCh * (kTrsmCh + 1);        // n x (kTrsmCh+1)
     const int item = blockIdx.x / a.slabs;
     const int slab = blockIdx.x % a.slabs;
+    const double* Lt = a.l_diag_nb > 0 ? a.L + (size_t)column_start(item, a.l_diag_nb) * n * n : a.L;
     double* B = a.A + (a.block_elems ? (size_t)(a.item0 + item) * a.block_elems : 0) + (size_t)slab * kTrsmRows * a.ldB;
     const int rows = min(kTrsmRows, a.rows_last - slab * kTrsmRows);
     for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
@@ -135,11 +138,11 @@ __global__ void __launch_bounds__(256) trsm_kernel(TrsmArgs a) {
         __syncthreads();
         for (int e = threadIdx.x; e < kn * kn; e += blockDim.x) {
             const int i = e / kn, k = e % kn;
-            Tc[i * (kTrsmCh + 1) + k] = a.L[(size_t)(k0 + i) * a.ldL + (k0 + k)];
+            Tc[i * (kTrsmCh + 1) + k] = Lt[(size_t)(k0 + i) * a.ldL + (k0 + k)];
         }
         for (int e = threadIdx.x; e < rest * kn; e += blockDim.x) {
             const int i = e / kn, k = e % kn;
-            Lp[i * (kTrsmCh + 1) + k] = a.L[(size_t)(k0 + kn + i) * a.ldL + (k0 + k)];
+            Lp[i * (kTrsmCh + 1) + k] = Lt[(size_t)(k0 + kn + i) * a.ldL + (k0 + k)];
         }
         __syncthreads();
         // chunk solve: one thread per row (rows are independent)
@@ -609,6 +612,49 @@ hs_status launch_diag_inverse(hs_ctx ctx, const double* Lkk, double* Y, double* 
     ctx->launches += 1;
     transpose_block_kernel<<<dim3(n / 32, n / 32), dim3(32, 8), 0, s>>>(Y, X, n);
     HS_CHECK_LAUNCH("transpose");
+    return HS_OK;
+}
+
+__global__ void identity_blocks_kernel(double* __restrict__ Y, int n, int64_t blocks) {
+    const int64_t total = (int64_t)n * n * blocks;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t w = e % ((int64_t)n * n);
+        Y[e] = (w / n == w % n) ? 1.0 : 0.0;
+    }
+}
+
+// P = the last diagonal block with a unit diagonal on its padding rows (valid < n)
+__global__ void pad_unit_block_kernel(const double* __restrict__ D, double* __restrict__ P, int n, int valid) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * n; e += gridDim.x * blockDim.x) {
+        const int i = e / n, j = e % n;
+        P[e] = (i < valid && j < valid) ? D[e] : (i == j ? 1.0 : 0.0);
+    }
+}
+
+hs_status launch_diag_inverses(hs_ctx ctx, const double* L, double* Y, double* pad, cudaStream_t s) {
+    // Y_k = L_kk^-T for every diagonal block: the substitution kernel on identity blocks,
+    // every item against its own triangle; the last block, when it has padding rows,
+    // against a copy with a unit diagonal there (its padding rows are never used)
+    hs_status st = set_attrs();
+    if (st != HS_OK) return st;
+    const int n = ctx->bsz, nb = ctx->nb;
+    const int64_t bb = (int64_t)n * n;
+    const int valid = (int)(ctx->N - (int64_t)(nb - 1) * n);
+    ctx->launches += 1;
+    identity_blocks_kernel<<<4 * ctx->num_sms, 256, 0, s>>>(Y, n, nb);
+    HS_CHECK_LAUNCH("identity blocks");
+    const int full = valid < n ? nb - 1 : nb;
+    if (full > 0) {
+        TrsmArgs ta{L, n, n, Y, n, 0, (n + kTrsmRows - 1) / kTrsmRows, n, bb, nb};
+        if ((st = launch_trsm_args(ctx, ta, full, s)) != HS_OK) return st;
+    }
+    if (full < nb) {
+        ctx->launches += 1;
+        pad_unit_block_kernel<<<64, 256, 0, s>>>(L + (size_t)column_start(nb - 1, nb) * bb, pad, n, valid);
+        HS_CHECK_LAUNCH("pad block");
+        TrsmArgs ta{pad, n, n, Y + (size_t)(nb - 1) * bb, n, 0, (n + kTrsmRows - 1) / kTrsmRows, n, bb, 0};
+        if ((st = launch_trsm_args(ctx, ta, 1, s)) != HS_OK) return st;
+    }
     return HS_OK;
 }
 

@@ -410,9 +410,9 @@ __device__ __forceinline__ void sweep_prefetch_l2(const void* p, uint32_t bytes)
 // kSweepAhead before the diagonal, so the chain reads them from L2.
 constexpr int kSweepAhead = 4;
 
-template <int BSZ>
-__global__ void __launch_bounds__(kThreads) mixed_sweep_whole_kernel(const float* __restrict__ A,
-                                                                     const float* __restrict__ Y,
+template <int BSZ, typename T>
+__global__ void __launch_bounds__(kThreads) mixed_sweep_whole_kernel(const T* __restrict__ A,
+                                                                     const T* __restrict__ Y,
                                                                      const double* __restrict__ in,
                                                                      double* __restrict__ out, int nb, int forward,
                                                                      unsigned epoch, unsigned* __restrict__ flags,
@@ -433,11 +433,11 @@ __global__ void __launch_bounds__(kThreads) mixed_sweep_whole_kernel(const float
 
     // the owner's diagonal solve of row i (running right-hand side in wk row q)
     auto solve = [&](int i, int q) {
-        const float* Yi = Y + (size_t)i * bb;
+        const T* Yi = Y + (size_t)i * bb;
         if (forward)
-            BlockApply<BSZ, float>::run(Yi, nullptr, wk + q * BSZ, nullptr, out + (size_t)i * BSZ, 2, smem);
+            BlockApply<BSZ, T>::run(Yi, nullptr, wk + q * BSZ, nullptr, out + (size_t)i * BSZ, 2, smem);
         else
-            BlockApply<BSZ, float>::run(Yi, wk + q * BSZ, nullptr, out + (size_t)i * BSZ, nullptr, 1, smem);
+            BlockApply<BSZ, T>::run(Yi, wk + q * BSZ, nullptr, out + (size_t)i * BSZ, nullptr, 1, smem);
         __syncthreads();
         if (tid == 0) {
             __threadfence();
@@ -446,11 +446,11 @@ __global__ void __launch_bounds__(kThreads) mixed_sweep_whole_kernel(const float
     };
     // wk row q -= (block (r, cc) or its transpose) xs
     auto update = [&](int r, int cc, int q) {
-        const float* M = A + (size_t)block_id(r, cc, nb) * bb;
+        const T* M = A + (size_t)block_id(r, cc, nb) * bb;
         if (forward)
-            BlockApply<BSZ, float>::run(M, xs, nullptr, tmp, nullptr, 1, smem);
+            BlockApply<BSZ, T>::run(M, xs, nullptr, tmp, nullptr, 1, smem);
         else
-            BlockApply<BSZ, float>::run(M, nullptr, xs, nullptr, tmp, 2, smem);
+            BlockApply<BSZ, T>::run(M, nullptr, xs, nullptr, tmp, 2, smem);
         __syncthreads();
         for (int e = tid; e < BSZ; e += blockDim.x) wk[q * BSZ + e] -= tmp[e];
         __syncthreads();
@@ -515,8 +515,8 @@ __global__ void __launch_bounds__(kThreads) mixed_sweep_whole_kernel(const float
                                           : (i + kSweepAhead < nb - 1 ? i + kSweepAhead : nb - 1);
                 if (col == first) {
                     const int lr = forward ? i : i + 1, lc = lr - 1;
-                    sweep_prefetch_l2(A + (size_t)block_id(lr, lc, nb) * bb, (uint32_t)(bb * sizeof(float)));
-                    sweep_prefetch_l2(Y + (size_t)i * bb, (uint32_t)(bb * sizeof(float)));
+                    sweep_prefetch_l2(A + (size_t)block_id(lr, lc, nb) * bb, (uint32_t)(bb * sizeof(T)));
+                    sweep_prefetch_l2(Y + (size_t)i * bb, (uint32_t)(bb * sizeof(T)));
                 }
             }
         }
@@ -770,13 +770,16 @@ hs_status launch_bounded_wait_selftest(hs_ctx ctx, int64_t timeout_ns) {
     return HS_OK;
 }
 
-hs_status launch_mixed_sweep_whole(hs_ctx ctx, const float* A32, const float* Y, const double* in, double* out,
-                                   int forward, unsigned epoch, unsigned* flags, int* err, cudaStream_t s) {
+namespace {
+
+template <typename T>
+hs_status launch_sweep_whole(hs_ctx ctx, const T* A, const T* Y, const double* in, double* out, int forward,
+                             unsigned epoch, unsigned* flags, int* err, cudaStream_t s) {
     const int bsz = ctx->bsz, nb = ctx->nb;
-    HS_REQUIRE(bsz == 128 || bsz == 256, "the mixed sweep supports matrixBlockSize 128 or 256");
-    int dev = 0, per_sm = 0;
-    HS_CUDA(cudaGetDevice(&dev));
-    const void* fn = bsz == 256 ? (const void*)mixed_sweep_whole_kernel<256> : (const void*)mixed_sweep_whole_kernel<128>;
+    HS_REQUIRE(bsz == 128 || bsz == 256, "the whole-sweep solve supports matrixBlockSize 128 or 256");
+    int per_sm = 0;
+    const void* fn = bsz == 256 ? (const void*)mixed_sweep_whole_kernel<256, T>
+                                : (const void*)mixed_sweep_whole_kernel<128, T>;
     // rows per CTA for the grid used (at least one row each); shared memory for them
     auto smem_for = [&](int grid) {
         const int nown = (nb + grid - 1) / grid;
@@ -785,19 +788,30 @@ hs_status launch_mixed_sweep_whole(hs_ctx ctx, const float* A32, const float* Y,
     int grid = nb < 2 * ctx->num_sms ? nb : 2 * ctx->num_sms;
     HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem_for(grid)));
     if (grid > per_sm * ctx->num_sms) grid = per_sm * ctx->num_sms;
-    HS_REQUIRE(grid >= 1, "the mixed sweep does not fit on the device");
+    HS_REQUIRE(grid >= 1, "the whole-sweep solve does not fit on the device");
     const size_t smem = smem_for(grid);
-    HS_REQUIRE(smem <= 200 * 1024, "matrix too large for the single-launch mixed sweep");
+    HS_REQUIRE(smem <= 200 * 1024, "matrix too large for the single-launch sweep");
     if (smem > 48 * 1024) HS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    void* args[] = {(void*)&A32, (void*)&Y, (void*)&in, (void*)&out, (void*)&nb, (void*)&forward,
+    void* args[] = {(void*)&A, (void*)&Y, (void*)&in, (void*)&out, (void*)&nb, (void*)&forward,
                     (void*)&epoch, (void*)&flags, (void*)&err};
     prof_begin(ctx, s, HS_KERNEL_COLUPD);
     ctx->launches += 1;
     HS_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, s));
-    const double T = (double)nb * (nb - 1) / 2.0;
-    prof_end(ctx, s, HS_KERNEL_COLUPD, 2.0 * (T + nb) * bsz * bsz, (T * 4.0 + nb * 8.0) * bsz * bsz);
-    (void)dev;
+    const double Tb = (double)nb * (nb - 1) / 2.0;
+    prof_end(ctx, s, HS_KERNEL_COLUPD, 2.0 * (Tb + nb) * bsz * bsz, (Tb + nb) * sizeof(T) * bsz * bsz);
     return HS_OK;
+}
+
+}  // namespace
+
+hs_status launch_mixed_sweep_whole(hs_ctx ctx, const float* A32, const float* Y, const double* in, double* out,
+                                   int forward, unsigned epoch, unsigned* flags, int* err, cudaStream_t s) {
+    return launch_sweep_whole<float>(ctx, A32, Y, in, out, forward, epoch, flags, err, s);
+}
+
+hs_status launch_sweep_whole_f64(hs_ctx ctx, const double* L, const double* Y, const double* in, double* out,
+                                 int forward, unsigned epoch, unsigned* flags, int* err, cudaStream_t s) {
+    return launch_sweep_whole<double>(ctx, L, Y, in, out, forward, epoch, flags, err, s);
 }
 
 hs_status launch_column_update_f32(hs_ctx ctx, const float* A32, double* b, int blockStart, int blockCount,
