@@ -21,7 +21,7 @@ struct MixedWork {
     unsigned* flags = nullptr;  // per block row: epoch of the sweep that published it
     unsigned epoch = 0;         // last sweep launched (flags are cleared when it restarts at 0)
     float* Y32 = nullptr;       // FP32 copy of Yinv for the sweeps, in the P16 area once the factor is done
-    CUtensorMap mA128, mL128, mLB;       // 128-byte swizzle, 32-wide K boxes (TRSM)
+    CUtensorMap mA128, mL128, mL32;      // 128-byte swizzle, 32-wide K boxes of 128 / 32 rows (TRSM)
     CUtensorMap mU128, mUB, mV128, mVB;  // K boxes of 128 bytes over A32 / LO (TF32 update)
     CUtensorMap mP128, mPB;              // K boxes of 128 bytes over P16 (BF16 / FP16 update)
     CUtensorMap mC32;                    // 32x32 FP32 boxes over A32 (TMA reduce of the update's C tiles)

@@ -18,9 +18,10 @@
 //
 // Panel TRSM kernel (one 128 x bsz output tile per CTA, 4 warps):
 //   thread 0   TMA producer: A_hi, A_lo (128 x 32 FP32) and B_hi, B_lo
-//              (bsz x 32 FP32) per K slab, 128-byte swizzle, 2-stage ring
-//   thread 32  MMA issuer: 3 x 4 tcgen05.mma (K = 8 each) per slab, commit to
-//              the stage's "empty" barrier and finally to "done"
+//              (rows 32 kc .. bsz-1 x 32 FP32 of K slab kc: B = L_kk^-1 is lower
+//              triangular) per K slab, 128-byte swizzle, 2-stage ring
+//   thread 32  MMA issuer: 3 x 4 tcgen05.mma (K = 8 each, N = bsz - 32 kc) per
+//              slab, commit to the stage's "empty" barrier and finally to "done"
 //   all warps  epilogue: TMEM -> registers (warp w owns lanes 32w..32w+31 =
 //              tile rows), L = D and L_lo = D - tf32(D) or L's 16-bit split
 // The trailing update is the persistent tc_update_kernel further down.
@@ -95,6 +96,7 @@ struct TcSmem {
     static constexpr int kABytes = 128 * kSlab * 4;        // 16 KB
     static constexpr int kBBytes = BSZ * kSlab * 4;        // 16 / 32 KB
     static constexpr int kStage = 2 * kABytes + 2 * kBBytes;
+    static constexpr int kRowBox = 32 * kSlab * 4;         // 32 rows of B: 4 KB
     static constexpr int kStages = 2;
     static constexpr int kBytes = kStages * kStage + 1024 /* barriers, slot */ + 1024 /* alignment */;
 };
@@ -102,7 +104,7 @@ struct TcSmem {
 template <int BSZ, int MODE>
 __global__ void __launch_bounds__(kTcThreads, 1)
     tc_tile_kernel(const __grid_constant__ CUtensorMap mA128, const __grid_constant__ CUtensorMap mL128,
-                   const __grid_constant__ CUtensorMap mLB, TcArgs a) {
+                   const __grid_constant__ CUtensorMap mL32, TcArgs a) {
     using SM = TcSmem<BSZ>;
     if (factor_aborted(a.abort_flag)) return;
     extern __shared__ uint8_t smem_raw[];
@@ -148,17 +150,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     constexpr int kSlabs = BSZ / kSlab;
 
     if (tid == 0) {
-        // ---- producer
+        // ---- producer.  L_kk^-1 is lower triangular: the rows of B (= output
+        // columns) before 32 kc are zero in K slab kc, so only rows 32 kc .. BSZ - 1
+        // of the slab are loaded (32-row boxes, at their place in the stage)
+        constexpr int kRowBoxes = BSZ / 32;
         int issued = 0;
         for (int kc = 0; kc < kSlabs && ok; ++kc) {
             const int s = kc % SM::kStages, use = kc / SM::kStages;
             if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, deadline)) { ok = false; break; }
             uint8_t* st = smem + s * SM::kStage;
-            mbar_arrive_expect_tx(&full[s], SM::kStage);
+            mbar_arrive_expect_tx(&full[s], 2 * SM::kABytes + 2 * (kRowBoxes - kc) * SM::kRowBox);
             tma_load_3d(st, &mA128, &full[s], kc * kSlab, ti * 128, blkA);
             tma_load_3d(st + SM::kABytes, &mL128, &full[s], kc * kSlab, ti * 128, gA);
-            tma_load_3d(st + 2 * SM::kABytes, &mLB, &full[s], kc * kSlab, 0, blkB);
-            tma_load_3d(st + 2 * SM::kABytes + SM::kBBytes, &mLB, &full[s], kc * kSlab, 0, gB);
+            for (int rb = kc; rb < kRowBoxes; ++rb) {
+                tma_load_3d(st + 2 * SM::kABytes + rb * SM::kRowBox, &mL32, &full[s], kc * kSlab, 32 * rb, blkB);
+                tma_load_3d(st + 2 * SM::kABytes + SM::kBBytes + rb * SM::kRowBox, &mL32, &full[s], kc * kSlab,
+                            32 * rb, gB);
+            }
             ++issued;
         }
         if (!ok) {
@@ -171,23 +179,25 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         for (int kc = issued > SM::kStages ? issued - SM::kStages : 0; kc < issued; ++kc)
             if (!mbar_wait_for(&full[kc % SM::kStages], (kc / SM::kStages) & 1, kWaitNs)) atomicExch(a.err, 1);
     } else if (tid == 32) {
-        // ---- MMA issuer
-        constexpr uint32_t idesc = umma_idesc(kFmtTF32, kFmtTF32, 128, BSZ);
+        // ---- MMA issuer: slab kc adds into output columns 32 kc .. BSZ - 1 only
+        // (N = BSZ - 32 kc; the columns before it would get exact zeros from this slab)
         for (int kc = 0; kc < kSlabs; ++kc) {
             const int s = kc % SM::kStages, use = kc / SM::kStages;
             if (!mbar_wait(&full[s], use & 1, deadline)) { ok = false; break; }
             tc_fence_after();
+            const uint32_t idesc = umma_idesc(kFmtTF32, kFmtTF32, 128, BSZ - 32 * kc);
             const uint32_t base = smem_u32(smem + s * SM::kStage);
             const uint32_t aHi = base, aLo = base + SM::kABytes;
-            const uint32_t bHi = base + 2 * SM::kABytes, bLo = bHi + SM::kBBytes;
+            const uint32_t bHi = base + 2 * SM::kABytes + kc * SM::kRowBox, bLo = bHi + SM::kBBytes;
+            const uint32_t dcol = taddr + (uint32_t)(32 * kc);
 #pragma unroll
             for (int ks = 0; ks < kSlab / 8; ++ks) {
                 const uint32_t off = ks * 32;  // 8 TF32 = 32 bytes along K
                 const uint64_t dAh = umma_desc_sw128(aHi + off), dAl = umma_desc_sw128(aLo + off);
                 const uint64_t dBh = umma_desc_sw128(bHi + off), dBl = umma_desc_sw128(bLo + off);
-                umma_tf32(taddr, dAh, dBh, idesc, (kc | ks) != 0);
-                umma_tf32(taddr, dAh, dBl, idesc, 1);
-                umma_tf32(taddr, dAl, dBh, idesc, 1);
+                umma_tf32(dcol, dAh, dBh, idesc, (kc | ks) != 0);
+                umma_tf32(dcol, dAh, dBl, idesc, 1);
+                umma_tf32(dcol, dAl, dBh, idesc, 1);
             }
             umma_commit(&empty[s]);
         }
@@ -1071,7 +1081,7 @@ hs_status tc_launch(hs_ctx ctx, const MixedWork& w, TcArgs a, int64_t items, cud
     if (grid <= 0) return HS_OK;
     HS_REQUIRE(grid < (1LL << 31), "too many tiles");
     ctx->launches += 1;
-    tc_tile_kernel<BSZ, MODE_TRSM><<<(unsigned)grid, kTcThreads, SM::kBytes, s>>>(w.mA128, w.mL128, w.mLB, a);
+    tc_tile_kernel<BSZ, MODE_TRSM><<<(unsigned)grid, kTcThreads, SM::kBytes, s>>>(w.mA128, w.mL128, w.mL32, a);
     HS_CHECK_LAUNCH("tc_tile_kernel");
     return HS_OK;
 }
@@ -1165,7 +1175,7 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
     w->flags = reinterpret_cast<unsigned*>(p + 1024);
     hs_status st = make_map(&w->mA128, w->A32, bsz, (int64_t)T, 128);
     if (st == HS_OK) st = make_map(&w->mL128, w->LO, bsz, kPanelGroup * nb + 2, 128);
-    if (st == HS_OK) st = make_map(&w->mLB, w->LO, bsz, kPanelGroup * nb + 2, bsz);
+    if (st == HS_OK) st = make_map(&w->mL32, w->LO, bsz, kPanelGroup * nb + 2, 32);
     if (st == HS_OK) st = make_map(&w->mU128, w->A32, bsz, (int64_t)T, 128, kUpdK);
     if (st == HS_OK) st = make_map(&w->mUB, w->A32, bsz, (int64_t)T, bsz, kUpdK);
     if (st == HS_OK) st = make_map(&w->mV128, w->LO, bsz, kPanelGroup * nb + 2, 128, kUpdK);
