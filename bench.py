@@ -573,7 +573,7 @@ def main():
     launches = ctx.launch_count() - launches0
     ctx.set_profiling(False)
     t_ms = e0.elapsed_time(e1)
-    kernels = ("update", "potrf", "trsm", "assemble", "trsv", "colupd", "symv", "vector")
+    kernels = ("update", "update_side", "potrf", "trsm", "assemble", "trsv", "colupd", "symv", "vector")
     prof = {k: ctx.read_profile(k) for k in kernels}
     t_max_ms, value = replicas_throughput(torch, dist, t_ms, args.steps, world, dev)
     if world > 1:
@@ -582,6 +582,28 @@ def main():
     mixed_report = {f: getattr(mrep, f) for f, _ in hs._lib.MixedReport._fields_ if f != "reserved"}
     x_mixed = xd.clone()
     bwd_mixed = backward_error(x_mixed)
+
+    # ---------------- the same step with the look-ahead by one diagonal block only (the
+    # trailing-update launches then have every SM to themselves): step time, and the
+    # update kernel's rate per launch on the whole GPU, against the timed default
+    ahead = None
+    if not args.no_fp64:
+        ctx.set_mixed_lookahead(0, 0)
+        torch.cuda.synchronize()
+        ctx.reset_profile()
+        ctx.set_profiling(True)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        step_mixed()
+        a1.record()
+        torch.cuda.synchronize()
+        ctx.set_profiling(False)
+        ctx.set_mixed_lookahead()
+        pa = ctx.read_profile("update")
+        ahead = {"one_block_lookahead_ms_per_step": a0.elapsed_time(a1),
+                 "group_lookahead_ms_per_step": ms_per_step,
+                 "one_block_lookahead_update_tflops": pa["flops"] / (pa["ms"] * 1e-3) / 1e12 if pa["ms"] else None,
+                 "same_x": bool(torch.equal(xd, x_mixed))}
 
     # ---------------- the other split variant of the mixed form on the same system
     other = {"f16x3": "bf16x3", "bf16x3": "f16x3", "tf32x3": "f16x3"}[args.precision]
@@ -749,7 +771,12 @@ def main():
             "frac": useful / peak3 if useful else None, "traffic": traffic,
             "kernel": f"tc_update_kernel<256, {args.precision}> (split-product SYRK+GEMM trailing update, tcgen05, "
                       "persistent)",
+            "launches": "main-stream launches; while the trailing matrix is large, 16 of the SMs run the next "
+                        "panel group beside each update launch and then join it",
             "peak_source": peak_src, "tf32_gemm_peak": tf32_peak, issued_key: 3 * useful if useful else None}
+
+    if ahead and ahead["one_block_lookahead_update_tflops"]:
+        roof["frac_all_sms_one_block_lookahead"] = ahead["one_block_lookahead_update_tflops"] / peak3
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -787,6 +814,7 @@ def main():
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "phases": phases, "mixed": mixed_report, "backward_error": bwd_mixed, "fp64": fp64,
             "precision": args.precision, "other_split_variant": alt, "lml_grad": lml, "cg": cg_info,
+            "lookahead": ahead,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -62,7 +62,7 @@ class KernelProfile(ctypes.Structure):
 
 # hs_kernel_id
 KERNEL_IDS = {"update": 0, "potrf": 1, "trsm": 2, "symv": 3, "trsv": 4, "colupd": 5, "assemble": 6, "vector": 7,
-              "adjoint": 8, "grad": 9}
+              "adjoint": 8, "grad": 9, "update_side": 10}
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -89,6 +89,7 @@ SIGNATURES = {
     "hs_ctx_launch_count": [_P],
     "hs_ctx_set_reference_order": [_P, _I],
     "hs_ctx_set_mixed_accumulation": [_P, _I],
+    "hs_ctx_set_mixed_lookahead": [_P, _I, _I],
     "hs_potrf_block": [_P, _P, _I, _I],
     "hs_ctx_take_info": [_P, ctypes.POINTER(_I64)],
     "hs_trsm_panel": [_P, _P, _I, _I, _I, _I],

@@ -114,6 +114,13 @@ class Context:
         FP32 matrix; fewer is the more accurate factor and log|K|, more adds."""
         call("hs_ctx_set_mixed_accumulation", self.handle, int(panels))
 
+    def set_mixed_lookahead(self, side_sms=16, min_rows=24576):
+        """Mixed-precision factor: while at least `min_rows` rows follow the next group
+        of panels, factor that group on `side_sms` SMs beside the current group's
+        trailing update (0: look-ahead by one diagonal block).  The factor is the same
+        bit for bit either way."""
+        call("hs_ctx_set_mixed_lookahead", self.handle, int(side_sms), int(min_rows))
+
     def launch_count(self):
         return _lib.load().hs_ctx_launch_count(self.handle)
 

@@ -379,6 +379,16 @@ hs_status hs_ctx_set_mixed_accumulation(hs_ctx ctx, int panels) {
     return HS_OK;
 }
 
+hs_status hs_ctx_set_mixed_lookahead(hs_ctx ctx, int side_sms, int min_rows) {
+    if (!ctx || side_sms < 0 || side_sms > ctx->num_sms / 2 || min_rows < 0) {
+        set_error("hs_ctx_set_mixed_lookahead: side_sms must be in [0, SMs / 2] and min_rows >= 0");
+        return HS_ERR_INVALID_ARG;
+    }
+    ctx->mixed_side_sms = side_sms;
+    ctx->mixed_min_rows = min_rows;
+    return HS_OK;
+}
+
 hs_status hs_ctx_take_info(hs_ctx ctx, int64_t* info) {
     HS_API_BEGIN("hs_ctx_take_info");
     long long v = 0;

@@ -61,6 +61,11 @@ struct hs_ctx_s {
     // tensor cores' accumulator before one add into the FP32 matrix
     // (hs_ctx_set_mixed_accumulation)
     int mixed_acc_panels = 4;
+    // mixed factor: look-ahead by a panel group on this many SMs while at least
+    // mixed_min_rows rows follow the next group (hs_ctx_set_mixed_lookahead;
+    // 0 SMs: look-ahead by one diagonal block only)
+    int mixed_side_sms = 16;
+    int mixed_min_rows = 24576;
 
     // kernels launched through this context (all launch sites count)
     int64_t launches = 0;

@@ -220,7 +220,7 @@ hs_status mixed_solve_impl(hs_ctx ctx, const double* K, const double* b, double*
                           acc_panels > 0 ? acc_panels : ctx->mixed_acc_panels);
         if (st != HS_OK) return st;
         HS_CUDA(cudaStreamSynchronize(s));
-        if (ctx->side) HS_CUDA(cudaStreamSynchronize(ctx->side));
+        if (ctx->side_hi) HS_CUDA(cudaStreamSynchronize(ctx->side_hi));
         st = mixed_check_error(ctx, w);
         if (st != HS_OK) return st;
         long long piv_bits = LLONG_MIN;

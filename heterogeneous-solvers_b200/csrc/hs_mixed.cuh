@@ -12,12 +12,13 @@ namespace hs {
 // device workspace of one mixed-precision factorization
 struct MixedWork {
     float* A32 = nullptr;   // packed FP32 copy of K; its off-diagonal blocks end as L (used by the solves)
-    float* LO = nullptr;    // low parts of a panel group (panel p: slots p nb..), then L_kk^-1 hi / lo
+    float* LO = nullptr;    // low parts of two panel groups (slot set p: slots p nb..), then L_kk^-1 hi / lo
     double* Ld = nullptr;   // FP64 diagonal blocks of L (nb blocks; only the diagonal entries are written)
     double* Yinv = nullptr; // FP64 inverse diagonal blocks, Y_k = L_kk^-T (nb blocks)
     double* S = nullptr;    // FP64 scratch block (POTRF)
-    __nv_bfloat16* P16 = nullptr;  // 16-bit (BF16 or FP16) split of a panel group: panel p hi blocks 2p nb.., lo (2p+1) nb..
+    __nv_bfloat16* P16 = nullptr;  // 16-bit (BF16 or FP16) split of two panel groups: set p hi blocks 2p nb.., lo (2p+1) nb..
     int* err = nullptr;     // [0] tensor-core tile timeout, [1] triangular-sweep timeout
+    unsigned long long* tile_ctr = nullptr;  // tile counters of the trailing-update launches (zeroed per factor)
     unsigned* flags = nullptr;  // per block row: epoch of the sweep that published it
     unsigned epoch = 0;         // last sweep launched (flags are cleared when it restarts at 0)
     float* Y32 = nullptr;       // FP32 copy of Yinv for the sweeps, in the P16 area once the factor is done

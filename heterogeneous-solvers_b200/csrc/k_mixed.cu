@@ -54,15 +54,25 @@ struct TcArgs {
     int64_t blockID;   // id of the diagonal block of column k
     int k, nb;
     int* err;          // error flag (timeouts)
-    int part;          // persistent update: 0 columns first_col.., 1 column first_col only, 2 columns first_col+1..
+    // persistent update: 0 columns first_col.., 1 column first_col only, 2 columns
+    // first_col+1.., 3 columns first_col .. first_col + ncols - 1
+    int part, ncols;
+    // panel p of the update sits in slot set set0 + p (sets 0..kPanelGroup-1 and
+    // kPanelGroup..2 kPanelGroup-1 are the two banks of a group look-ahead)
+    int set0;
+    // non-null: the update's CTAs take tiles from this counter (zero before the
+    // first launch that uses it), so that a second launch can share the tiles of
+    // the first; null: CTA i takes tiles i, i + grid, ...
+    unsigned long long* tile_ctr;
     const long long* abort_flag;  // smallest failing pivot row so far (INT64_MAX: none)
     // slots (bsz x bsz blocks): FP32 low parts of panel k in LO from lo_base (row r at
     // lo_base + r - k - 1), L_kk^-1 hi / lo at LO[inv], LO[inv + 1]
     int lo_base, inv;
     // persistent update with the npanels (1..kPanelGroup) consecutive panel columns
     // k + p, updating the trailing columns from first_col on.  Panel p keeps its FP32
-    // low parts from LO slot p nb and its 16-bit split from P16 slot 2 p nb (hi of row r
-    // at 2 p nb + r - (k + p) - 1, lo nb slots further)
+    // low parts from LO slot (set0 + p) nb and its 16-bit split from P16 slot
+    // 2 (set0 + p) nb (hi of row r at 2 (set0 + p) nb + r - (k + p) - 1, lo nb slots
+    // further)
     int npanels;
     // panels summed in one TMEM accumulation before the add into C (1, 2 or
     // kPanelGroup; the last unit of a tile takes what is left of its npanels): fewer
@@ -314,6 +324,11 @@ constexpr int kUpdK = 32;
 // plausibly from the longer FP32 accumulation chains in TMEM before each
 // round-to-nearest add into C — and the solve no faster.)
 constexpr int kPanelGroup = 4;
+// panel slot sets: two banks of kPanelGroup, so that the next group's panels can be
+// factored while the trailing update still reads the current group's
+constexpr int kSets = 2 * kPanelGroup;
+// tile counters of one factor: one per look-ahead by a group (a shared update)
+__host__ __device__ constexpr int64_t tile_counters(int64_t nb) { return nb / kPanelGroup + 2; }
 constexpr uint64_t kStepWaitNs = 2000000000ull;
 
 // operand formats of the update: TF32 (FP32 storage, hi = the FP32 value as
@@ -352,6 +367,54 @@ __device__ __forceinline__ uint64_t upd_desc(uint32_t addr) {
 
 __host__ __device__ __forceinline__ int64_t tri64(int64_t n) { return n * (n + 1) / 2; }
 
+// Tile hand-off inside a CTA of the persistent update.  The producer takes the
+// CTA's j-th tile (from the shared counter, or by stride) and publishes it in slot
+// j % kRing as ((j + 1) << 32) | tile with a release store (kNoTile: no tiles
+// left); the MMA issuer and the epilogue warps read it with acquire loads.  A slot
+// is rewritten only after every reader is past its previous tile: the producer
+// publishes tile j after the empty-barrier waits of tile j - 1, so the issuer has
+// consumed every slab of tile j - 2 (a tile has >= kStages slabs), and before it
+// began tile j - 2 the epilogue had released the accumulator of tile j - 4.
+constexpr int kRing = 8;
+constexpr uint32_t kNoTile = 0xffffffffu;
+
+__device__ __forceinline__ void ring_publish(uint64_t* slot, uint32_t j, uint32_t tile) {
+    const uint64_t v = ((uint64_t)(j + 1) << 32) | tile;
+    asm volatile("st.release.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(slot)), "l"(v) : "memory");
+}
+
+// tile j of this CTA; kNoTile when none is left, or when the wait ran out (then
+// *ok = false)
+__device__ __forceinline__ uint32_t ring_take(const uint64_t* slot, uint32_t j, uint64_t timeout_ns, bool* ok) {
+    const uint64_t want = (uint64_t)j + 1;
+    uint64_t deadline = 0;
+    for (;;) {
+        uint64_t v;
+        asm volatile("ld.acquire.cta.shared::cta.b64 %0, [%1];" : "=l"(v) : "r"(smem_u32(slot)) : "memory");
+        if ((v >> 32) == want) return (uint32_t)v;
+        if ((v >> 32) > want) break;  // overwritten before it was read: cannot happen (see above)
+        const uint64_t now = globaltimer_ns();
+        if (deadline == 0)
+            deadline = now + timeout_ns;
+        else if (now > deadline)
+            break;
+    }
+    *ok = false;
+    return kNoTile;
+}
+
+// tiles of the persistent update (128 x BSZ each, BSZ / 128 per block) for a part
+__host__ __device__ __forceinline__ int64_t update_tiles(int part, int m, int ncols, int tiles_per_block) {
+    int64_t blocks;
+    if (part == 1)
+        blocks = m;
+    else if (part == 3)
+        blocks = (int64_t)ncols * m - (int64_t)ncols * (ncols - 1) / 2;
+    else
+        blocks = tri64(part == 2 ? m - 1 : m);
+    return blocks * tiles_per_block;
+}
+
 // pair p of the grouped enumeration of the m x m lower triangle -> (r', c')
 __device__ __forceinline__ void grouped_pair(int64_t p, int m, int* rr, int* cc) {
     int lo = 0, hi = (m + kGroup - 1) / kGroup;
@@ -388,6 +451,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     if (factor_aborted(a.abort_flag)) return;
     constexpr int kTiles = BSZ / 128;
     constexpr int kSlabsP = BSZ / F::kK;  // slabs per panel
+    static_assert(kSlabsP >= SM::kStages, "a tile needs at least kStages slabs (tile hand-off)");
     const int kSlabs = a.npanels * kSlabsP;
     constexpr uint32_t kAccCols = 2 * BSZ;  // two accumulators
     extern __shared__ uint8_t smem_raw[];
@@ -399,13 +463,15 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
     uint64_t* tempty = tfull + 2;
     uint64_t* drained = tempty + 2;  // every MMA of the issuer has completed
     uint32_t* tslot = reinterpret_cast<uint32_t*>(drained + 1);
+    uint64_t* ring = drained + 2;    // kRing tile slots (after tslot's 8 bytes)
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m = a.nb - a.first_col;
     // part 1: the m blocks of column first_col; part 2: the lower triangle of the
-    // columns after it; part 0: both (the m x m lower triangle from first_col on)
+    // columns after it; part 0: both (the m x m lower triangle from first_col on);
+    // part 3: the blocks of columns first_col .. first_col + ncols - 1
     const int mt = a.part == 2 ? m - 1 : m;
-    const int64_t ntiles = (a.part == 1 ? (int64_t)m : tri64(mt)) * kTiles;
+    const int64_t ntiles = update_tiles(a.part, m, a.ncols, kTiles);
 
     if (tid == 0) {
         for (int s = 0; s < SM::kStages; ++s) {
@@ -417,6 +483,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             mbar_init(&tempty[b], 8);
         }
         mbar_init(drained, 1);
+        for (int i = 0; i < kRing; ++i) ring[i] = 0;
         fence_barrier_init();
     }
     if (warp == 0) {
@@ -437,6 +504,17 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             *c = a.first_col;
             return;
         }
+        if (a.part == 3) {  // column j of the part holds m - j blocks
+            int j = 0;
+            int64_t q = p;
+            while (j + 1 < a.ncols && q >= m - j) {
+                q -= m - j;
+                ++j;
+            }
+            *r = a.first_col + j + (int)q;
+            *c = a.first_col + j;
+            return;
+        }
         int rr, cc;
         grouped_pair(p, mt, &rr, &cc);
         const int base = a.first_col + (a.part == 2 ? 1 : 0);
@@ -448,7 +526,14 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         if (lane == 0) {
             // ---- producer
             uint32_t g = 0;
-            for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+            for (uint32_t j = 0;; ++j) {
+                int64_t t = kNoTile;
+                if (ok) {
+                    t = a.tile_ctr ? (int64_t)atomicAdd(a.tile_ctr, 1ull) : blockIdx.x + (int64_t)j * gridDim.x;
+                    if (t >= ntiles) t = kNoTile;
+                }
+                ring_publish(&ring[j % kRing], j, (uint32_t)t);
+                if (t == kNoTile) break;
                 int r, c, ti;
                 decode(t, &r, &c, &ti);
                 // the tile's 128 rows of C are contiguous: bring them into L2 now, so
@@ -468,7 +553,7 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                     const int colp = a.k + pi;
                     const int gA = r - colp - 1, gB = c - colp - 1;
                     const int64_t dblk = block_id(colp, colp, a.nb);
-                    const int lob = pi * a.nb, pb = 2 * pi * a.nb;
+                    const int lob = (a.set0 + pi) * a.nb, pb = 2 * (a.set0 + pi) * a.nb;
                     const int hiA = bf ? pb + gA : (int)(dblk + (r - colp));
                     const int loA = bf ? pb + a.nb + gA : lob + gA;
                     const int hiB = bf ? pb + gB : (int)(dblk + (c - colp));
@@ -500,7 +585,8 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
             constexpr uint32_t idesc = umma_idesc(F::kFmt, F::kFmt, 128, BSZ);
             uint32_t g = 0;
             int un = 0;
-            for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+            for (uint32_t j = 0; ok; ++j) {
+                if (ring_take(&ring[j % kRing], j, kStepWaitNs, &ok) == kNoTile) break;
                 for (int p0 = 0; p0 < a.npanels && ok; p0 += a.unit_panels, ++un) {
                     const int unit_slabs = min(a.unit_panels, a.npanels - p0) * kSlabsP;
                     const int b = un & 1, u = un >> 1;
@@ -561,49 +647,63 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         int un = 0;
         bool eok = true;
         const int units = (a.npanels + a.unit_panels - 1) / a.unit_panels;
-        for (int64_t t = blockIdx.x; t < ntiles && eok; t += gridDim.x)
-        for (int pi = 0; pi < units; ++pi, ++un) {  // accumulation units (see the issuer)
-            const int b = un & 1, u = un >> 1;
-            int wok = 0;
-            if (lane == 0) wok = mbar_wait_for(&tfull[b], u & 1, kStepWaitNs) ? 1 : 0;
-            wok = __shfl_sync(0xffffffffu, wok, 0);
-            if (!wok) {
+        for (uint32_t jt = 0; eok; ++jt) {
+            uint32_t t = kNoTile;
+            int rok = 1;
+            if (lane == 0) {
+                bool tok = true;
+                t = ring_take(&ring[jt % kRing], jt, kStepWaitNs, &tok);
+                rok = tok ? 1 : 0;
+            }
+            t = __shfl_sync(0xffffffffu, t, 0);
+            if (!__shfl_sync(0xffffffffu, rok, 0)) {
                 if (lane == 0) atomicExch(a.err, 1);
-                eok = false;
                 break;
             }
-            tc_fence_after();
-            int r, c, ti;
-            decode(t, &r, &c, &ti);
-            const int cblk = (int)block_id(r, c, a.nb);
-            const int row0 = ti * 128 + q * 32;
-            const uint32_t tcol = taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BSZ + half * (BSZ / 2));
-            // the previous panel's adds into the same C entries (this warp's) have
-            // completed: the adds into an entry happen in panel order, so the result
-            // is the same every run
-            if (lane == 0 && pi > 0) bulk_wait0();
-#pragma unroll 1
-            for (int j = 0; j < kChunks; ++j) {
-                uint32_t v[32];
-                tmem_ld_32x32b_x32(tcol + (uint32_t)(j * 32), v);
-                tmem_ld_wait();
-                if (lane == 0) bulk_wait_read0();  // the previous chunk's reduce has read the tile
-                __syncwarp();
-#pragma unroll
-                for (int e = 0; e < 8; ++e)
-                    stile[lane * 8 + (e ^ (lane & 7))] =
-                        make_float4(-us * __uint_as_float(v[4 * e + 0]), -us * __uint_as_float(v[4 * e + 1]),
-                                    -us * __uint_as_float(v[4 * e + 2]), -us * __uint_as_float(v[4 * e + 3]));
-                fence_proxy_async_smem();
-                __syncwarp();
-                if (lane == 0) {
-                    tma_reduce_add_3d(&mC32, stile, half * (BSZ / 2) + j * 32, row0, cblk);
-                    bulk_commit();
+            if (t == kNoTile) break;
+            for (int pi = 0; pi < units; ++pi, ++un) {  // accumulation units (see the issuer)
+                const int b = un & 1, u = un >> 1;
+                int wok = 0;
+                if (lane == 0) wok = mbar_wait_for(&tfull[b], u & 1, kStepWaitNs) ? 1 : 0;
+                wok = __shfl_sync(0xffffffffu, wok, 0);
+                if (!wok) {
+                    if (lane == 0) atomicExch(a.err, 1);
+                    eok = false;
+                    break;
                 }
+                tc_fence_after();
+                int r, c, ti;
+                decode(t, &r, &c, &ti);
+                const int cblk = (int)block_id(r, c, a.nb);
+                const int row0 = ti * 128 + q * 32;
+                const uint32_t tcol = taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BSZ + half * (BSZ / 2));
+                // the previous panel's adds into the same C entries (this warp's) have
+                // completed: the adds into an entry happen in panel order, so the result
+                // is the same every run
+                if (lane == 0 && pi > 0) bulk_wait0();
+#pragma unroll 1
+                for (int j = 0; j < kChunks; ++j) {
+                    uint32_t v[32];
+                    tmem_ld_32x32b_x32(tcol + (uint32_t)(j * 32), v);
+                    tmem_ld_wait();
+                    if (lane == 0) bulk_wait_read0();  // the previous chunk's reduce has read the tile
+                    __syncwarp();
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        stile[lane * 8 + (e ^ (lane & 7))] =
+                            make_float4(-us * __uint_as_float(v[4 * e + 0]), -us * __uint_as_float(v[4 * e + 1]),
+                                        -us * __uint_as_float(v[4 * e + 2]), -us * __uint_as_float(v[4 * e + 3]));
+                    fence_proxy_async_smem();
+                    __syncwarp();
+                    if (lane == 0) {
+                        tma_reduce_add_3d(&mC32, stile, half * (BSZ / 2) + j * 32, row0, cblk);
+                        bulk_commit();
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[b]);
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&tempty[b]);
         }
     }
     if (warp >= 2 && lane == 0) bulk_wait0();  // every reduce into C has completed
@@ -1091,8 +1191,10 @@ hs_status tc_update_launch(hs_ctx ctx, const MixedWork& w, const TcArgs& a, int 
                            int max_ctas) {
     using SM = UpdSmem<BSZ>;
     const int m = a.nb - a.first_col;
-    const int64_t ntiles = (a.part == 1 ? (int64_t)m : tri64(a.part == 2 ? m - 1 : m)) * (BSZ / 128);
+    const int64_t ntiles = update_tiles(a.part, m, a.ncols, BSZ / 128);
     if (ntiles <= 0) return HS_OK;
+    HS_REQUIRE(ntiles < (int64_t)kNoTile, "too many update tiles");
+    HS_REQUIRE(a.part != 3 || (a.ncols >= 1 && a.ncols <= m), "update columns outside the trailing matrix");
     const int grid = (int)(ntiles < max_ctas ? ntiles : max_ctas);
     ctx->launches += 1;
     if (precision == HS_PRECISION_BF16X3)
@@ -1144,12 +1246,13 @@ size_t mixed_workspace_bytes(int64_t N, int bsz) {
     const size_t T = (size_t)(nb * (nb + 1) / 2);
     size_t bytes = 0;
     bytes += T * bb * 4;                 // A32 / L32
-    bytes += (size_t)(kPanelGroup * nb + 2) * bb * 4;  // LO: a group's low parts + L_kk^-1 hi / lo
+    bytes += (size_t)(kSets * nb + 2) * bb * 4;  // LO: two groups' low parts + L_kk^-1 hi / lo
     bytes += (size_t)nb * bb * 8;        // Ldiag64
     bytes += (size_t)nb * bb * 8;        // Yinv
-    bytes += (size_t)2 * kPanelGroup * nb * bb * 2;  // 16-bit split of a group's panels (hi / lo each)
+    bytes += (size_t)2 * kSets * nb * bb * 2;  // 16-bit split of two groups' panels (hi / lo each)
     bytes += bb * 8;                     // S
     bytes += 1024;                       // error flags
+    bytes += ((size_t)tile_counters(nb) * 8 + 255) & ~size_t(255);  // tile counters of the updates
     bytes += ((size_t)nb * 4 + 255) & ~size_t(255);  // sweep publication flags
     return bytes;
 }
@@ -1162,27 +1265,30 @@ hs_status mixed_bind(hs_ctx ctx, void* ws, MixedWork* w) {
     w->A32 = reinterpret_cast<float*>(p);
     p += T * bb * 4;
     w->LO = reinterpret_cast<float*>(p);
-    p += (size_t)(kPanelGroup * nb + 2) * bb * 4;
+    p += (size_t)(kSets * nb + 2) * bb * 4;
     w->Ld = reinterpret_cast<double*>(p);
     p += (size_t)nb * bb * 8;
     w->Yinv = reinterpret_cast<double*>(p);
     p += (size_t)nb * bb * 8;
     w->P16 = reinterpret_cast<__nv_bfloat16*>(p);
-    p += (size_t)2 * kPanelGroup * nb * bb * 2;
+    p += (size_t)2 * kSets * nb * bb * 2;
     w->S = reinterpret_cast<double*>(p);
     p += bb * 8;
     w->err = reinterpret_cast<int*>(p);
-    w->flags = reinterpret_cast<unsigned*>(p + 1024);
+    p += 1024;
+    w->tile_ctr = reinterpret_cast<unsigned long long*>(p);
+    p += ((size_t)tile_counters(nb) * 8 + 255) & ~size_t(255);
+    w->flags = reinterpret_cast<unsigned*>(p);
     hs_status st = make_map(&w->mA128, w->A32, bsz, (int64_t)T, 128);
-    if (st == HS_OK) st = make_map(&w->mL128, w->LO, bsz, kPanelGroup * nb + 2, 128);
-    if (st == HS_OK) st = make_map(&w->mL32, w->LO, bsz, kPanelGroup * nb + 2, 32);
+    if (st == HS_OK) st = make_map(&w->mL128, w->LO, bsz, kSets * nb + 2, 128);
+    if (st == HS_OK) st = make_map(&w->mL32, w->LO, bsz, kSets * nb + 2, 32);
     if (st == HS_OK) st = make_map(&w->mU128, w->A32, bsz, (int64_t)T, 128, kUpdK);
     if (st == HS_OK) st = make_map(&w->mUB, w->A32, bsz, (int64_t)T, bsz, kUpdK);
-    if (st == HS_OK) st = make_map(&w->mV128, w->LO, bsz, kPanelGroup * nb + 2, 128, kUpdK);
-    if (st == HS_OK) st = make_map(&w->mVB, w->LO, bsz, kPanelGroup * nb + 2, bsz, kUpdK);
+    if (st == HS_OK) st = make_map(&w->mV128, w->LO, bsz, kSets * nb + 2, 128, kUpdK);
+    if (st == HS_OK) st = make_map(&w->mVB, w->LO, bsz, kSets * nb + 2, bsz, kUpdK);
     if (st == HS_OK) st = make_map(&w->mC32, w->A32, bsz, (int64_t)T, 32, 32);
-    if (st == HS_OK) st = make_map(&w->mP128, w->P16, bsz, 2 * kPanelGroup * (int64_t)nb, 128, 2 * kUpdK, 2);
-    if (st == HS_OK) st = make_map(&w->mPB, w->P16, bsz, 2 * kPanelGroup * (int64_t)nb, bsz, 2 * kUpdK, 2);
+    if (st == HS_OK) st = make_map(&w->mP128, w->P16, bsz, 2 * kSets * (int64_t)nb, 128, 2 * kUpdK, 2);
+    if (st == HS_OK) st = make_map(&w->mPB, w->P16, bsz, 2 * kSets * (int64_t)nb, bsz, 2 * kUpdK, 2);
     return st;
 }
 
@@ -1199,6 +1305,7 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
     const int64_t T = total_blocks(nb);
     ctx->launches += 2;
     set_int_kernel<<<1, 1, 0, s>>>(w.err, 0);
+    HS_CUDA(cudaMemsetAsync(w.tile_ctr, 0, (size_t)tile_counters(nb) * sizeof(unsigned long long), s));
     if (fro_part && bsz % 2 == 0)
         f64_to_f32_fro2_kernel<<<mixed_fro_grid(T), 256, 0, s>>>(K64, w.A32, bsz, nb, T, fro_part);
     else
@@ -1217,7 +1324,7 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         float* dblk = w.A32 + (size_t)id * bb;
         const int64_t rem = ctx->N - (int64_t)k * bsz;
         const int valid = rem < bsz ? (int)rem : bsz;
-        float* invHi = w.LO + (size_t)kPanelGroup * nb * bb;
+        float* invHi = w.LO + (size_t)kSets * nb * bb;
         prof_begin(ctx, st_, HS_KERNEL_POTRF);
         ctx->launches += 1;
         if (bsz == 256)
@@ -1237,12 +1344,24 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
     // after a group are updated with all of its panels at once (K = g bsz per pass
     // over C), which divides the read-modify-write traffic on the trailing matrix by
     // g.  Inside a group, column k+i+1 is brought up to date with panels k..k+i just
-    // before its diagonal chain and panel.  Panel k+i keeps its low parts in slot set
-    // i.  Lookahead: the update after a group runs in two launches, its first column
-    // first; the diagonal chain of that column then runs on the side stream, on SMs
-    // the second (larger) launch leaves free.
-    const bool lookahead = ctx->side != nullptr && ctx->num_sms > 8;
+    // before its diagonal chain and panel.  Panel k+i keeps its low parts and 16-bit
+    // split in slot set kPanelGroup bank + i; consecutive groups alternate banks.
+    // Look-ahead by a group, while the trailing matrix is large: the update after a
+    // group first brings the next group's columns up to date (part 3); the next
+    // group's chains, panels and inner updates then run on the high-priority side
+    // stream, on the side_sms SMs that the update of the remaining columns (part 0)
+    // leaves free, and once they are done a second launch of that update joins on
+    // those SMs, taking tiles from the same counter.  Near the end, with too little
+    // update left to hide a group behind, the look-ahead is by one diagonal chain: the
+    // update runs as part 1 (the next column) and part 2 (the rest), with that
+    // column's chain on the side stream beside part 2.  Both orders add the same
+    // products into every block in the same sequence.
+    cudaStream_t sd = ctx->side_hi;
+    const bool lookahead = sd != nullptr && ctx->num_sms > 8;
     const int kFree = 2;
+    const int side_sms = ctx->mixed_side_sms < ctx->num_sms / 2 ? ctx->mixed_side_sms : ctx->num_sms / 2;
+    const bool group_ahead = lookahead && side_sms > 0;
+    int next_ctr = 0;  // tile counters used so far (one per group look-ahead)
     const double n3 = (double)bsz * bb;
     auto diag_id = [&](int k) { return T - (int64_t)(nb - k) * (nb - k + 1) / 2; };
     TcArgs base{};
@@ -1251,7 +1370,7 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
     base.nb = nb;
     base.err = w.err;
     base.abort_flag = ctx->d_info;
-    base.inv = kPanelGroup * nb;
+    base.inv = kSets * nb;
     // FP16 split: scale s = 2^e, the largest e with s sqrt(maxdiag) <= 2^15.  Every
     // |L_ij| <= sqrt(K_ii) <= sqrt(maxdiag), so s L stays below 2^15 (FP16 holds up to
     // 65504), and entries small enough to reach FP16's subnormal range carry an absolute
@@ -1270,12 +1389,12 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
     }
     // blocks k+1..nb-1 of column k: FP32 low parts into set `set`, TRSM-as-GEMM with
     // L_kk^-T (writes L and its low part), and for BF16 / FP16 the split of L into P16
-    auto panel = [&](int k, int set) -> hs_status {
+    auto panel = [&](int k, int set, cudaStream_t st_) -> hs_status {
         const int64_t blockID = diag_id(k);
         float* dblk = w.A32 + (size_t)blockID * bb;
         const int m = nb - k - 1;
         ctx->launches += 1;
-        lo_part_kernel<<<grid_for_elems((int64_t)m * bb / 4, ctx->num_sms), 256, 0, s>>>(
+        lo_part_kernel<<<grid_for_elems((int64_t)m * bb / 4, ctx->num_sms), 256, 0, st_>>>(
             dblk + bb, w.LO + (size_t)set * nb * bb, (int64_t)m * bb / 4);
         HS_CHECK_LAUNCH("lo_part");
         TcArgs a = base;
@@ -1285,15 +1404,17 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         // 16-bit products downstream: the TRSM writes L's 16-bit split itself
         a.split16 = (precision == HS_PRECISION_BF16X3 || precision == HS_PRECISION_F16X3) ? precision : 0;
         a.P16 = w.P16;
-        prof_begin(ctx, s, HS_KERNEL_TRSM);
-        hs_status r = bsz == 256 ? tc_launch<256>(ctx, w, a, m, s) : tc_launch<128>(ctx, w, a, m, s);
+        prof_begin(ctx, st_, HS_KERNEL_TRSM);
+        hs_status r = bsz == 256 ? tc_launch<256>(ctx, w, a, m, st_) : tc_launch<128>(ctx, w, a, m, st_);
         if (r != HS_OK) return r;
-        prof_end(ctx, s, HS_KERNEL_TRSM, (double)m * 2.0 * bsz * bb, 4.0 * m * bb * 4.0);
+        prof_end(ctx, st_, HS_KERNEL_TRSM, (double)m * 2.0 * bsz * bb, 4.0 * m * bb * 4.0);
         return HS_OK;
     };
-    // trailing update with panels k .. k + npanels - 1: part 1 = column c0, part 2 =
-    // the columns after it
-    auto update = [&](int k, int npanels, int c0, int part, int cap) -> hs_status {
+    // trailing update with panels k .. k + npanels - 1 (slot sets set0 ..) of the
+    // columns from c0 on: part 1 = column c0, part 2 = the columns after it, part 0 =
+    // both, part 3 = columns c0 .. c0 + ncols - 1.  ctr >= 0: tiles from that counter.
+    auto update = [&](int k, int npanels, int c0, int part, int ncols, int set0, cudaStream_t st_, int cap,
+                      int ctr) -> hs_status {
         TcArgs a = base;
         a.k = k;
         a.blockID = diag_id(k);
@@ -1301,51 +1422,84 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
         a.unit_panels = acc_panels < npanels ? acc_panels : npanels;
         a.first_col = c0;
         a.part = part;
-        const double m = nb - c0, np = npanels;
-        double flops, bytes;
-        if (part == 1) {
-            flops = np * ((m - 1.0) * 2.0 * n3 + (double)bsz * bsz * (bsz + 1.0));
-            bytes = (m * 2.0 + 2.0 * np * (m + 1.0)) * bb * 4.0;
-        } else {
-            const double gp = (m - 1.0) * (m - 2.0) / 2.0;
-            flops = np * (gp * 2.0 * n3 + (m - 1.0) * bsz * bsz * (bsz + 1.0));
-            bytes = ((gp + m - 1.0) * 2.0 + 2.0 * np * m) * bb * 4.0;
-        }
-        prof_begin(ctx, s, HS_KERNEL_UPDATE);
-        hs_status r = bsz == 256 ? tc_update_launch<256>(ctx, w, a, precision, s, cap)
-                                 : tc_update_launch<128>(ctx, w, a, precision, s, cap);
+        a.ncols = ncols;
+        a.set0 = set0;
+        a.tile_ctr = ctr >= 0 ? w.tile_ctr + ctr : nullptr;
+        // the part's columns hold hi, hi - 1, ..., lo blocks (diagonal block included)
+        const int m = nb - c0;
+        const int hi = part == 2 ? m - 1 : m;
+        const int lo = part == 1 ? m : (part == 3 ? m - ncols + 1 : 1);
+        const double cols = hi - lo + 1.0, blocks = cols * (hi + lo) / 2.0, np = npanels;
+        // the second launch of a shared update: its tiles are counted with the first
+        const bool joining = st_ != s && ctr >= 0;
+        const double flops = joining ? 0.0 : np * ((blocks - cols) * 2.0 * n3 + cols * bsz * bsz * (bsz + 1.0));
+        const double bytes = joining ? 0.0 : (blocks * 2.0 + 2.0 * np * m) * bb * 4.0;
+        const int pk = st_ == s ? HS_KERNEL_UPDATE : HS_KERNEL_UPDATE_SIDE;
+        prof_begin(ctx, st_, pk);
+        hs_status r = bsz == 256 ? tc_update_launch<256>(ctx, w, a, precision, st_, cap)
+                                 : tc_update_launch<128>(ctx, w, a, precision, st_, cap);
         if (r != HS_OK) return r;
-        prof_end(ctx, s, HS_KERNEL_UPDATE, flops, bytes);
+        prof_end(ctx, st_, pk, flops, bytes);
+        return HS_OK;
+    };
+    // panels k .. k+g-1 of a group whose first diagonal block is factored, with the
+    // updates and chains between them
+    auto in_group = [&](int k, int g, int bank, cudaStream_t st_, int cap) -> hs_status {
+        hs_status r;
+        for (int i = 0; i < g; ++i) {
+            if ((r = panel(k + i, kPanelGroup * bank + i, st_)) != HS_OK) return r;
+            if (i + 1 < g) {
+                if ((r = update(k, i + 1, k + i + 1, 1, 1, kPanelGroup * bank, st_, cap, -1)) != HS_OK) return r;
+                if ((r = diag_chain(k + i + 1, st_)) != HS_OK) return r;
+            }
+        }
         return HS_OK;
     };
     if ((st = diag_chain(0, s)) != HS_OK) return st;
-    for (int k = 0; k < nb - 1; k += kPanelGroup) {
+    bool ready = false;  // the group at k has been factored ahead
+    for (int k = 0, bank = 0; k < nb - 1; bank ^= 1) {
         // precondition: column k has seen every panel before it and its diagonal
         // block is factored
         const int g = kPanelGroup < nb - 1 - k ? kPanelGroup : nb - 1 - k;
-        for (int i = 0; i < g; ++i) {
-            if ((st = panel(k + i, i)) != HS_OK) return st;
-            if (i + 1 < g) {
-                if ((st = update(k, i + 1, k + i + 1, 1, ctx->num_sms)) != HS_OK) return st;
-                if ((st = diag_chain(k + i + 1, s)) != HS_OK) return st;
-            }
-        }
+        const int set0 = kPanelGroup * bank;
+        if (!ready && (st = in_group(k, g, bank, s, ctx->num_sms)) != HS_OK) return st;
         const int c0 = k + g;
-        if ((st = update(k, g, c0, 1, ctx->num_sms)) != HS_OK) return st;
-        const bool more = c0 + 1 < nb;  // columns after c0
-        const bool side = lookahead && more;
-        if (side) {
+        const int g2 = c0 < nb - 1 ? (kPanelGroup < nb - 1 - c0 ? kPanelGroup : nb - 1 - c0) : 0;
+        const int64_t rest_rows = ctx->N - (int64_t)(c0 + g2) * bsz;  // rows after the next group
+        if (group_ahead && g2 > 0 && rest_rows >= ctx->mixed_min_rows) {
+            HS_REQUIRE(next_ctr < tile_counters(nb), "tile counters exhausted");
+            if ((st = update(k, g, c0, 3, g2, set0, s, ctx->num_sms, -1)) != HS_OK) return st;
             HS_CUDA(cudaEventRecord(ctx->ev_a, s));
-            HS_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_a, 0));
-            if ((st = diag_chain(c0, ctx->side)) != HS_OK) return st;
-            HS_CUDA(cudaEventRecord(ctx->ev_b, ctx->side));
-        }
-        if (more && (st = update(k, g, c0, 2, side ? ctx->num_sms - kFree : ctx->num_sms)) != HS_OK) return st;
-        if (side) {
+            HS_CUDA(cudaStreamWaitEvent(sd, ctx->ev_a, 0));
+            if ((st = diag_chain(c0, sd)) != HS_OK) return st;
+            if ((st = in_group(c0, g2, bank ^ 1, sd, side_sms)) != HS_OK) return st;
+            const int ctr = next_ctr++;
+            if ((st = update(k, g, c0 + g2, 0, 0, set0, s, ctx->num_sms - side_sms, ctr)) != HS_OK) return st;
+            if ((st = update(k, g, c0 + g2, 0, 0, set0, sd, side_sms, ctr)) != HS_OK) return st;
+            HS_CUDA(cudaEventRecord(ctx->ev_b, sd));
             HS_CUDA(cudaStreamWaitEvent(s, ctx->ev_b, 0));
-        } else if ((st = diag_chain(c0, s)) != HS_OK) {
-            return st;
+            ready = true;
+        } else {
+            if ((st = update(k, g, c0, 1, 1, set0, s, ctx->num_sms, -1)) != HS_OK) return st;
+            const bool more = c0 + 1 < nb;  // columns after c0
+            const bool side = lookahead && more;
+            if (side) {
+                HS_CUDA(cudaEventRecord(ctx->ev_a, s));
+                HS_CUDA(cudaStreamWaitEvent(sd, ctx->ev_a, 0));
+                if ((st = diag_chain(c0, sd)) != HS_OK) return st;
+                HS_CUDA(cudaEventRecord(ctx->ev_b, sd));
+            }
+            if (more && (st = update(k, g, c0, 2, 0, set0, s, side ? ctx->num_sms - kFree : ctx->num_sms, -1)) !=
+                            HS_OK)
+                return st;
+            if (side) {
+                HS_CUDA(cudaStreamWaitEvent(s, ctx->ev_b, 0));
+            } else if ((st = diag_chain(c0, s)) != HS_OK) {
+                return st;
+            }
+            ready = false;
         }
+        k = c0;
     }
     return HS_OK;
 }

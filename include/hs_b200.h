@@ -93,7 +93,10 @@ typedef enum hs_kernel_id {
     HS_KERNEL_VECTOR = 7,    /* vector ops, dots, CG updates */
     HS_KERNEL_ADJOINT = 8,   /* reverse-mode Cholesky block products (FP64 DMMA) */
     HS_KERNEL_GRAD = 9,      /* GP gradient contraction */
-    HS_KERNEL_COUNT = 10
+    HS_KERNEL_UPDATE_SIDE = 10, /* mixed factor: trailing-update launches on the look-ahead stream
+                                   (flops are counted where the tiles are: the in-group updates
+                                   here, a shared update's tiles with its first launch) */
+    HS_KERNEL_COUNT = 11
 } hs_kernel_id;
 typedef struct hs_kernel_profile {
     int64_t launches;
@@ -124,6 +127,16 @@ hs_status hs_ctx_set_reference_order(hs_ctx ctx, int cpu_chunks);
  * 2569 against 2184 ms); hs_mixed_solve's x reaches its target either way.
  * hs_gp_nlml_grad_mixed always uses one panel. */
 hs_status hs_ctx_set_mixed_accumulation(hs_ctx ctx, int panels);
+
+/* Mixed-precision factor (no reference counterpart): look-ahead by one panel group.
+ * While at least `min_rows` rows follow the next group of 4 panels, that group's
+ * diagonal blocks, panel TRSMs and in-group updates run on a high-priority stream on
+ * `side_sms` SMs, beside the trailing update of the current group on the others; the
+ * update's remaining tiles are then shared with a second launch on those SMs.
+ * side_sms = 0 keeps the look-ahead by one diagonal block.  Defaults: 16 SMs, 24576
+ * rows.  The factor is the same bit for bit either way: every block receives the same
+ * products in the same order.  side_sms must be in [0, SMs / 2], min_rows >= 0. */
+hs_status hs_ctx_set_mixed_lookahead(hs_ctx ctx, int side_sms, int min_rows);
 
 /* ------------------------------------------------------------------ operators */
 /* MatrixOperations::cholesky / cholesky_GPU / cholesky_optimizedGPU

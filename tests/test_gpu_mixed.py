@@ -290,3 +290,34 @@ def test_per_panel_accumulation_is_more_accurate_and_deterministic(hs, ctx):
     assert err[1] < 0.5 * err[4]
     assert out[1][0][0]["logdet"] == out[1][1][0]["logdet"]
     assert torch.equal(out[1][0][1], out[1][1][1])
+
+
+@pytest.mark.parametrize("N,bsz,prec", [
+    (3000, 128, "f16x3"), (2900, 256, "f16x3"), (1300, 128, "tf32x3"), (5000, 256, "bf16x3"),
+    (700, 128, "f16x3"), (257, 128, "f16x3"), (128, 128, "f16x3"),
+])
+def test_group_lookahead_gives_the_same_factor(hs, ctx, N, bsz, prec):
+    """hs_ctx_set_mixed_lookahead: factoring the next panel group on a few SMs beside
+    the current group's trailing update (the update's tiles shared between two
+    launches through a counter) adds the same products into every block in the same
+    order as the look-ahead by one diagonal block, so log|K| and the refined x are
+    identical bit for bit.  Run with the group look-ahead forced on for every group
+    (min_rows 0), on 16 and on a single side SM, on ragged sizes and group counts that
+    end on a partial group."""
+    A, b, _, _ = _system(hs, ctx, N, bsz, 8, 0.5, 1e-2, seed=N)
+    runs = {}
+    try:
+        for cfg in ((0, 0), (16, 0), (1, 0), (16, 24576)):
+            ctx.set_mixed_lookahead(*cfg)
+            solver = hs.MixedPrecisionSolver(A, ctx, prec)
+            x = solver.solve(b, tol=1e-14, max_steps=30).clone()
+            assert solver.report["backward_error"] <= 1e-14, (cfg, solver.report)
+            runs[cfg] = (solver.report, x)
+    finally:
+        ctx.set_mixed_lookahead()
+    rep0, x0 = runs[(0, 0)]
+    for cfg, (rep, x) in runs.items():
+        assert rep["logdet"] == rep0["logdet"], cfg
+        assert rep["initial_backward_error"] == rep0["initial_backward_error"], cfg
+        assert rep["refinement_steps"] == rep0["refinement_steps"], cfg
+        assert torch.equal(x, x0), cfg

@@ -28,3 +28,9 @@ def test_context_setters_reject_bad_arguments_without_a_device(hs):
 def test_gp_nlml_grad_rejects_unknown_precision(hs):
     with pytest.raises(ValueError, match="precision must be one of"):
         hs.gp_nlml_grad(None, [[0.0]], [0.0], [0.0, 0.0, 0.0], precision="fp8x3")
+
+
+def test_lookahead_setter_rejects_bad_arguments_without_a_device(hs):
+    lib = hs._lib.load()
+    assert lib.hs_ctx_set_mixed_lookahead(None, 16, 0) == 1
+    assert "side_sms must be in" in lib.hs_last_error().decode()
