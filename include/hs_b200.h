@@ -291,9 +291,10 @@ hs_status hs_gp_solve_host(hs_ctx ctx, const double* X_host, const double* y_hos
  * factor: half the packed matrix) is kept by the context between calls.  When
  * the low-precision factor of K meets a non-positive pivot (K too ill-conditioned
  * for it; the factorization stops at that block), a BF16- or FP16-split factor is
- * redone with 3xTF32 products, and then K + shift*I is factored with shift = 1e-6, 1e-5,
- * ... 1e-1 times the largest diagonal entry, the solve going straight to CG
- * preconditioned by that factor (report->shift, report->precision_used;
+ * redone with 3xTF32 products (an FP16 split that met a finite negative pivot is not),
+ * and then K + shift*I is factored, the shift growing from the failing pivot's size (at
+ * least 1e-6 times the largest diagonal entry, 10x the previous shift, at most 0.05x), the
+ * solve going straight to CG preconditioned by that factor (report->shift, report->precision_used;
  * report->logdet is then the log-determinant of the shifted matrix).  Returns HS_ERR_REFINEMENT_STALLED
  * when the target is not reached, HS_ERR_NOT_SPD when every shift fails. */
 typedef enum hs_precision {
