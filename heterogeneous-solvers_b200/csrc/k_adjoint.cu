@@ -29,8 +29,11 @@ namespace {
 constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3;
 constexpr int WM = 32, WN = 32, kWarpsN = BN / WN;
 constexpr int SPAD = 20;        // row pitch (doubles) of K-contiguous operand rows
-constexpr int LDTA = BM + 8;    // row pitch (doubles) of M-contiguous A rows
-constexpr int LDTB = BN + 8;    // row pitch (doubles) of N-contiguous B rows
+// M- / N-contiguous rows are read by lane (g, t) at row 4 kk + t, column 8 i + g: a pitch
+// of 4 (mod 16) doubles puts the 16 lanes of each half-warp's 8-byte loads on 16
+// different 8-byte bank pairs (a pitch of 8 mod 16 would put t and t + 2 on the same pair)
+constexpr int LDTA = BM + 4;    // row pitch (doubles) of M-contiguous A rows
+constexpr int LDTB = BN + 4;    // row pitch (doubles) of N-contiguous B rows
 constexpr int kStageA = BM * SPAD;  // >= BK * LDTA
 constexpr int kStageB = BN * SPAD;  // >= BK * LDTB
 constexpr int kStage = kStageA + kStageB;
