@@ -110,8 +110,9 @@ class Context:
 
     def set_mixed_accumulation(self, panels):
         """Mixed-precision factor: the trailing-update products of `panels` (1, 2 or 4)
-        panels are summed in the tensor cores' accumulator before each add into the
-        FP32 matrix; fewer is the more accurate factor and log|K|, more adds."""
+        panels are summed in the tensor cores' accumulator, a tile's units then in
+        registers before one add into the FP32 matrix; fewer is the more accurate factor
+        and log|K| (default 1)."""
         call("hs_ctx_set_mixed_accumulation", self.handle, int(panels))
 
     def set_mixed_lookahead(self, side_sms=16, min_rows=24576):

@@ -60,7 +60,7 @@ struct hs_ctx_s {
     // mixed factor: panels (1, 2 or 4) whose trailing-update products are summed in the
     // tensor cores' accumulator before one add into the FP32 matrix
     // (hs_ctx_set_mixed_accumulation)
-    int mixed_acc_panels = 4;
+    int mixed_acc_panels = 1;
     // mixed factor: look-ahead by a panel group on this many SMs while at least
     // mixed_min_rows rows follow the next group (hs_ctx_set_mixed_lookahead;
     // 0 SMs: look-ahead by one diagonal block only)

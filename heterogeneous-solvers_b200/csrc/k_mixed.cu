@@ -577,11 +577,11 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
         if (lane == 0) {
             // ---- MMA issuer
             // one accumulation unit = one tile x unit_panels panels: with unit_panels = 1
-            // each panel's product is added into C on its own (an FP32 round-to-nearest
-            // add in L2) instead of the whole group's K = npanels x BSZ sum in TMEM first,
-            // whose accumulation measured several times less accurate (log|K|, the
-            // unrefined backward error); the C tile stays in L2 across its units, so the
-            // DRAM traffic of a group pass is unchanged, but the extra adds cost time
+            // each panel's product is accumulated in TMEM on its own and the epilogue sums
+            // the units in registers (FP32 round-to-nearest adds), instead of the whole
+            // group's K = npanels x BSZ sum in TMEM, whose accumulation measured several
+            // times less accurate (log|K|, the unrefined backward error); C still gets
+            // one add a tile
             constexpr uint32_t idesc = umma_idesc(F::kFmt, F::kFmt, 128, BSZ);
             uint32_t g = 0;
             int un = 0;
@@ -661,6 +661,10 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                 break;
             }
             if (t == kNoTile) break;
+            // the tile's accumulation units, summed in registers (round-to-nearest FP32
+            // adds, in unit order): each unit's accumulator is released as soon as it is
+            // read, and C receives one add per tile
+            float sum[kChunks][32];
             for (int pi = 0; pi < units; ++pi, ++un) {  // accumulation units (see the issuer)
                 const int b = un & 1, u = un >> 1;
                 int wok = 0;
@@ -672,37 +676,41 @@ __global__ void __launch_bounds__(kUpdThreads, 1)
                     break;
                 }
                 tc_fence_after();
-                int r, c, ti;
-                decode(t, &r, &c, &ti);
-                const int cblk = (int)block_id(r, c, a.nb);
-                const int row0 = ti * 128 + q * 32;
                 const uint32_t tcol = taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BSZ + half * (BSZ / 2));
-                // the previous panel's adds into the same C entries (this warp's) have
-                // completed: the adds into an entry happen in panel order, so the result
-                // is the same every run
-                if (lane == 0 && pi > 0) bulk_wait0();
-#pragma unroll 1
-                for (int j = 0; j < kChunks; ++j) {
-                    uint32_t v[32];
-                    tmem_ld_32x32b_x32(tcol + (uint32_t)(j * 32), v);
-                    tmem_ld_wait();
-                    if (lane == 0) bulk_wait_read0();  // the previous chunk's reduce has read the tile
-                    __syncwarp();
 #pragma unroll
-                    for (int e = 0; e < 8; ++e)
-                        stile[lane * 8 + (e ^ (lane & 7))] =
-                            make_float4(-us * __uint_as_float(v[4 * e + 0]), -us * __uint_as_float(v[4 * e + 1]),
-                                        -us * __uint_as_float(v[4 * e + 2]), -us * __uint_as_float(v[4 * e + 3]));
-                    fence_proxy_async_smem();
-                    __syncwarp();
-                    if (lane == 0) {
-                        tma_reduce_add_3d(&mC32, stile, half * (BSZ / 2) + j * 32, row0, cblk);
-                        bulk_commit();
+                for (int h = 0; h < 2 * kChunks; ++h) {  // 16 columns at a time
+                    uint32_t v[16];
+                    tmem_ld_32x32b_x16(tcol + (uint32_t)(h * 16), v);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        float& sv = sum[h >> 1][(h & 1) * 16 + e];
+                        sv = (pi == 0 ? 0.0f : sv) + __uint_as_float(v[e]);
                     }
                 }
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&tempty[b]);
+            }
+            if (!eok) break;
+            int r, c, ti;
+            decode(t, &r, &c, &ti);
+            const int cblk = (int)block_id(r, c, a.nb);
+            const int row0 = ti * 128 + q * 32;
+#pragma unroll
+            for (int j = 0; j < kChunks; ++j) {
+                if (lane == 0) bulk_wait_read0();  // the previous chunk's reduce has read the tile
+                __syncwarp();
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                    stile[lane * 8 + (e ^ (lane & 7))] = make_float4(-us * sum[j][4 * e + 0], -us * sum[j][4 * e + 1],
+                                                                     -us * sum[j][4 * e + 2], -us * sum[j][4 * e + 3]);
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) {
+                    tma_reduce_add_3d(&mC32, stile, half * (BSZ / 2) + j * 32, row0, cblk);
+                    bulk_commit();
+                }
             }
         }
     }

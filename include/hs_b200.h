@@ -120,12 +120,13 @@ int64_t hs_ctx_launch_count(hs_ctx ctx);
 hs_status hs_ctx_set_reference_order(hs_ctx ctx, int cpu_chunks);
 
 /* Mixed-precision factor (no reference counterpart): `panels` (1, 2 or 4) trailing-update
- * panel products are summed in the tensor cores' FP32 accumulator before each
- * round-to-nearest add into the FP32 working matrix.  Fewer panels an add is the more
- * accurate factor and more adds into C: at N=131072 one panel gives a 3.8x smaller
- * log|K| error and 3 refinement steps instead of 5 for a 21 % slower factor (solve
- * 2569 against 2184 ms); hs_mixed_solve's x reaches its target either way.
- * hs_gp_nlml_grad_mixed always uses one panel. */
+ * panel products are summed in the tensor cores' FP32 accumulator as one unit; the units
+ * of an output tile are then summed with round-to-nearest FP32 adds in registers before
+ * one add into the FP32 working matrix.  Fewer panels a unit is the more accurate factor:
+ * at N=131072 one panel (the default) gives a 3.8x smaller log|K| error than four and 3
+ * refinement steps instead of 5 for ~1 % more factor time (solve 2222 against 2257 ms);
+ * hs_mixed_solve's x reaches its target either way.  hs_gp_nlml_grad_mixed always uses
+ * one panel. */
 hs_status hs_ctx_set_mixed_accumulation(hs_ctx ctx, int panels);
 
 /* Mixed-precision factor (no reference counterpart): look-ahead by one panel group.

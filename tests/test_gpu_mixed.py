@@ -284,7 +284,7 @@ def test_per_panel_accumulation_is_more_accurate_and_deterministic(hs, ctx):
             assert solver.report["backward_error"] <= 1e-14
             out.setdefault(mode, []).append((solver.report, x))
     finally:
-        ctx.set_mixed_accumulation(4)
+        ctx.set_mixed_accumulation(1)
     err = {m: abs(v[0][0]["logdet"] - ld_ref) for m, v in out.items()}
     print("log|K| error by panels an add:", err, "steps", {m: v[0][0]["refinement_steps"] for m, v in out.items()})
     assert err[1] < 0.5 * err[4]
