@@ -100,7 +100,7 @@ struct DevBuf {
 
 size_t adjoint_work_bytes(int nb, int bsz) {
     const size_t bb = (size_t)bsz * bsz * sizeof(double);
-    return bb * ((size_t)nb + 4 + (size_t)kAdjointPartialBlocks);
+    return bb * (2 * (size_t)nb + 3 + (size_t)kAdjointPartialBlocks);
 }
 
 void adjoint_bind(void* base, int nb, int bsz, AdjointWork* w) {
@@ -109,7 +109,7 @@ void adjoint_bind(void* base, int nb, int bsz, AdjointWork* w) {
     w->T = p;
     p += (size_t)nb * bb;
     w->Y = p;
-    p += bb;
+    p += (size_t)nb * bb;
     w->W1 = p;
     p += bb;
     w->W2 = p;
@@ -126,6 +126,9 @@ hs_status cholesky_adjoint_impl(hs_ctx ctx, const double* L, double* Abar, const
     const int valid_last = (int)(ctx->N - (int64_t)(nb - 1) * bsz);
     hs_status st = launch_zero_diag_upper(ctx, Abar, s);
     if (st != HS_OK) return st;
+    // Y_k = L_kk^-T for every k in one batched substitution (the last block against a
+    // copy with a unit diagonal on its padding rows)
+    if ((st = launch_diag_inverses(ctx, L, w.Y, w.Dp, s)) != HS_OK) return st;
     for (int k = nb - 1; k >= 0; --k) {
         const int m = nb - k - 1;
         const int64_t dk = block_id(k, k, nb);
@@ -136,9 +139,7 @@ hs_status cholesky_adjoint_impl(hs_ctx ctx, const double* L, double* Abar, const
             D = w.Dp;
         }
         double* Dbar = Abar + dk * bb;
-        // Y = D^-T
-        if ((st = launch_identity(ctx, w.Y, s)) != HS_OK) return st;
-        if ((st = launch_trsm_on(ctx, D, bsz, w.Y, 1, s)) != HS_OK) return st;
+        const double* Y = w.Y + (size_t)k * bb;  // D^-T
         if (m > 0) {
             double* Pbar = Abar + (dk + 1) * bb;  // panel blocks (k+1..nb-1, k), contiguous
             const double* P = L + (dk + 1) * bb;
@@ -161,7 +162,7 @@ hs_status cholesky_adjoint_impl(hs_ctx ctx, const double* L, double* Abar, const
             a.chain = 1;
             a.A0 = Pbar;
             a.sAi = bb;
-            a.B0 = w.Y;
+            a.B0 = Y;
             a.tb = 1;
             a.C0 = w.T;
             a.sCi = bb;
@@ -196,14 +197,14 @@ hs_status cholesky_adjoint_impl(hs_ctx ctx, const double* L, double* Abar, const
         a.items = 1;
         a.chain = 1;
         a.A0 = w.W2;
-        a.B0 = w.Y;
+        a.B0 = Y;
         a.tb = 1;
         a.C0 = w.W1;
         if ((st = launch_chain(ctx, a, nullptr, 0, s)) != HS_OK) return st;  // W1 = W2 Y^T
         a = chain_args(bsz);
         a.items = 1;
         a.chain = 1;
-        a.A0 = w.Y;
+        a.A0 = Y;
         a.B0 = w.W1;
         a.C0 = Dbar;
         a.epi = EPI_TRIL_HALF;

@@ -55,7 +55,7 @@ hs_status launch_trsm_on(hs_ctx ctx, const double* L, int n, double* B, int item
 // workspace of the reverse sweep
 struct AdjointWork {
     double* T;        // panel temporary (nb blocks)
-    double* Y;        // D^-T
+    double* Y;        // L_kk^-T for every diagonal block k (nb blocks)
     double* W1;
     double* W2;
     double* Dp;       // last diagonal block with unit padding diagonal
