@@ -75,18 +75,22 @@ __global__ void offdiag_f32_to_f64_kernel(const float* __restrict__ A32, double*
     }
 }
 
-// X = Y^T (one bsz x bsz block)
-__global__ void transpose_kernel(const double* __restrict__ Y, double* __restrict__ X, int n) {
-    __shared__ double t[32][33];
-    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
-    for (int i = threadIdx.y; i < 32; i += blockDim.y) t[i][threadIdx.x] = Y[(size_t)(by + i) * n + bx + threadIdx.x];
-    __syncthreads();
-    for (int i = threadIdx.y; i < 32; i += blockDim.y) X[(size_t)(bx + i) * n + by + threadIdx.x] = t[threadIdx.x][i];
-}
-
 __global__ void copy_pad_kernel(const double* __restrict__ y, double* __restrict__ b, int64_t N, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         b[i] = i < N ? y[i] : 0.0;
+}
+
+// L's diagonal blocks from the mixed factor's FP64 copies: the lower triangle of Ld_k,
+// zero above
+__global__ void tril_blocks_kernel(const double* __restrict__ Ld, double* __restrict__ L, int bsz, int nb) {
+    const int64_t bb = (int64_t)bsz * bsz;
+    const int k = blockIdx.y;
+    double* Dk = L + block_id(k, k, nb) * bb;
+    const double* Sk = Ld + (int64_t)k * bb;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < bb; e += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / bsz), j = (int)(e % bsz);
+        Dk[e] = j <= i ? Sk[e] : 0.0;
+    }
 }
 
 struct DevBuf {
@@ -267,7 +271,6 @@ static hs_status gp_nlml_grad_impl(hs_ctx ctx, const double* X, const double* y,
     const int nb = ctx->nb, bsz = ctx->bsz;
     const int64_t N = ctx->N, n = (int64_t)nb * bsz;
     const size_t packed = (size_t)total_blocks(nb) * bsz * bsz;
-    const size_t bb = (size_t)bsz * bsz;
     std::vector<double> ell(n_ell), inv_ell(d);
     for (int q = 0; q < n_ell; ++q) ell[q] = std::exp(theta[q]);
     for (int k = 0; k < d; ++k) inv_ell[k] = 1.0 / ell[n_ell == 1 ? 0 : k];
@@ -344,17 +347,10 @@ static hs_status gp_nlml_grad_impl(hs_ctx ctx, const double* X, const double* y,
         ctx->launches += 1;
         offdiag_f32_to_f64_kernel<<<4 * ctx->num_sms, 256, 0, s>>>(mw.A32, L, nb, bsz);
         HS_CHECK_LAUNCH("widen factor");
-        const dim3 tg(bsz / 32, bsz / 32), tb(32, 8);
-        for (int k = 0; k < nb; ++k) {
-            double* Dk = L + block_id(k, k, nb) * bb;
-            ctx->launches += 2;
-            transpose_kernel<<<tg, tb, 0, s>>>(mw.Yinv + (size_t)k * bb, w.W1, bsz);  // W1 = L_kk^-1
-            HS_CHECK_LAUNCH("transpose");
-            if ((st = launch_identity(ctx, w.W2, s)) != HS_OK) return st;
-            if ((st = launch_trsm_on(ctx, w.W1, bsz, w.W2, 1, s)) != HS_OK) return st;  // W2 = L_kk^T
-            transpose_kernel<<<tg, tb, 0, s>>>(w.W2, Dk, bsz);
-            HS_CHECK_LAUNCH("transpose");
-        }
+        // the diagonal blocks: the FP64 L_kk the diagonal chains factored (lower triangle)
+        ctx->launches += 1;
+        tril_blocks_kernel<<<dim3(16, nb), 256, 0, s>>>(mw.Ld, L, bsz, nb);
+        HS_CHECK_LAUNCH("diagonal blocks");
         HS_CUDA(cudaEventRecord(ev[1], s));
     }
     // the two NLML terms

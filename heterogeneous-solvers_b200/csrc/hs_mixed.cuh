@@ -13,7 +13,7 @@ namespace hs {
 struct MixedWork {
     float* A32 = nullptr;   // packed FP32 copy of K; its off-diagonal blocks end as L (used by the solves)
     float* LO = nullptr;    // low parts of two panel groups (slot set p: slots p nb..), then L_kk^-1 hi / lo
-    double* Ld = nullptr;   // FP64 diagonal blocks of L (nb blocks; only the diagonal entries are written)
+    double* Ld = nullptr;   // FP64 diagonal blocks of L (nb blocks; the lower triangle is written)
     double* Yinv = nullptr; // FP64 inverse diagonal blocks, Y_k = L_kk^-T (nb blocks)
     double* S = nullptr;    // FP64 scratch block (POTRF)
     __nv_bfloat16* P16 = nullptr;  // 16-bit (BF16 or FP16) split of two panel groups: set p hi blocks 2p nb.., lo (2p+1) nb..

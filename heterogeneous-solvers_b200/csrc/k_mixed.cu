@@ -804,8 +804,9 @@ __global__ void lo_part_kernel(const float* __restrict__ a, float* __restrict__ 
 // S (the working matrix) and B (held transposed in Y, which ends as X^T) stay in
 // global memory (L2-resident; S is read from the FP32 block directly at panel 0);
 // the panel is staged in shared memory k-major, block row p of B / X as [a][c].
-// Outputs: the diagonal of L in Ld (nothing reads the rest of L, and the FP32 block
-// keeps its input), Y = X^T, invHi = float(X), invLo = invHi - tf32(invHi).
+// Outputs: L's lower triangle in FP64 in Ld (the solves read its diagonal for log|K|,
+// the mixed NLML the whole block; the FP32 block keeps its input), Y = X^T,
+// invHi = float(X), invLo = invHi - tf32(invHi).
 // A pivot that is not > 0 on a valid row records its global row in *info.
 constexpr int kChainThreads = 256;
 
@@ -1074,9 +1075,17 @@ __global__ void __launch_bounds__(kChainThreads, 1)
             for (int j = 0; j < 32; ++j) PsT[j * kLt + rr] = v[j];
         }
         __syncthreads();
-        // the diagonal of L -> Ld (D is rewritten below); block row p of X goes out
-        // during the updates
-        if (tid < 32) Ld[(size_t)(c0 + tid) * n + c0 + tid] = D[tid * kD + tid];
+        // panel p of L -> Ld in FP64 (its diagonal block from D, lower triangle, and the
+        // rows below from PsT; D is rewritten below); block row p of X goes out during
+        // the updates
+        for (int e = tid; e < 32 * 32; e += kChainThreads) {
+            const int i = e >> 5, j = e & 31;
+            if (j <= i) Ld[(size_t)(c0 + i) * n + c0 + j] = D[i * kD + j];
+        }
+        for (int e = tid; e < mb * 32; e += kChainThreads) {
+            const int k = e & 31, rr = e >> 5;
+            Ld[(size_t)(c0 + 32 + rr) * n + c0 + k] = PsT[k * kLt + rr];
+        }
         if (mb == 0) {
             chain_outputs<BSZ>(Y, invHi, invLo, Xr, c0, zero_upper != 0, tid, kChainThreads);
             break;
