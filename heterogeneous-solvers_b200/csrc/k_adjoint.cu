@@ -84,6 +84,27 @@ __device__ __forceinline__ Elem chain_elem(const ChainArgs& a, int item, int64_t
     return e;
 }
 
+// One K slab of the warp's 32 x 32 tile, for one operand orientation (TA: A staged
+// M-contiguous, TB: B staged K-contiguous), as straight-line code per orientation
+template <bool TA, bool TB>
+__device__ __forceinline__ void slab_mma(double (&acc)[4][4][2], const double* __restrict__ As,
+                                         const double* __restrict__ Bs, int wm, int wn, int g, int t) {
+#pragma unroll
+    for (int kk = 0; kk < BK / 4; ++kk) {
+        double av[4], bv[4];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+            av[mi] = TA ? As[(kk * 4 + t) * LDTA + wm * WM + mi * 8 + g] : As[(wm * WM + mi * 8 + g) * SPAD + kk * 4 + t];
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+            bv[ni] = TB ? Bs[(wn * WN + ni * 8 + g) * SPAD + kk * 4 + t] : Bs[(kk * 4 + t) * LDTB + wn * WN + ni * 8 + g];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) dmma884(acc[mi][ni], av[mi], bv[ni]);
+    }
+}
+
 // One CTA = one 128 x 64 tile of one output block, accumulating the chain
 // elements [q0, q1) of its item; 8 warps of 32 x 32, K streamed in 16-wide
 // slabs through a 3-stage cp.async ring.  Operands that enter transposed are
@@ -160,28 +181,14 @@ __global__ void __launch_bounds__(256, 2) chain_dmma_kernel(ChainArgs a) {
         const int etb = a.mode == CHAIN_SYMM ? 0 : a.tb;
         const double* As = smem + (int)(kt % STAGES) * kStage;
         const double* Bs = As + kStageA;
-#pragma unroll
-        for (int kk = 0; kk < BK / 4; ++kk) {
-            double av[4], bv[4];
-            if (!eta) {
-#pragma unroll
-                for (int mi = 0; mi < 4; ++mi) av[mi] = As[(wm * WM + mi * 8 + g) * SPAD + kk * 4 + t];
-            } else {
-#pragma unroll
-                for (int mi = 0; mi < 4; ++mi) av[mi] = As[(kk * 4 + t) * LDTA + wm * WM + mi * 8 + g];
-            }
-            if (!etb) {
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(kk * 4 + t) * LDTB + wn * WN + ni * 8 + g];
-            } else {
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(wn * WN + ni * 8 + g) * SPAD + kk * 4 + t];
-            }
-#pragma unroll
-            for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni) dmma884(acc[mi][ni], av[mi], bv[ni]);
-        }
+        if (!eta && !etb)
+            slab_mma<false, false>(acc, As, Bs, wm, wn, g, t);
+        else if (eta && !etb)
+            slab_mma<true, false>(acc, As, Bs, wm, wn, g, t);
+        else if (!eta)
+            slab_mma<false, true>(acc, As, Bs, wm, wn, g, t);
+        else
+            slab_mma<true, true>(acc, As, Bs, wm, wn, g, t);
     }
     cp_async_wait<0>();
 
