@@ -119,8 +119,10 @@ __global__ void __launch_bounds__(256, 2) chain_dmma_kernel(ChainArgs a) {
     const int item = (int)(rest / (tpm * tpn));
     const int ti = tile / tpn, tj = tile % tpn;
     const int64_t q0 = a.chain * split / a.splits, q1 = a.chain * (split + 1) / a.splits;
-    const int spb = a.bsz / BK;  // slabs per chain element
-    const int64_t nk = (q1 - q0) * spb;
+    // slabs per chain element: bsz / BK = 16 or 8, a power of two, so that the slab
+    // index splits by shift and mask (no 64-bit division in the loop)
+    const int lg = a.bsz == 256 ? 4 : 3, spb = 1 << lg;
+    const int nk = (int)(q1 - q0) * spb;
     const int bsz = a.bsz;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -133,9 +135,9 @@ __global__ void __launch_bounds__(256, 2) chain_dmma_kernel(ChainArgs a) {
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
 
-    auto load_stage = [&](int stage, int64_t kt) {
-        const Elem e = chain_elem(a, item, q0 + kt / spb);
-        const int kc = (int)(kt % spb) * BK;
+    auto load_stage = [&](int stage, int kt) {
+        const Elem e = chain_elem(a, item, q0 + (kt >> lg));
+        const int kc = (kt & (spb - 1)) * BK;
         double* As = smem + stage * kStage;
         double* Bs = As + kStageA;
 #pragma unroll
@@ -166,20 +168,20 @@ __global__ void __launch_bounds__(256, 2) chain_dmma_kernel(ChainArgs a) {
         if (s < nk) load_stage(s, s);
         cp_async_commit();
     }
-    for (int64_t kt = 0; kt < nk; ++kt) {
+    for (int kt = 0, st = 0; kt < nk; ++kt, st = st + 1 == STAGES ? 0 : st + 1) {
         cp_async_wait<STAGES - 2>();
         __syncthreads();
         {
-            const int64_t nx = kt + STAGES - 1;
-            if (nx < nk) load_stage((int)(nx % STAGES), nx);
+            const int nx = kt + STAGES - 1;
+            if (nx < nk) load_stage(st == 0 ? STAGES - 1 : st - 1, nx);
             cp_async_commit();
         }
         // operand orientation of this slab's chain element (its pointers are only
         // needed by the loads): CHAIN_SYMM takes Abar_cr^T from c = r on (q >= r - k)
-        const int64_t q = q0 + kt / spb;
+        const int64_t q = q0 + (kt >> lg);
         const int eta = a.mode == CHAIN_SYMM ? (q >= item + 1) : a.ta;
         const int etb = a.mode == CHAIN_SYMM ? 0 : a.tb;
-        const double* As = smem + (int)(kt % STAGES) * kStage;
+        const double* As = smem + st * kStage;
         const double* Bs = As + kStageA;
         if (!eta && !etb)
             slab_mma<false, false>(acc, As, Bs, wm, wn, g, t);
@@ -338,6 +340,7 @@ hs_status launch_chain(hs_ctx ctx, ChainArgs a, double* partial, int64_t partial
     if (st != HS_OK) return st;
     HS_REQUIRE(a.bsz == 128 || a.bsz == 256, "the tensor-core adjoint supports matrixBlockSize 128 or 256");
     if (a.items <= 0 || a.chain <= 0) return HS_OK;
+    HS_REQUIRE(a.chain * (a.bsz / BK) < (1LL << 31), "product chain too long");
     const int64_t base = (int64_t)a.items * (a.bsz / BM) * (a.bsz / BN);
     a.splits = (partial && a.allow_split) ? pick_splits(base, a.chain, a.items, partial_blocks, 2 * ctx->num_sms) : 1;
     a.partial = partial;
