@@ -112,6 +112,7 @@ struct TrsmArgs {
     int64_t block_elems;  // panel mode: stride between B blocks (elements); 0: single item at A
     int l_diag_nb;        // > 0: item q solves against its own triangle, the diagonal block q of the
                           // packed matrix at L with this many block columns (L = its base)
+    int slab_rows;        // rows of B a CTA solves (0: kTrsmRows); fewer rows, more CTAs an item
 };
 
 __global__ void __launch_bounds__(256) trsm_kernel(TrsmArgs a) {
@@ -124,8 +125,9 @@ __global__ void __launch_bounds__(256) trsm_kernel(TrsmArgs a) {
     const int item = blockIdx.x / a.slabs;
     const int slab = blockIdx.x % a.slabs;
     const double* Lt = a.l_diag_nb > 0 ? a.L + (size_t)column_start(item, a.l_diag_nb) * n * n : a.L;
-    double* B = a.A + (a.block_elems ? (size_t)(a.item0 + item) * a.block_elems : 0) + (size_t)slab * kTrsmRows * a.ldB;
-    const int rows = min(kTrsmRows, a.rows_last - slab * kTrsmRows);
+    const int sr = a.slab_rows > 0 ? a.slab_rows : kTrsmRows;
+    double* B = a.A + (a.block_elems ? (size_t)(a.item0 + item) * a.block_elems : 0) + (size_t)slab * sr * a.ldB;
+    const int rows = min(sr, a.rows_last - slab * sr);
     for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
         const int r = e / n, c = e % n;
         Bs[r * bld + c] = B[(size_t)r * a.ldB + c];
@@ -607,7 +609,11 @@ hs_status launch_diag_inverse(hs_ctx ctx, const double* Lkk, double* Y, double* 
     ctx->launches += 1;
     identity_block_kernel<<<64, 256, 0, s>>>(Y, n);
     HS_CHECK_LAUNCH("identity");
-    hs_status st = launch_trsm_on(ctx, Lkk, n, Y, 1, s);
+    // one block on the critical path of the factor: 16 rows of Y a CTA (16 CTAs for
+    // bsz 256) instead of 64, the trailing products of a chunk spread 4x wider
+    constexpr int kRows = 16;
+    TrsmArgs ta{Lkk, n, n, Y, n, 0, (n + kRows - 1) / kRows, n, (int64_t)n * n, 0, kRows};
+    hs_status st = launch_trsm_args(ctx, ta, 1, s);
     if (st != HS_OK) return st;
     ctx->launches += 1;
     transpose_block_kernel<<<dim3(n / 32, n / 32), dim3(32, 8), 0, s>>>(Y, X, n);
