@@ -750,18 +750,36 @@ __global__ void f64_to_f32_fro2_kernel(const double* __restrict__ in, float* __r
                                        int64_t T, double* __restrict__ part) {
     __shared__ double sh[32];
     double acc = 0.0;
-    const int64_t bb2 = (int64_t)bsz * bsz / 2;
+    // a thread converts 4 consecutive values a step (two 16-byte loads, one 16-byte
+    // store), four steps' loads issued before their stores
+    const int bb4 = bsz * bsz / 4;
     for (int64_t blk = blockIdx.x; blk < T; blk += gridDim.x) {
         int bi, bj;
         block_coords(blk, nb, &bi, &bj);
-        const double2* src = reinterpret_cast<const double2*>(in) + blk * bb2;
-        float2* dst = reinterpret_cast<float2*>(out) + blk * bb2;
+        const double2* src = reinterpret_cast<const double2*>(in) + blk * 2 * bb4;
+        float4* dst = reinterpret_cast<float4*>(out) + blk * bb4;
         double sq = 0.0;
-        for (int64_t e = threadIdx.x; e < bb2; e += blockDim.x) {
-            const double2 v = __ldcs(src + e);
-            dst[e] = make_float2((float)v.x, (float)v.y);
-            sq += v.x * v.x;
-            sq += v.y * v.y;
+        for (int e0 = threadIdx.x; e0 < bb4; e0 += 4 * blockDim.x) {
+            double2 v[4][2];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = e0 + u * blockDim.x;
+                if (e < bb4) {
+                    v[u][0] = __ldcs(src + 2 * e);
+                    v[u][1] = __ldcs(src + 2 * e + 1);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = e0 + u * blockDim.x;
+                if (e < bb4) {
+                    dst[e] = make_float4((float)v[u][0].x, (float)v[u][0].y, (float)v[u][1].x, (float)v[u][1].y);
+                    sq += v[u][0].x * v[u][0].x;
+                    sq += v[u][0].y * v[u][0].y;
+                    sq += v[u][1].x * v[u][1].x;
+                    sq += v[u][1].y * v[u][1].y;
+                }
+            }
         }
         acc += ((bi == bj) ? 1.0 : 2.0) * sq;
     }
@@ -1323,7 +1341,7 @@ hs_status mixed_factor(hs_ctx ctx, const double* K64, MixedWork& w, cudaStream_t
     ctx->launches += 2;
     set_int_kernel<<<1, 1, 0, s>>>(w.err, 0);
     HS_CUDA(cudaMemsetAsync(w.tile_ctr, 0, (size_t)tile_counters(nb) * sizeof(unsigned long long), s));
-    if (fro_part && bsz % 2 == 0)
+    if (fro_part && bsz % 4 == 0)
         f64_to_f32_fro2_kernel<<<mixed_fro_grid(T), 256, 0, s>>>(K64, w.A32, bsz, nb, T, fro_part);
     else
         f64_to_f32_kernel<<<grid_for_elems(T * (int64_t)bb / 2, ctx->num_sms), 256, 0, s>>>(K64, w.A32,
